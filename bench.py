@@ -1,0 +1,390 @@
+"""Benchmark of the B200 K-Litho SOCS imaging path.
+
+Headline workload (the batched SOCS forward configuration): 384 seeded
+random-rectangle binary clips -- 128 x 512^2, 192 x 1024^2, 64 x 2048^2,
+1 nm pixels, 25-40 % density -- each imaged at 3 focus values with K = 24
+kernels per focus (one kernel set per clip size and focus).  A step images
+every clip at every focus once.  Metric: 1024^2-equivalent SOCS images per
+second (total image pixels / 1024^2 / time).
+
+`value` is device-resident throughput (masks already in HBM, images left in
+HBM); `e2e` is the same metric through the public host entry point
+(kl_socs_forward_host: pinned host masks in, host images out).  The roofline
+object covers the kernel with the largest share of device time.
+`--impl reference` times the reference's own CPU implementation of the path
+(oracle/_ref, else the restated oracle) on the host cores instead.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "k-litho_b200"))
+sys.path.insert(0, REPO)
+
+METRIC = "1024^2-equivalent SOCS images/s"
+UNIT = "images/s"
+CLASSES = [(512, 128), (1024, 192), (2048, 64)]  # (clip size, clips)
+FOCUS_NM = [-25.0, 0.0, 25.0]
+NK = 24
+SEED = 2024
+
+
+def peaks():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def class_band(L):
+    # config-0 optics: annular 0.6/0.9 on 41^2, NA 1.35 (sigma_o = 0.9)
+    import klitho as K
+    src = K.createSource(41, "Annular", 0.6, 0.9)
+    return K.bandSize(1.35, L, L, K.getOuterSigma(src))
+
+
+def make_masks(L, n, seed):
+    import synth
+    rng = np.random.default_rng(seed)
+    out = np.empty((n, L, L), dtype=np.float32)
+    for i in range(n):
+        out[i] = synth.rect_mask_fill(L, int(rng.integers(1 << 30)), float(rng.uniform(0.25, 0.40)))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev_index=0):
+        self.dev = dev_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    import klitho as K
+    import synth
+
+    ws, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    stream = torch.cuda.current_stream()
+
+    # weak scaling: every rank images its own full batch (clips are independent)
+    plans, masks_d, imgs_d, masks_h = [], [], [], []
+    for ci, (L, n) in enumerate(CLASSES):
+        Nx, Ny = class_band(L)
+        p = K.SocsPlan(L, L, Nx, Ny, NK, nsets=len(FOCUS_NM), max_clips=n)
+        for s, _f in enumerate(FOCUS_NM):
+            krn, sc = synth.random_kernels(NK, Nx, Ny, seed=SEED + 31 * ci + s)
+            p.set_kernels(s, krn, sc)
+        m = make_masks(L, n, SEED + 1000 * ci + rank)
+        masks_h.append(m)
+        masks_d.append(torch.from_numpy(m).to(f"cuda:{local}"))
+        imgs_d.append(torch.empty((n, len(FOCUS_NM), L, L), dtype=torch.float32,
+                                  device=f"cuda:{local}"))
+        plans.append(p)
+    px_per_step = sum(L * L * n * len(FOCUS_NM) for L, n in CLASSES)
+    img_equiv = px_per_step / float(1024 * 1024)
+
+    def step():
+        for p, md, im in zip(plans, masks_d, imgs_d):
+            p.forward(md, im, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    for p in plans:
+        p.enable_timing(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    stage_ms = np.zeros(3)
+    stage_n = np.zeros(3, dtype=int)
+    per_class = []
+    for (L, n), p in zip(CLASSES, plans):
+        t, c = p.stage_times()
+        stage_ms += np.array(t)
+        stage_n += np.array(c)
+        per_class.append({"L": L, "clips": n, "fwd_ms": t[0] / max(c[0], 1),
+                          "spectral_ms": t[1] / max(c[1], 1), "inverse_ms": t[2] / max(c[2], 1)})
+        p.enable_timing(False)
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = img_equiv * ws / (ms_per_step / 1e3)
+
+    # roofline of the dominant kernel (largest share of device time)
+    names = ["socs_forward", "socs_spectral", "socs_inverse"]
+    dom = int(np.argmax(stage_ms))
+    bytes_per_step = [sum(4 * L * L * n for L, n in CLASSES),
+                      0,
+                      sum(4 * L * L * n * len(FOCUS_NM) for L, n in CLASSES)]
+    launches_per_step = stage_n[dom] / args.steps
+    avg_launch_ms = stage_ms[dom] / max(stage_n[dom], 1)
+    peak, peak_kind = peaks()
+    roof = None
+    if bytes_per_step[dom] > 0:
+        achieved = bytes_per_step[dom] / launches_per_step / (avg_launch_ms / 1e3) / 1e9
+        roof = {"kernel": names[dom], "bound": "hbm", "achieved": round(achieved, 1),
+                "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None,
+                "algorithmic_bytes_per_launch": int(bytes_per_step[dom] / launches_per_step)}
+    else:
+        roof = {"kernel": names[dom], "bound": "compute", "achieved": None, "peak": None,
+                "unit": None, "frac": None, "traffic": None}
+    # the other streaming kernel too, for context
+    other = {names[i]: {"ms_per_step": round(stage_ms[i] / args.steps, 4)} for i in range(3)}
+    for i in (0, 2):
+        if stage_n[i]:
+            lps = stage_n[i] / args.steps
+            bw = bytes_per_step[i] / lps / (stage_ms[i] / stage_n[i] / 1e3) / 1e9
+            other[names[i]]["GBps"] = round(bw, 1)
+            other[names[i]]["frac_of_peak"] = round(bw / peak, 4)
+
+    # end-to-end through the host entry point (pinned host buffers)
+    e2e = run_e2e(plans, masks_h, args, ws, img_equiv)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(max_seconds=args.cpu_seconds)
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded random-rectangle masks; random complex kernels K=24)",
+            "config": {"workload": "batched SOCS forward: 128x512^2 + 192x1024^2 + 64x2048^2 "
+                                   "clips x 3 focus, K=24",
+                       "clips_per_gpu": sum(n for _, n in CLASSES), "focus_nm": FOCUS_NM,
+                       "image_equiv_1024_per_step_per_gpu": img_equiv,
+                       "l2": "inputs larger than L2 (1.9 GB masks, 5.8 GB images per GPU)",
+                       "parallelism": f"clip sharding, {ws} GPU(s), no collective on the data path"},
+            "roofline": roof, "stages": other, "per_class": per_class,
+            "clocks": clk, "e2e": e2e,
+            "gpu_launches": int(stage_n.sum()),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out))
+    for p in plans:
+        p.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_e2e(plans, masks_h, args, ws, img_equiv):
+    import torch
+    steps = max(1, min(args.steps, args.e2e_steps))
+    pinned_in, pinned_out = [], []
+    for (L, n), m in zip(CLASSES, masks_h):
+        ti = torch.from_numpy(m).pin_memory()
+        to = torch.empty((n, len(FOCUS_NM), L, L), dtype=torch.float32).pin_memory()
+        pinned_in.append(ti)
+        pinned_out.append(to)
+    import klitho as K
+    stream = torch.cuda.current_stream()
+
+    def once():
+        for p, ti, to in zip(plans, pinned_in, pinned_out):
+            K.check(K.lib().kl_socs_forward_host(
+                p._h, K.ctypes.cast(ti.data_ptr(), K._c_float_p), int(ti.shape[0]),
+                K.ctypes.cast(to.data_ptr(), K._c_float_p), int(stream.cuda_stream)),
+                "kl_socs_forward_host")
+
+    once()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        once()
+    torch.cuda.synchronize()
+    dt = (time.perf_counter() - t0) / steps
+    h2d = sum(int(t.numel()) * 4 for t in pinned_in)
+    d2h = sum(int(t.numel()) * 4 for t in pinned_out)
+    return {"value": round(img_equiv * ws / dt, 2), "unit": UNIT, "h2d_bytes_per_step": h2d,
+            "d2h_bytes_per_step": d2h, "ms_per_step": round(dt * 1e3, 2), "steps": steps,
+            "path": "kl_socs_forward_host (C ABI), pinned host buffers, copies timed"}
+
+
+# ---------------------------------------------------------------------------
+# CPU: the reference's own implementation of the path on the host cores
+# ---------------------------------------------------------------------------
+
+def _cpu_task(args):
+    """One reference SOCS image (FT_r2c + calcSOCS + FI) of an L^2 clip."""
+    L, seed, use_ref = args
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "k-litho_b200"))
+    import synth
+    from oracle import oracle as O
+    Nx = {512: 6, 1024: 13, 2048: 27}[L]
+    krn, sc = synth.random_kernels(NK, Nx, Nx, seed=seed)
+    mask = synth.rect_mask_fill(L, seed, 0.3)
+    t0 = time.perf_counter()
+    if use_ref:
+        O.ref_socs_image(mask, krn.real, krn.imag, sc, Nx, Nx)
+    else:
+        O.socs_image(mask, krn.astype(np.complex128), sc, Nx, Nx)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline_sample(max_seconds=20.0, processes=1):
+    """Time the reference SOCS path on 1024^2 clips (1 focus each) for about
+    `max_seconds`; returns images/s in the bench unit."""
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    done, t_start = 0, time.perf_counter()
+    with ctx.Pool(processes) as pool:
+        while time.perf_counter() - t_start < max_seconds:
+            pool.map(_cpu_task, [(1024, 100 + done + i, use_ref) for i in range(processes)])
+            done += processes
+    wall = time.perf_counter() - t_start
+    return {"value": round(done / wall, 4), "unit": UNIT, "cores": processes,
+            "kind": "reference" if use_ref else "port",
+            "sample": f"{done} clips of 1024^2 at one focus, K=24 "
+                      f"({'reference klitho_socs.cpp compiled with the project FFT shim' if use_ref else 'restated FP64 oracle'})"
+                      f", {wall:.1f} s wall"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    nproc = os.cpu_count() or 1
+    from oracle import oracle as O
+    use_ref = O.ref_available()
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    per_step = max(nproc, 1)
+    times = []
+    with ctx.Pool(nproc) as pool:
+        for s in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_task, [(1024, 7 + s * per_step + i, use_ref) for i in range(per_step)])
+            if s >= args.warmup:
+                times.append(time.perf_counter() - t0)
+    dt = float(np.mean(times))
+    value = per_step / dt
+    kind = "reference" if use_ref else "port"
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+           "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "batched SOCS forward (sampled: 1024^2 clips at one focus, K=24)"},
+           "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": nproc, "kind": kind,
+                            "sample": f"{per_step} x 1024^2 clips per step, one process per core"},
+           "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,144 @@
+/*
+ * klitho_gpu.h -- C ABI of the B200-native K-Litho Hopkins/SOCS imaging path.
+ *
+ * The reference (LithoSimulator/K-Litho) is two single-threaded C++ programs
+ * whose imaging functions take std::vector arguments and are called only
+ * from their own main()s; it has no library boundary.  This header
+ * re-expresses those functions as plain-C entry points (pointers, sizes,
+ * int status) so that a host program -- the drop-in klitho_tcc/klitho_socs
+ * CLIs shipped here, or a ctypes/cgo/JNI caller -- can bind them.  Each entry
+ * point names the reference function it replaces (file:line).
+ *
+ * Conventions
+ *  - Return value: KL_OK (0) on success, a KL_ERR_* code otherwise;
+ *    kl_last_error() returns a thread-local message for the last failure.
+ *  - "_dev" pointers are device (cudaMalloc'd) memory owned by the caller;
+ *    "_host" pointers are host memory.  Complex arrays are interleaved
+ *    (re, im) float32 ("c64") or float64 ("c128").
+ *  - `stream` is a cudaStream_t passed as void*; NULL means the legacy
+ *    default stream.  Device entry points are stream-ordered and do not
+ *    synchronise unless they return host results.
+ *  - Arrays are row-major with x fastest, as in the reference.  Band arrays
+ *    ("kernel layout") are (2Ny+1) x (2Nx+1) with frequency (ky, kx) at
+ *    [(ky+Ny)(2Nx+1) + kx+Nx], the layout of krn_<i>_{r,i}.bin.
+ *  - One handle per host thread; handles are not thread-safe.
+ */
+#ifndef KLITHO_GPU_H
+#define KLITHO_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KL_OK 0
+#define KL_ERR_INVALID 1        /* bad argument or size                     */
+#define KL_ERR_CUDA 2           /* CUDA runtime / launch failure            */
+#define KL_ERR_NOMEM 3          /* device or host allocation failed         */
+#define KL_ERR_UNSUPPORTED 4    /* geometry outside the compiled kernels    */
+#define KL_ERR_NOT_CONVERGED 5  /* eigen-solver hit its iteration cap       */
+#define KL_ERR_IO 6             /* file could not be opened / read / written */
+
+/* Library version (major*10000 + minor*100 + patch). */
+int kl_version(void);
+/* Message describing the most recent failure on this thread ("" if none). */
+const char* kl_last_error(void);
+
+/* ------------------------------------------------------------------------- */
+/* Host-side inputs (no GPU needed)                                            */
+/* ------------------------------------------------------------------------- */
+
+/* createSource: K-Litho-TCC/source.cpp:105-142 (shapes :5-88, point :122-129,
+ * import :130-139, normalisation to sum 1 :89-103,141).  `type` is one of
+ * "Annular", "Dipole", "CrossQuadrupole", "Point", "Import".  `out` holds
+ * srcSize*srcSize floats. */
+int kl_create_source(int srcSize, const char* type, float innerRadius, float outerRadius,
+                     float radius, float offset, int onXAxis, float ptX, float ptY,
+                     const char* sourceFile, float* out);
+
+/* createMask: common/mask.cpp:31-60 (line/space :5-29, import :42-52, centred
+ * embedding times dose :53-59).  `type` is "LineSpace" or "Import"; `out`
+ * holds Lx*Ly floats. */
+int kl_create_mask(int Lx, int Ly, int maskSizeX, int maskSizeY, const char* type, int lineWidth,
+                   int spaceWidth, int isHorizontal, const char* maskFile, float dose, float* out);
+
+/* getOuterSigma: K-Litho-TCC/klitho_tcc.cpp:52-67 (before main's clamp). */
+float kl_outer_sigma(const float* src_host, int srcSize);
+
+/* Band half-widths Nx, Ny: K-Litho-TCC/klitho_tcc.cpp:479-486 (outerSigma is
+ * clamped to 1 as at :480-483).  lambda is 193 nm (:439). */
+int kl_band_size(double NA, int Lx, int Ly, float outerSigma, int* Nx, int* Ny);
+
+/* Number of source pixels that enter the TCC (klitho_tcc.cpp:202-205). */
+int kl_source_point_count(const float* src_host, int srcSize, float outerSigma);
+
+/* readFloatArrayFromBinary / readFloatArrayFromTxt: common/file_io.cpp:204-260.
+ * Reads up to `size` floats ('.bin' raw little-endian, else whitespace text);
+ * a short file is zero-padded and, like the reference, a size mismatch is
+ * reported as a warning on stderr.  *count receives the number of floats the
+ * file held. */
+int kl_read_float_file(const char* path, int size, float* out, int* count);
+/* writeFloatArrayToBinary: common/file_io.cpp:137-150 */
+int kl_write_float_file(const char* path, const float* data, int size);
+
+/* writeKernelInfo / readKernelInfo: common/file_io.cpp:262-307 (same text). */
+int kl_write_kernel_info(const char* path, int krnSizeX, int krnSizeY, int nk,
+                         const float* scales);
+/* scales receives up to `cap` eigenvalues; *nk the declared kernel count. */
+int kl_read_kernel_info(const char* path, int* krnSizeX, int* krnSizeY, int* nk, float* scales,
+                        int cap);
+
+/* ------------------------------------------------------------------------- */
+/* SOCS imaging: K-Litho-SOCS/klitho_socs.cpp:196-241 (calcSOCS) + :158-194   */
+/* (FI), fed by FT_r2c :70-121.  Fused single-precision path.                 */
+/* ------------------------------------------------------------------------- */
+
+typedef struct kl_socs_plan_s* kl_socs_plan;
+
+/* Plan for clips of period Lx x Ly imaged with `nsets` kernel sets (e.g. one
+ * per focus) of `nk` kernels of band (2Nx+1) x (2Ny+1), for batches of up to
+ * `max_clips` clips.  Allocates the plan's device workspace on the current
+ * device.  Returns KL_ERR_UNSUPPORTED (with a message) for geometries the
+ * compiled kernels do not cover. */
+int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
+                        int max_clips);
+int kl_socs_plan_destroy(kl_socs_plan plan);
+
+/* Upload kernel set `set`: nk planes of the kernel layout, real and imaginary
+ * parts separately (as krn_<i>_r.bin / krn_<i>_i.bin hold them), and nk
+ * eigenvalues (kernel_info.txt).  Host pointers; synchronous. */
+int kl_socs_set_kernels(kl_socs_plan plan, int set, const float* krn_re_host,
+                        const float* krn_im_host, const float* scales_host);
+
+/* images_dev[c][s] (nclips x nsets x Ly x Lx float32) from masks_dev
+ * (nclips x Ly x Lx float32, already embedded in the period as createMask
+ * does).  Stream-ordered. */
+int kl_socs_forward(kl_socs_plan plan, const float* masks_dev, int nclips, float* images_dev,
+                    void* stream);
+
+/* Same computation from and to host memory: copies the masks in, images
+ * out, and synchronises `stream` before returning. */
+int kl_socs_forward_host(kl_socs_plan plan, const float* masks_host, int nclips,
+                         float* images_host, void* stream);
+
+/* Stage timing for diagnostics and roofline accounting.  While enabled, every
+ * kl_socs_forward records CUDA events on its stream around its three kernels
+ * (mask forward transform, spectral core, image synthesis).
+ * kl_socs_stage_times synchronises on those events, returns the summed
+ * milliseconds and launch counts per stage (ms[3], launches[3]) and clears
+ * them.  No reference counterpart (the reference prints wall time only,
+ * klitho_socs.cpp:355-361). */
+int kl_socs_enable_timing(kl_socs_plan plan, int enable);
+int kl_socs_stage_times(kl_socs_plan plan, double* ms, int* launches);
+
+/* The band of FT_r2c (K-Litho-TCC/klitho_tcc.cpp:97-148): centred spectrum
+ * scaled by 1/(Lx Ly), cropped to the kernel band; band_dev receives nclips
+ * c64 arrays in the kernel layout.  Stream-ordered. */
+int kl_mask_spectrum(kl_socs_plan plan, const float* masks_dev, int nclips, float* band_dev,
+                     void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KLITHO_GPU_H */

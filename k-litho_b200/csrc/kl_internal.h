@@ -1,0 +1,69 @@
+// kl_internal.h -- host-side internal types shared by the library sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/klitho_gpu.h"
+
+namespace kl {
+
+// thread-local last error text, returned by kl_last_error()
+void set_error(const std::string& msg);
+const char* last_error();
+
+#define KL_CUDA_TRY(expr)                                                      \
+  do {                                                                         \
+    cudaError_t _e = (expr);                                                   \
+    if (_e != cudaSuccess) {                                                   \
+      ::kl::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));     \
+      return KL_ERR_CUDA;                                                      \
+    }                                                                          \
+  } while (0)
+
+#define KL_CHECK_ARG(cond, msg)        \
+  do {                                 \
+    if (!(cond)) {                     \
+      ::kl::set_error(msg);            \
+      return KL_ERR_INVALID;           \
+    }                                  \
+  } while (0)
+
+// Geometry of the fused FP32 SOCS pipeline for one clip size.
+struct SocsGeom {
+  int Lx, Ly;      // clip period in pixels (1 nm each)
+  int Nx, Ny;      // kernel band half-widths
+  int nbx, nby;    // 2N+1
+  int nf;          // Nx+1 row-DFT bins kept by the forward pass (fx >= 0)
+  int ntx, nty;    // 2Nx+1 and 4Ny+1: intensity spectrum half plane
+  int P;           // points per lane in the row transforms
+  int V;           // virtual lanes per row, Lx = V * P
+  int J;           // rows per strip (power of two >= max(32, 2Ny+1))
+  int nS;          // strips per clip, Ly = nS * J
+  int G;           // spectral grid (power of two >= max(32, 4Nx+1, 4Ny+1))
+  int dx, dy;      // one-pixel output shift of odd periods (0 or 1)
+  int NFM, NBM;    // padded forward / inverse bin counts (16, 32 or 64)
+};
+
+// Fill geometry; returns KL_OK or KL_ERR_UNSUPPORTED with a message.
+int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g);
+
+// Device workspace bytes needed for `nclips` clips and `nsets` kernel sets.
+size_t socs_partial_bytes(const SocsGeom& g, int nclips);
+size_t socs_spectrum_bytes(const SocsGeom& g, int nclips, int nsets);
+
+// Launchers (stream-ordered).  Buffers are device pointers.
+int socs_launch_forward(const SocsGeom& g, const float* masks, int nclips, float2* partial,
+                        cudaStream_t st);
+int socs_launch_spectral(const SocsGeom& g, const float2* partial, int nclips, const float2* H,
+                         const float* lam, int K, int nsets, float2* T, cudaStream_t st);
+int socs_launch_inverse(const SocsGeom& g, const float2* T, int nclips, int nsets, float* images,
+                        cudaStream_t st);
+// centred band of FT_r2c (DC at the band centre), complex64 nby x nbx per clip
+int socs_launch_band(const SocsGeom& g, const float2* partial, int nclips, float2* band,
+                     cudaStream_t st);
+
+}  // namespace kl

@@ -1,0 +1,199 @@
+// kl_socs_api.cpp -- C ABI for SOCS imaging plans (see include/klitho_gpu.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kl_internal.h"
+
+struct kl_socs_plan_s {
+  kl::SocsGeom g{};
+  int K = 0, nsets = 0, max_clips = 0;
+  int device = 0;
+  float2* H = nullptr;       // nsets x K x nby x nbx
+  float* lam = nullptr;      // nsets x K
+  float2* partial = nullptr; // max_clips strip partials
+  float2* T = nullptr;       // max_clips x nsets intensity spectra
+  float* stage_in = nullptr; // host-entry staging (lazily allocated)
+  float* stage_out = nullptr;
+  size_t stage_clips = 0;
+  // optional stage timing: 4 events per kl_socs_forward (start, after the
+  // forward, spectral and inverse kernels)
+  bool timing = false;
+  std::vector<cudaEvent_t> events;
+};
+
+namespace {
+void drop_events(kl_socs_plan p) {
+  for (cudaEvent_t e : p->events) cudaEventDestroy(e);
+  p->events.clear();
+}
+
+void free_plan(kl_socs_plan p) {
+  if (!p) return;
+  drop_events(p);
+  cudaFree(p->H);
+  cudaFree(p->lam);
+  cudaFree(p->partial);
+  cudaFree(p->T);
+  cudaFree(p->stage_in);
+  cudaFree(p->stage_out);
+  delete p;
+}
+
+int alloc(void** ptr, size_t bytes, const char* what) {
+  cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    kl::set_error(std::string("cudaMalloc(") + what + "): " + cudaGetErrorString(e));
+    cudaGetLastError();
+    return KL_ERR_NOMEM;
+  }
+  return KL_OK;
+}
+
+int mark(kl_socs_plan p, cudaStream_t st) {
+  if (!p->timing) return KL_OK;
+  cudaEvent_t e;
+  KL_CUDA_TRY(cudaEventCreate(&e));
+  p->events.push_back(e);
+  KL_CUDA_TRY(cudaEventRecord(e, st));
+  return KL_OK;
+}
+
+int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st) {
+  int rc;
+  if ((rc = mark(p, st))) return rc;
+  if ((rc = kl::socs_launch_forward(p->g, masks, nclips, p->partial, st))) return rc;
+  if ((rc = mark(p, st))) return rc;
+  rc = kl::socs_launch_spectral(p->g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, p->T, st);
+  if (rc) return rc;
+  if ((rc = mark(p, st))) return rc;
+  if ((rc = kl::socs_launch_inverse(p->g, p->T, nclips, p->nsets, images, st))) return rc;
+  return mark(p, st);
+}
+}  // namespace
+
+extern "C" {
+
+int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
+                        int max_clips) {
+  KL_CHECK_ARG(plan != nullptr, "kl_socs_plan_create: plan is NULL");
+  *plan = nullptr;
+  KL_CHECK_ARG(nk > 0 && nsets > 0 && max_clips > 0, "kl_socs_plan_create: nk, nsets, max_clips must be positive");
+  kl::SocsGeom g;
+  int rc = kl::socs_geometry(Lx, Ly, Nx, Ny, &g);
+  if (rc) return rc;
+  kl_socs_plan p = new (std::nothrow) kl_socs_plan_s;
+  if (!p) {
+    kl::set_error("kl_socs_plan_create: out of host memory");
+    return KL_ERR_NOMEM;
+  }
+  p->g = g;
+  p->K = nk;
+  p->nsets = nsets;
+  p->max_clips = max_clips;
+  cudaGetDevice(&p->device);
+  const size_t nb2 = (size_t)g.nby * g.nbx;
+  if ((rc = alloc((void**)&p->H, sizeof(float2) * nb2 * nk * nsets, "kernels")) ||
+      (rc = alloc((void**)&p->lam, sizeof(float) * (size_t)nk * nsets, "eigenvalues")) ||
+      (rc = alloc((void**)&p->partial, kl::socs_partial_bytes(g, max_clips), "partials")) ||
+      (rc = alloc((void**)&p->T, kl::socs_spectrum_bytes(g, max_clips, nsets), "spectra"))) {
+    free_plan(p);
+    return rc;
+  }
+  cudaMemset(p->H, 0, sizeof(float2) * nb2 * nk * nsets);
+  cudaMemset(p->lam, 0, sizeof(float) * (size_t)nk * nsets);
+  *plan = p;
+  return KL_OK;
+}
+
+int kl_socs_plan_destroy(kl_socs_plan plan) {
+  free_plan(plan);
+  return KL_OK;
+}
+
+int kl_socs_set_kernels(kl_socs_plan p, int set, const float* re, const float* im,
+                        const float* scales) {
+  KL_CHECK_ARG(p && re && im && scales, "kl_socs_set_kernels: NULL argument");
+  KL_CHECK_ARG(set >= 0 && set < p->nsets, "kl_socs_set_kernels: set out of range");
+  const size_t nb2 = (size_t)p->g.nby * p->g.nbx;
+  std::vector<float2> h(nb2 * p->K);
+  for (size_t i = 0; i < h.size(); ++i) h[i] = make_float2(re[i], im[i]);
+  KL_CUDA_TRY(cudaMemcpy(p->H + (size_t)set * p->K * nb2, h.data(), sizeof(float2) * h.size(),
+                         cudaMemcpyHostToDevice));
+  KL_CUDA_TRY(cudaMemcpy(p->lam + (size_t)set * p->K, scales, sizeof(float) * p->K,
+                         cudaMemcpyHostToDevice));
+  return KL_OK;
+}
+
+int kl_socs_forward(kl_socs_plan p, const float* masks, int nclips, float* images, void* stream) {
+  KL_CHECK_ARG(p && masks && images, "kl_socs_forward: NULL argument");
+  KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_socs_forward: nclips exceeds the plan");
+  return run_forward(p, masks, nclips, images, (cudaStream_t)stream);
+}
+
+int kl_socs_forward_host(kl_socs_plan p, const float* masks_host, int nclips, float* images_host,
+                         void* stream) {
+  KL_CHECK_ARG(p && masks_host && images_host, "kl_socs_forward_host: NULL argument");
+  KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_socs_forward_host: nclips exceeds the plan");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t px = (size_t)p->g.Lx * p->g.Ly;
+  if (p->stage_clips < (size_t)nclips) {
+    cudaFree(p->stage_in);
+    cudaFree(p->stage_out);
+    p->stage_in = p->stage_out = nullptr;
+    p->stage_clips = 0;
+    int rc;
+    if ((rc = alloc((void**)&p->stage_in, sizeof(float) * px * nclips, "mask staging")) ||
+        (rc = alloc((void**)&p->stage_out, sizeof(float) * px * nclips * p->nsets, "image staging")))
+      return rc;
+    p->stage_clips = (size_t)nclips;
+  }
+  KL_CUDA_TRY(cudaMemcpyAsync(p->stage_in, masks_host, sizeof(float) * px * nclips,
+                              cudaMemcpyHostToDevice, st));
+  int rc = run_forward(p, p->stage_in, nclips, p->stage_out, st);
+  if (rc) return rc;
+  KL_CUDA_TRY(cudaMemcpyAsync(images_host, p->stage_out, sizeof(float) * px * nclips * p->nsets,
+                              cudaMemcpyDeviceToHost, st));
+  KL_CUDA_TRY(cudaStreamSynchronize(st));
+  return KL_OK;
+}
+
+int kl_socs_enable_timing(kl_socs_plan p, int enable) {
+  KL_CHECK_ARG(p, "kl_socs_enable_timing: NULL plan");
+  p->timing = enable != 0;
+  if (!p->timing) drop_events(p);
+  return KL_OK;
+}
+
+int kl_socs_stage_times(kl_socs_plan p, double* ms, int* launches) {
+  KL_CHECK_ARG(p && ms && launches, "kl_socs_stage_times: NULL argument");
+  for (int i = 0; i < 3; ++i) {
+    ms[i] = 0.0;
+    launches[i] = 0;
+  }
+  for (size_t b = 0; b + 3 < p->events.size(); b += 4) {
+    KL_CUDA_TRY(cudaEventSynchronize(p->events[b + 3]));
+    for (int i = 0; i < 3; ++i) {
+      float t = 0.f;
+      KL_CUDA_TRY(cudaEventElapsedTime(&t, p->events[b + i], p->events[b + i + 1]));
+      ms[i] += t;
+      launches[i] += 1;
+    }
+  }
+  drop_events(p);
+  return KL_OK;
+}
+
+int kl_mask_spectrum(kl_socs_plan p, const float* masks, int nclips, float* band, void* stream) {
+  KL_CHECK_ARG(p && masks && band, "kl_mask_spectrum: NULL argument");
+  KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_mask_spectrum: nclips exceeds the plan");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = kl::socs_launch_forward(p->g, masks, nclips, p->partial, st);
+  if (rc) return rc;
+  return kl::socs_launch_band(p->g, p->partial, nclips, reinterpret_cast<float2*>(band), st);
+}
+
+}  // extern "C"

@@ -1,0 +1,243 @@
+"""ctypes binding of libklitho_gpu (include/klitho_gpu.h).
+
+The Python-side mirror of the K-Litho imaging interface: the same function
+names and argument meanings as the reference's C++ functions (createSource,
+createMask, getOuterSigma, calcSOCS, ...), backed by the B200 library.  It
+loads ``lib/libklitho_gpu.so`` from this directory and raises if it is
+missing -- there is no CPU fallback.  Device buffers are torch CUDA tensors
+(PyTorch provides allocation and streams only); every computation runs in
+the library's own CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libklitho_gpu.so")
+
+KL_OK = 0
+KL_ERR_INVALID = 1
+KL_ERR_CUDA = 2
+KL_ERR_NOMEM = 3
+KL_ERR_UNSUPPORTED = 4
+KL_ERR_NOT_CONVERGED = 5
+KL_ERR_IO = 6
+
+_c_int_p = ctypes.POINTER(ctypes.c_int)
+_c_float_p = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+_LIB = None
+
+
+class KLError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where} failed with status {code}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Load the library (raises if it has not been built)."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing; run `make -C k-litho_b200` "
+                              "(or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        L.kl_version.restype = ctypes.c_int
+        L.kl_last_error.restype = ctypes.c_char_p
+        L.kl_create_source.argtypes = [ctypes.c_int, ctypes.c_char_p, ctypes.c_float,
+                                       ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                       ctypes.c_char_p, _c_float_p]
+        L.kl_create_mask.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_char_p, ctypes.c_float, _c_float_p]
+        L.kl_outer_sigma.restype = ctypes.c_float
+        L.kl_outer_sigma.argtypes = [_c_float_p, ctypes.c_int]
+        L.kl_band_size.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                   _c_int_p, _c_int_p]
+        L.kl_source_point_count.argtypes = [_c_float_p, ctypes.c_int, ctypes.c_float]
+        L.kl_read_float_file.argtypes = [ctypes.c_char_p, ctypes.c_int, _c_float_p, _c_int_p]
+        L.kl_write_float_file.argtypes = [ctypes.c_char_p, _c_float_p, ctypes.c_int]
+        L.kl_write_kernel_info.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _c_float_p]
+        L.kl_read_kernel_info.argtypes = [ctypes.c_char_p, _c_int_p, _c_int_p, _c_int_p,
+                                          _c_float_p, ctypes.c_int]
+        L.kl_socs_plan_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int]
+        L.kl_socs_plan_destroy.argtypes = [_vp]
+        L.kl_socs_set_kernels.argtypes = [_vp, ctypes.c_int, _c_float_p, _c_float_p, _c_float_p]
+        L.kl_socs_forward.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+        L.kl_socs_forward_host.argtypes = [_vp, _c_float_p, ctypes.c_int, _c_float_p, _vp]
+        L.kl_mask_spectrum.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+        L.kl_socs_enable_timing.argtypes = [_vp, ctypes.c_int]
+        L.kl_socs_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), _c_int_p]
+        _LIB = L
+    return _LIB
+
+
+def last_error() -> str:
+    return lib().kl_last_error().decode(errors="replace")
+
+
+def check(rc: int, where: str) -> None:
+    if rc != KL_OK:
+        raise KLError(rc, where, last_error())
+
+
+def _fp(a: np.ndarray):
+    return a.ctypes.data_as(_c_float_p)
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+def _dev_ptr(t) -> int:
+    if not (t.is_cuda and t.is_contiguous()):
+        raise ValueError("expected a contiguous CUDA tensor")
+    return int(t.data_ptr())
+
+
+# ---------------------------------------------------------------------------
+# host-side inputs (mirrors of source.cpp / mask.cpp / file_io.cpp)
+# ---------------------------------------------------------------------------
+
+def createSource(srcSize: int, srcType: str, innerRadius=0.6, outerRadius=0.9, radius=0.1,
+                 offset=0.5, onXAxis=1, ptX=0.6, ptY=0.2, sourceFile="") -> np.ndarray:
+    out = np.zeros(srcSize * srcSize, dtype=np.float32)
+    check(lib().kl_create_source(int(srcSize), srcType.encode(), innerRadius, outerRadius,
+                                 radius, offset, int(onXAxis), ptX, ptY, sourceFile.encode(),
+                                 _fp(out)), "kl_create_source")
+    return out.reshape(srcSize, srcSize)
+
+
+def createMask(Lx, Ly, maskSizeX, maskSizeY, maskType="LineSpace", lineWidth=128,
+               spaceWidth=128, isHorizontal=0, maskFile="", dose=1.0) -> np.ndarray:
+    out = np.zeros(Lx * Ly, dtype=np.float32)
+    check(lib().kl_create_mask(int(Lx), int(Ly), int(maskSizeX), int(maskSizeY),
+                               maskType.encode(), int(lineWidth), int(spaceWidth),
+                               int(isHorizontal), maskFile.encode(), float(dose), _fp(out)),
+          "kl_create_mask")
+    return out.reshape(Ly, Lx)
+
+
+def getOuterSigma(src: np.ndarray) -> float:
+    s = np.ascontiguousarray(src, dtype=np.float32)
+    return float(lib().kl_outer_sigma(_fp(s), int(s.shape[0])))
+
+
+def bandSize(NA: float, Lx: int, Ly: int, outerSigma: float) -> tuple[int, int]:
+    nx, ny = ctypes.c_int(), ctypes.c_int()
+    check(lib().kl_band_size(float(NA), int(Lx), int(Ly), float(outerSigma), ctypes.byref(nx),
+                             ctypes.byref(ny)), "kl_band_size")
+    return nx.value, ny.value
+
+
+def sourcePointCount(src: np.ndarray, outerSigma: float) -> int:
+    s = np.ascontiguousarray(src, dtype=np.float32)
+    return int(lib().kl_source_point_count(_fp(s), int(s.shape[0]), float(outerSigma)))
+
+
+def readFloatArray(path: str, size: int) -> tuple[np.ndarray, int]:
+    out = np.zeros(size, dtype=np.float32)
+    cnt = ctypes.c_int()
+    check(lib().kl_read_float_file(path.encode(), int(size), _fp(out), ctypes.byref(cnt)),
+          "kl_read_float_file")
+    return out, cnt.value
+
+
+def writeFloatArray(path: str, data: np.ndarray) -> None:
+    d = np.ascontiguousarray(data, dtype=np.float32).ravel()
+    check(lib().kl_write_float_file(path.encode(), _fp(d), int(d.size)), "kl_write_float_file")
+
+
+def writeKernelInfo(path: str, kx: int, ky: int, scales) -> None:
+    s = np.ascontiguousarray(scales, dtype=np.float32)
+    check(lib().kl_write_kernel_info(path.encode(), int(kx), int(ky), int(s.size), _fp(s)),
+          "kl_write_kernel_info")
+
+
+def readKernelInfo(path: str, cap: int = 4096):
+    kx, ky, nk = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_int(0)
+    sc = np.zeros(cap, dtype=np.float32)
+    check(lib().kl_read_kernel_info(path.encode(), ctypes.byref(kx), ctypes.byref(ky),
+                                    ctypes.byref(nk), _fp(sc), cap), "kl_read_kernel_info")
+    return kx.value, ky.value, nk.value, sc[: max(nk.value, 0)].copy()
+
+
+# ---------------------------------------------------------------------------
+# SOCS imaging plan
+# ---------------------------------------------------------------------------
+
+class SocsPlan:
+    """GPU SOCS imaging for clips of one period (calcSOCS + FI on device)."""
+
+    def __init__(self, Lx: int, Ly: int, Nx: int, Ny: int, nk: int, nsets: int = 1,
+                 max_clips: int = 1):
+        self.Lx, self.Ly, self.Nx, self.Ny = int(Lx), int(Ly), int(Nx), int(Ny)
+        self.nk, self.nsets, self.max_clips = int(nk), int(nsets), int(max_clips)
+        h = _vp()
+        check(lib().kl_socs_plan_create(ctypes.byref(h), self.Lx, self.Ly, self.Nx, self.Ny,
+                                        self.nk, self.nsets, self.max_clips),
+              "kl_socs_plan_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().kl_socs_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_kernels(self, set_index: int, krn: np.ndarray, scales: np.ndarray) -> None:
+        """krn: nk x (2Ny+1)(2Nx+1) complex (kernel-file layout)."""
+        k = np.asarray(krn)
+        re = np.ascontiguousarray(k.real, dtype=np.float32)
+        im = np.ascontiguousarray(k.imag, dtype=np.float32)
+        sc = np.ascontiguousarray(scales, dtype=np.float32)
+        check(lib().kl_socs_set_kernels(self._h, int(set_index), _fp(re), _fp(im), _fp(sc)),
+              "kl_socs_set_kernels")
+
+    def forward(self, masks_dev, images_dev, nclips: int | None = None, stream=None) -> None:
+        n = masks_dev.shape[0] if nclips is None else nclips
+        check(lib().kl_socs_forward(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(images_dev),
+                                    _stream_ptr(stream)), "kl_socs_forward")
+
+    def forward_host(self, masks: np.ndarray, images: np.ndarray | None = None,
+                     stream=None) -> np.ndarray:
+        m = np.ascontiguousarray(masks, dtype=np.float32)
+        n = m.shape[0]
+        if images is None:
+            images = np.empty((n, self.nsets, self.Ly, self.Lx), dtype=np.float32)
+        check(lib().kl_socs_forward_host(self._h, _fp(m), int(n), _fp(images),
+                                         _stream_ptr(stream)), "kl_socs_forward_host")
+        return images
+
+    def enable_timing(self, on: bool = True) -> None:
+        check(lib().kl_socs_enable_timing(self._h, int(bool(on))), "kl_socs_enable_timing")
+
+    def stage_times(self):
+        """(ms[3], launches[3]) for the forward, spectral and inverse kernels."""
+        ms = (ctypes.c_double * 3)()
+        n = (ctypes.c_int * 3)()
+        check(lib().kl_socs_stage_times(self._h, ms, n), "kl_socs_stage_times")
+        return list(ms), list(n)
+
+    def mask_spectrum(self, masks_dev, band_dev, nclips: int | None = None, stream=None) -> None:
+        n = masks_dev.shape[0] if nclips is None else nclips
+        check(lib().kl_mask_spectrum(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(band_dev),
+                                     _stream_ptr(stream)), "kl_mask_spectrum")
