@@ -165,13 +165,15 @@ def run_ours(args):
         for p, md, im in zip(plans, masks_d, imgs_d):
             p.forward(md, im, stream=stream)
 
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    time.sleep(0.5)  # let the sampler start before the timed region
+    clocks.lines.clear()
     for p in plans:
         p.enable_timing(True)
-    clocks = ClockSampler(local)
-    clocks.start()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -231,7 +233,7 @@ def run_ours(args):
             other[names[i]]["frac_of_peak"] = round(bw / peak, 4)
 
     # end-to-end through the host entry point (pinned host buffers)
-    e2e = run_e2e(plans, masks_h, args, ws, img_equiv)
+    e2e = None if args.no_e2e else run_e2e(plans, masks_h, args, ws, img_equiv)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -371,15 +373,22 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--only", type=int, default=0,
+                    help="restrict to one clip size (profiling cases)")
+    ap.add_argument("--clips", type=int, default=0, help="clip count for --only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.only:
+        n = args.clips or dict(CLASSES).get(args.only, 16)
+        CLASSES[:] = [(args.only, n)]
     if args.impl == "reference":
         run_reference(args)
     else:

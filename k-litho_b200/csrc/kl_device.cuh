@@ -101,6 +101,16 @@ struct TwTable {
 // e^{+2*pi*i*k/128}; other power-of-two lengths use a stride
 __constant__ const TwTable c_tw = TwTable();
 
+// the same table in global memory, for lane-dependent indices (the constant
+// cache serialises divergent addresses)
+__device__ const TwTable g_twd = TwTable();
+
+// e^{+2*pi*i*num/den} for den a power of two dividing 128
+__device__ __forceinline__ float2 expi2pi_pow2(int num, int den) {
+  const int idx = (num & (den - 1)) * (kTwN / den);
+  return make_float2(g_twd.c[idx], g_twd.s[idx]);
+}
+
 // e^{SIGN*2*pi*i*k/N}, k and N compile-time after unrolling
 template <int N, int SIGN>
 __device__ __forceinline__ float2 tw_const(int k) {
@@ -120,6 +130,26 @@ __host__ __device__ constexpr int brevc(int v, int bits) {
 // In-register radix-2 DIT FFT of length N (natural order in and out).
 // X[k] = sum_n x[n] e^{SIGN 2 pi i k n / N}, unnormalised.
 // ---------------------------------------------------------------------------
+// one radix-2 stage of butterfly span LEN, then the next (compile-time recursion
+// keeps every register index a constant expression)
+template <int N, int SIGN, int LEN>
+__device__ __forceinline__ void fft_stages(float2 (&a)[N]) {
+  if constexpr (LEN <= N) {
+#pragma unroll
+    for (int i = 0; i < N; i += LEN) {
+#pragma unroll
+      for (int k = 0; k < LEN / 2; ++k) {
+        float2 u = a[i + k];
+        float2 v = a[i + k + LEN / 2];
+        if (k != 0) v = cmul(v, tw_const<N, SIGN>(k * (N / LEN)));
+        a[i + k] = cadd(u, v);
+        a[i + k + LEN / 2] = csub(u, v);
+      }
+    }
+    fft_stages<N, SIGN, LEN * 2>(a);
+  }
+}
+
 template <int N, int SIGN>
 __device__ __forceinline__ void fft_reg(float2 (&a)[N]) {
   constexpr int B = ilog2c(N);
@@ -132,20 +162,7 @@ __device__ __forceinline__ void fft_reg(float2 (&a)[N]) {
       a[j] = t;
     }
   }
-#pragma unroll
-  for (int len = 2; len <= N; len <<= 1) {
-#pragma unroll
-    for (int i = 0; i < N; i += len) {
-#pragma unroll
-      for (int k = 0; k < len / 2; ++k) {
-        float2 u = a[i + k];
-        float2 v = a[i + k + len / 2];
-        if (k != 0) v = cmul(v, tw_const<N, SIGN>(k * (N / len)));
-        a[i + k] = cadd(u, v);
-        a[i + k + len / 2] = csub(u, v);
-      }
-    }
-  }
+  fft_stages<N, SIGN, 2>(a);
 }
 
 // Real-input DFT of length P (P even, P/2 <= 64): out[k] for k in [0, P/2],
@@ -205,13 +222,13 @@ struct WarpFFT {
   __device__ __forceinline__ void init(int lane) {
 #pragma unroll
     for (int q = 0; q < R; ++q) {
-      float2 e = expi2pi_frac((long long)q * lane, 32LL * R);
+      float2 e = expi2pi_pow2(q * lane, 32 * R);
       tw4[q] = make_float2(e.x, SIGN > 0 ? e.y : -e.y);
     }
 #pragma unroll
     for (int s = 0; s < 5; ++s) {
       int h = 16 >> s;
-      float2 e = expi2pi_frac(lane & (h - 1), 2LL * h);
+      float2 e = expi2pi_pow2(lane & (h - 1), 2 * h);
       tws[s] = make_float2(e.x, SIGN > 0 ? e.y : -e.y);
     }
   }

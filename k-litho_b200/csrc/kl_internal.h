@@ -46,22 +46,34 @@ struct SocsGeom {
   int G;           // spectral grid (power of two >= max(32, 4Nx+1, 4Ny+1))
   int dx, dy;      // one-pixel output shift of odd periods (0 or 1)
   int NFM, NBM;    // padded forward / inverse bin counts (16, 32 or 64)
+  int KX;          // rows of the x twiddle table, max(NFM, NBM)
 };
+
+// Largest number of kernel slices the spectral stage splits a (clip, set) into.
+constexpr int kSocsMaxSplit = 8;
 
 // Fill geometry; returns KL_OK or KL_ERR_UNSUPPORTED with a message.
 int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g);
 
-// Device workspace bytes needed for `nclips` clips and `nsets` kernel sets.
+// Device workspace sizes.
 size_t socs_partial_bytes(const SocsGeom& g, int nclips);
-size_t socs_spectrum_bytes(const SocsGeom& g, int nclips, int nsets);
+size_t socs_spectrum_bytes(const SocsGeom& g, int nclips, int nsets, int nsplit);
+size_t socs_table_x_elems(const SocsGeom& g);  // float2 elements of tx
+size_t socs_table_y_elems(const SocsGeom& g);  // float2 elements of ty
+// kernel slices per (clip, set) for a launch of `nclips` clips
+int socs_choose_split(const SocsGeom& g, int nclips, int nsets, int K);
+
+// Plan-time twiddle tables (stream-ordered).
+int socs_build_tables(const SocsGeom& g, float2* tx, float2* ty, cudaStream_t st);
 
 // Launchers (stream-ordered).  Buffers are device pointers.
-int socs_launch_forward(const SocsGeom& g, const float* masks, int nclips, float2* partial,
-                        cudaStream_t st);
+int socs_launch_forward(const SocsGeom& g, const float2* tx, const float2* ty, const float* masks,
+                        int nclips, float2* partial, cudaStream_t st);
 int socs_launch_spectral(const SocsGeom& g, const float2* partial, int nclips, const float2* H,
-                         const float* lam, int K, int nsets, float2* T, cudaStream_t st);
-int socs_launch_inverse(const SocsGeom& g, const float2* T, int nclips, int nsets, float* images,
-                        cudaStream_t st);
+                         const float* lam, int K, int nsets, int nsplit, float2* T,
+                         cudaStream_t st);
+int socs_launch_inverse(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T,
+                        int nclips, int nsets, int nsplit, float* images, cudaStream_t st);
 // centred band of FT_r2c (DC at the band centre), complex64 nby x nbx per clip
 int socs_launch_band(const SocsGeom& g, const float2* partial, int nclips, float2* band,
                      cudaStream_t st);

@@ -15,7 +15,9 @@ struct kl_socs_plan_s {
   float2* H = nullptr;       // nsets x K x nby x nbx
   float* lam = nullptr;      // nsets x K
   float2* partial = nullptr; // max_clips strip partials
-  float2* T = nullptr;       // max_clips x nsets intensity spectra
+  float2* T = nullptr;       // intensity spectra (clip x set x kernel slice)
+  float2* tx = nullptr;      // plan-time twiddle tables
+  float2* ty = nullptr;
   float* stage_in = nullptr; // host-entry staging (lazily allocated)
   float* stage_out = nullptr;
   size_t stage_clips = 0;
@@ -38,6 +40,8 @@ void free_plan(kl_socs_plan p) {
   cudaFree(p->lam);
   cudaFree(p->partial);
   cudaFree(p->T);
+  cudaFree(p->tx);
+  cudaFree(p->ty);
   cudaFree(p->stage_in);
   cudaFree(p->stage_out);
   delete p;
@@ -65,12 +69,15 @@ int mark(kl_socs_plan p, cudaStream_t st) {
 int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st) {
   int rc;
   if ((rc = mark(p, st))) return rc;
-  if ((rc = kl::socs_launch_forward(p->g, masks, nclips, p->partial, st))) return rc;
+  const int nsplit = kl::socs_choose_split(p->g, nclips, p->nsets, p->K);
+  if ((rc = kl::socs_launch_forward(p->g, p->tx, p->ty, masks, nclips, p->partial, st))) return rc;
   if ((rc = mark(p, st))) return rc;
-  rc = kl::socs_launch_spectral(p->g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, p->T, st);
+  rc = kl::socs_launch_spectral(p->g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, nsplit,
+                                p->T, st);
   if (rc) return rc;
   if ((rc = mark(p, st))) return rc;
-  if ((rc = kl::socs_launch_inverse(p->g, p->T, nclips, p->nsets, images, st))) return rc;
+  rc = kl::socs_launch_inverse(p->g, p->tx, p->ty, p->T, nclips, p->nsets, nsplit, images, st);
+  if (rc) return rc;
   return mark(p, st);
 }
 }  // namespace
@@ -99,9 +106,26 @@ int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int 
   if ((rc = alloc((void**)&p->H, sizeof(float2) * nb2 * nk * nsets, "kernels")) ||
       (rc = alloc((void**)&p->lam, sizeof(float) * (size_t)nk * nsets, "eigenvalues")) ||
       (rc = alloc((void**)&p->partial, kl::socs_partial_bytes(g, max_clips), "partials")) ||
-      (rc = alloc((void**)&p->T, kl::socs_spectrum_bytes(g, max_clips, nsets), "spectra"))) {
+      (rc = alloc((void**)&p->tx, sizeof(float2) * kl::socs_table_x_elems(g), "x twiddles")) ||
+      (rc = alloc((void**)&p->ty, sizeof(float2) * kl::socs_table_y_elems(g), "y twiddles"))) {
     free_plan(p);
     return rc;
+  }
+  // spectra buffer: the largest clips x slices product any batch size needs
+  int tcap = 0;
+  for (int n = 1; n <= max_clips; ++n) {
+    const int c = n * kl::socs_choose_split(g, n, nsets, nk);
+    tcap = c > tcap ? c : tcap;
+  }
+  if ((rc = alloc((void**)&p->T, kl::socs_spectrum_bytes(g, tcap, nsets, 1), "spectra")) ||
+      (rc = kl::socs_build_tables(g, p->tx, p->ty, nullptr))) {
+    free_plan(p);
+    return rc;
+  }
+  if (cudaStreamSynchronize(nullptr) != cudaSuccess) {
+    kl::set_error(std::string("kl_socs_plan_create: ") + cudaGetErrorString(cudaGetLastError()));
+    free_plan(p);
+    return KL_ERR_CUDA;
   }
   cudaMemset(p->H, 0, sizeof(float2) * nb2 * nk * nsets);
   cudaMemset(p->lam, 0, sizeof(float) * (size_t)nk * nsets);
@@ -191,7 +215,7 @@ int kl_mask_spectrum(kl_socs_plan p, const float* masks, int nclips, float* band
   KL_CHECK_ARG(p && masks && band, "kl_mask_spectrum: NULL argument");
   KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_mask_spectrum: nclips exceeds the plan");
   cudaStream_t st = (cudaStream_t)stream;
-  int rc = kl::socs_launch_forward(p->g, masks, nclips, p->partial, st);
+  int rc = kl::socs_launch_forward(p->g, p->tx, p->ty, masks, nclips, p->partial, st);
   if (rc) return rc;
   return kl::socs_launch_band(p->g, p->partial, nclips, reinterpret_cast<float2*>(band), st);
 }

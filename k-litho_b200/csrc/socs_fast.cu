@@ -15,21 +15,22 @@
 //     bins.  The strip's J rows then go through a J-point warp FFT along y
 //     (rows are J-periodic in the strip), giving the strip's partial band
 //     spectrum D_s[fy][fx], |fy| <= Ny.
-//  2. k_socs_spectral (on-chip; one CTA per clip and kernel set)
+//  2. k_socs_spectral (on-chip; CTAs per clip, kernel set and kernel slice)
 //     Sums the strip partials into the band spectrum, then for each kernel
-//     forms H_k . M, runs a pruned 2-D inverse FFT on a G x G grid
-//     (G >= 4N+1, so |E_k|^2 is sampled without aliasing) with warp FFTs in
-//     shared memory and accumulates lambda_k |E_k|^2 in registers.  A
-//     forward 2-D FFT of that intensity gives its exact band-limited
-//     spectrum T[a][b], |a| <= 2Ny, 0 <= b <= 2Nx.
+//     of its slice forms H_k . M, runs a pruned 2-D inverse FFT on a G x G
+//     grid (G >= 4N+1, so |E_k|^2 is sampled without aliasing) with warp FFTs
+//     in shared memory and accumulates lambda_k |E_k|^2 in registers.  A
+//     forward 2-D FFT of that intensity gives the slice's share of the exact
+//     band-limited intensity spectrum T[a][b], |a| <= 2Ny, 0 <= b <= 2Nx.
 //  3. k_socs_inverse  (HBM-bound; writes the image once)
-//     One CTA per (image, strip).  Rows of the strip come from T by a
-//     J-point warp FFT along y; each warp then synthesises a row of Lx real
-//     pixels from its 2Nx+1 bins with a real-output length-P inverse DFT per
-//     lane.
+//     One CTA per (image, strip).  Sums the slices of T, forms the strip's
+//     rows by a J-point warp FFT along y, and each warp synthesises a row of
+//     Lx real pixels from its 2Nx+1 bins with a real-output length-P inverse
+//     DFT per lane.
 //
-// Only the strip partials (Ly/J x (2Ny+1) x (Nx+1) complex per clip) and T
-// ((4Ny+1) x (2Nx+1) complex per image) pass through global memory.
+// Twiddle factors that depend on the clip size are made once per plan
+// (k_socs_tables, exact double-precision arguments) and read from L2.
+// Only the strip partials, T and the tables pass through global memory.
 #include <climits>
 
 #include "kl_device.cuh"
@@ -74,6 +75,11 @@ int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g) {
     return KL_ERR_UNSUPPORTED;
   }
   r.V = Lx / r.P;
+  if (r.V != 32 && r.V != 64 && r.V != 96) {
+    set_error("fast SOCS path supports Lx in {256, 512, 768, 1024, 1536, 2048, 3072} (got " +
+              std::to_string(Lx) + ")");
+    return KL_ERR_UNSUPPORTED;
+  }
   if (r.nf <= 16)
     r.NFM = 16;
   else if (r.nf <= 32)
@@ -83,6 +89,7 @@ int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g) {
     return KL_ERR_UNSUPPORTED;
   }
   r.NBM = r.ntx <= 32 ? 32 : 64;
+  r.KX = r.NBM > r.NFM ? r.NBM : r.NFM;
   r.J = pow2_at_least(r.nby);
   if (r.J < 32) r.J = 32;
   if (r.J > 64 || Ly % r.J != 0) {
@@ -112,50 +119,88 @@ int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g) {
 size_t socs_partial_bytes(const SocsGeom& g, int nclips) {
   return sizeof(float2) * (size_t)nclips * g.nS * g.nby * g.nf;
 }
-size_t socs_spectrum_bytes(const SocsGeom& g, int nclips, int nsets) {
-  return sizeof(float2) * (size_t)nclips * nsets * g.nty * g.ntx;
+size_t socs_spectrum_bytes(const SocsGeom& g, int nclips, int nsets, int nsplit) {
+  return sizeof(float2) * (size_t)nclips * nsets * nsplit * g.nty * g.ntx;
+}
+size_t socs_table_x_elems(const SocsGeom& g) { return (size_t)g.KX * g.V; }
+size_t socs_table_y_elems(const SocsGeom& g) { return (size_t)g.nS * g.nty; }
+
+int socs_choose_split(const SocsGeom& g, int nclips, int nsets, int K) {
+  // enough CTAs to cover the GPU about twice; slices of at least 3 kernels
+  const int ctas = nclips * nsets;
+  int ns = 1;
+  while (ns < kSocsMaxSplit && ctas * ns < 2 * 148 && K / (2 * ns) >= 3) ns *= 2;
+  (void)g;
+  return ns;
+}
+
+// ---------------------------------------------------------------------------
+// plan-time tables: tx[k][l'] = e^{-2 pi i k l'/Lx}, ty[s][a+2Ny] = e^{+2 pi i a s/Ly}
+// ---------------------------------------------------------------------------
+__global__ void k_socs_tables(const SocsGeom g, float2* __restrict__ tx, float2* __restrict__ ty) {
+  const int nx = g.KX * g.V, ny = g.nS * g.nty;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nx + ny; i += gridDim.x * blockDim.x) {
+    if (i < nx) {
+      const int k = i / g.V, lp = i - k * g.V;
+      tx[i] = expi2pi_frac(-(long long)k * lp, g.Lx);
+    } else {
+      const int j = i - nx, s = j / g.nty, a = j - s * g.nty - 2 * g.Ny;
+      ty[j] = expi2pi_frac((long long)a * s, g.Ly);
+    }
+  }
+}
+
+int socs_build_tables(const SocsGeom& g, float2* tx, float2* ty, cudaStream_t st) {
+  const int n = (int)(socs_table_x_elems(g) + socs_table_y_elems(g));
+  k_socs_tables<<<(n + 255) / 256, 256, 0, st>>>(g, tx, ty);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_error(std::string("k_socs_tables: ") + cudaGetErrorString(e));
+    return KL_ERR_CUDA;
+  }
+  return KL_OK;
 }
 
 // ---------------------------------------------------------------------------
 // 1. forward: mask rows -> per-strip partial band spectra
 // ---------------------------------------------------------------------------
-template <int P, int NFM, int RJ>
+template <int P, int V, int NFM, int RJ>
 __global__ void __launch_bounds__(kThreads) k_socs_forward(const float* __restrict__ masks,
                                                            const SocsGeom g,
+                                                           const float2* __restrict__ tx,
+                                                           const float2* __restrict__ ty,
                                                            float2* __restrict__ partial) {
+  constexpr int J = 32 * RJ;
   extern __shared__ float4 smem4[];
   float2* twf = reinterpret_cast<float2*>(smem4);  // [NFM][V]   e^{-2 pi i fx l'/Lx}
-  float2* rowbuf = twf + NFM * g.V;                // [J][NFM]   row bins of the strip
+  float2* rowbuf = twf + NFM * V;                  // [J][NFM]   row bins of the strip
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int s = blockIdx.x, clip = blockIdx.y;
   const float* mask = masks + (size_t)clip * g.Lx * g.Ly;
 
-  for (int i = threadIdx.x; i < NFM * g.V; i += kThreads) {
-    int fx = i / g.V, lp = i - fx * g.V;
-    twf[i] = expi2pi_frac(-(long long)fx * lp, g.Lx);
-  }
+  for (int i = threadIdx.x; i < NFM * V; i += kThreads) twf[i] = __ldg(tx + i);
   __syncthreads();
 
-  const int nv = g.V / 32;
-  for (int jj = warp; jj < g.J; jj += kWarps) {
-    const float* row = mask + (size_t)(s + g.nS * jj) * g.Lx;
+  for (int jj = warp; jj < J; jj += kWarps) {
+    const float* row = mask + (size_t)(s + g.nS * jj) * (V * P);
     float acc[2 * NFM];
 #pragma unroll
     for (int i = 0; i < 2 * NFM; ++i) acc[i] = 0.f;
-    for (int c = 0; c < nv; ++c) {
+#pragma unroll 1
+    for (int c = 0; c < V / 32; ++c) {
       const int lp = lane + 32 * c;
       float val[P];
 #pragma unroll
-      for (int i = 0; i < P; ++i) val[i] = __ldg(row + lp + g.V * i);
+      for (int i = 0; i < P; ++i) val[i] = __ldcs(row + lp + V * i);
       float2 S[P / 2 + 1];
       rdft_reg<P>(val, S);
 #pragma unroll
       for (int fx = 0; fx < NFM; ++fx) {
         const int k = fx % P;
         const float2 sv = (k <= P / 2) ? S[k] : cconj(S[P - k]);
-        const float2 r = cmul(sv, twf[fx * g.V + lp]);
-        acc[2 * fx] += r.x;
-        acc[2 * fx + 1] += r.y;
+        const float2 w = twf[fx * V + lp];
+        acc[2 * fx] = fmaf(sv.x, w.x, fmaf(-sv.y, w.y, acc[2 * fx]));
+        acc[2 * fx + 1] = fmaf(sv.x, w.y, fmaf(sv.y, w.x, acc[2 * fx + 1]));
       }
     }
     warp_reduce_scatter<2 * NFM>(acc, lane);
@@ -170,6 +215,7 @@ __global__ void __launch_bounds__(kThreads) k_socs_forward(const float* __restri
   WarpFFT<RJ, -1> wf;
   wf.init(lane);
   const int br = (int)(__brev((unsigned)lane) >> 27);
+  const float2* tys = ty + (size_t)s * g.nty + 2 * g.Ny;  // e^{+2 pi i a s/Ly} at [a]
   for (int fx = warp; fx < g.nf; fx += kWarps) {
     float2 vv[RJ];
 #pragma unroll
@@ -178,11 +224,10 @@ __global__ void __launch_bounds__(kThreads) k_socs_forward(const float* __restri
 #pragma unroll
     for (int q1 = 0; q1 < RJ; ++q1) {
       const int bin = q1 + RJ * br;
-      const int fy = bin <= g.J / 2 ? bin : bin - g.J;
-      if (fy >= -g.Ny && fy <= g.Ny) {
-        const float2 ph = expi2pi_frac(-(long long)fy * s, g.Ly);
-        partial[(((size_t)clip * g.nS + s) * g.nby + (fy + g.Ny)) * g.nf + fx] = cmul(vv[q1], ph);
-      }
+      const int fy = bin <= J / 2 ? bin : bin - J;
+      if (fy >= -g.Ny && fy <= g.Ny)
+        partial[(((size_t)clip * g.nS + s) * g.nby + (fy + g.Ny)) * g.nf + fx] =
+            cmulc(vv[q1], __ldg(tys + fy));
     }
   }
 }
@@ -198,7 +243,7 @@ __device__ __forceinline__ void load_band(const float2* __restrict__ partial, co
   for (int i = threadIdx.x; i < g.nby * g.nf; i += blockDim.x) {
     const int r = i / g.nf, fx = i - r * g.nf;
     float2 sum = make_float2(0.f, 0.f);
-    for (int s = 0; s < g.nS; ++s) sum = cadd(sum, p0[(size_t)s * per + i]);
+    for (int s = 0; s < g.nS; ++s) sum = cadd(sum, __ldg(p0 + (size_t)s * per + i));
     sum = cscale(sum, inv);
     Cm[r * g.nbx + g.Nx + fx] = sum;
     if (fx > 0) Cm[(2 * g.Ny - r) * g.nbx + g.Nx - fx] = cconj(sum);
@@ -213,15 +258,18 @@ __global__ void __launch_bounds__(kThreads) k_socs_spectral(const float2* __rest
                                                             float2* __restrict__ Tout) {
   constexpr int G = 32 * RG;
   constexpr int GP = G + 1;  // padded row pitch (bank-conflict free columns)
+  constexpr int CW = G / kWarps;  // columns owned by each warp
   extern __shared__ float4 smem4[];
   float2* Cm = reinterpret_cast<float2*>(smem4);  // [nby][nbx] band spectrum / (Lx Ly)
   float2* E1 = Cm + g.nby * g.nbx;                // [nby][GP] stage-1 rows; later T1 [G][ntx]
   const int e1n = g.nby * GP > G * g.ntx ? g.nby * GP : G * g.ntx;
   float* Is = reinterpret_cast<float*>(E1 + e1n);  // [G][GP] intensity
-  float2* Zs = reinterpret_cast<float2*>(Is + G * GP + (G * GP & 1));  // [warps][G]
+  float2* Zs = reinterpret_cast<float2*>(Is + G * GP);  // [warps][G]
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int clip = blockIdx.x, set = blockIdx.y, nsets = gridDim.y;
+  const int clip = blockIdx.x, set = blockIdx.y, split = blockIdx.z;
+  const int nsets = gridDim.y, nsplit = gridDim.z;
+  const int k0 = (int)(((long long)K * split) / nsplit), k1 = (int)(((long long)K * (split + 1)) / nsplit);
   const int br = (int)(__brev((unsigned)lane) >> 27);
 
   load_band(partial, g, clip, Cm);
@@ -229,38 +277,49 @@ __global__ void __launch_bounds__(kThreads) k_socs_spectral(const float2* __rest
 
   WarpFFT<RG, +1> wi;
   wi.init(lane);
-  float acc[G / kWarps][RG];
+  float acc[CW][RG];
 #pragma unroll
-  for (int t = 0; t < G / kWarps; ++t)
+  for (int t = 0; t < CW; ++t)
 #pragma unroll
     for (int q = 0; q < RG; ++q) acc[t][q] = 0.f;
 
   const size_t nb2 = (size_t)g.nby * g.nbx;
   const float2* Hs = H + (size_t)set * K * nb2;
-  for (int k = 0; k < K; ++k) {
+  for (int k = k0; k < k1; ++k) {
     const float2* Hk = Hs + (size_t)k * nb2;
     const float lk = __ldg(lam + set * K + k);
-    // stage 1: rows fy, inverse FFT along x of H_k . M
-    for (int r = warp; r < g.nby; r += kWarps) {
-      float2 vv[RG];
+    // stage 1: rows fy, inverse FFT along x of H_k . M (two rows per pass)
+    for (int r0 = warp; r0 < g.nby; r0 += 2 * kWarps) {
+      float2 va[RG], vb[RG];
+      const int r1 = r0 + kWarps;
+      const bool has1 = r1 < g.nby;
 #pragma unroll
       for (int j = 0; j < RG; ++j) {
         const int n = lane + 32 * j;
         const int fx = n <= g.Nx ? n : (n >= G - g.Nx ? n - G : INT_MIN);
-        vv[j] = make_float2(0.f, 0.f);
+        va[j] = make_float2(0.f, 0.f);
+        vb[j] = make_float2(0.f, 0.f);
         if (fx != INT_MIN) {
-          const int o = r * g.nbx + fx + g.Nx;
-          vv[j] = cmul(__ldg(Hk + o), Cm[o]);
+          const int o0 = r0 * g.nbx + fx + g.Nx;
+          va[j] = cmul(__ldg(Hk + o0), Cm[o0]);
+          if (has1) {
+            const int o1 = r1 * g.nbx + fx + g.Nx;
+            vb[j] = cmul(__ldg(Hk + o1), Cm[o1]);
+          }
         }
       }
-      wi.run(vv, lane);
+      wi.run(va, lane);
+      wi.run(vb, lane);
 #pragma unroll
-      for (int q1 = 0; q1 < RG; ++q1) E1[r * GP + q1 + RG * br] = vv[q1];
+      for (int q1 = 0; q1 < RG; ++q1) {
+        E1[r0 * GP + q1 + RG * br] = va[q1];
+        if (has1) E1[r1 * GP + q1 + RG * br] = vb[q1];
+      }
     }
     __syncthreads();
     // stage 2: columns q, inverse FFT along y; accumulate lambda |E|^2
 #pragma unroll
-    for (int t = 0; t < G / kWarps; ++t) {
+    for (int t = 0; t < CW; ++t) {
       const int q = warp + kWarps * t;
       float2 vv[RG];
 #pragma unroll
@@ -278,7 +337,7 @@ __global__ void __launch_bounds__(kThreads) k_socs_spectral(const float2* __rest
 
   // intensity to shared memory: I[p][q], p = q1 + RG*brev(lane), q = warp + 8t
 #pragma unroll
-  for (int t = 0; t < G / kWarps; ++t)
+  for (int t = 0; t < CW; ++t)
 #pragma unroll
     for (int q1 = 0; q1 < RG; ++q1) Is[(q1 + RG * br) * GP + warp + kWarps * t] = acc[t][q1];
   __syncthreads();
@@ -314,7 +373,7 @@ __global__ void __launch_bounds__(kThreads) k_socs_spectral(const float2* __rest
 
   // stage B: forward FFT along y of each kept column b; scale and shift phase
   const float invg = 1.0f / ((float)G * (float)G);
-  float2* To = Tout + ((size_t)clip * nsets + set) * g.nty * g.ntx;
+  float2* To = Tout + (((size_t)clip * nsets + set) * nsplit + split) * g.nty * g.ntx;
   for (int b = warp; b < g.ntx; b += kWarps) {
     float2 vv[RG];
 #pragma unroll
@@ -341,27 +400,33 @@ __global__ void __launch_bounds__(kThreads) k_socs_spectral(const float2* __rest
 // ---------------------------------------------------------------------------
 // 3. inverse: intensity spectrum -> image rows
 // ---------------------------------------------------------------------------
-template <int P, int NBM, int RJ>
+template <int P, int V, int NBM, int RJ>
 __global__ void __launch_bounds__(kThreads) k_socs_inverse(const float2* __restrict__ T,
                                                            const SocsGeom g,
+                                                           const float2* __restrict__ tx,
+                                                           const float2* __restrict__ ty,
+                                                           int nsplit,
                                                            float* __restrict__ images) {
+  constexpr int J = 32 * RJ;
   constexpr int QP = NBM + 1;
   extern __shared__ float4 smem4[];
-  float2* twi = reinterpret_cast<float2*>(smem4);  // [NBM][V]  e^{+2 pi i b l'/Lx}
-  float2* Qs = twi + NBM * g.V;                     // [J][QP]   row coefficients
-  float2* Ts = Qs + g.J * QP;                       // [nty][ntx]
+  float2* twi = reinterpret_cast<float2*>(smem4);  // [NBM][V]  e^{-2 pi i b l'/Lx} (conj used)
+  float2* Qs = twi + NBM * V;                       // [J][QP]   row coefficients
+  float2* Ts = Qs + J * QP;                         // [nty][ntx]
   float2* ph = Ts + g.nty * g.ntx;                  // [nty]     e^{2 pi i a s / Ly}
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int s = blockIdx.x, img = blockIdx.y;
-  const float2* Ti = T + (size_t)img * g.nty * g.ntx;
+  const size_t tsz = (size_t)g.nty * g.ntx;
+  const float2* Ti = T + (size_t)img * nsplit * tsz;
 
-  for (int i = threadIdx.x; i < g.nty * g.ntx; i += kThreads) Ts[i] = __ldg(Ti + i);
-  for (int i = threadIdx.x; i < NBM * g.V; i += kThreads) {
-    int b = i / g.V, lp = i - b * g.V;
-    twi[i] = expi2pi_frac((long long)b * lp, g.Lx);
+  for (int i = threadIdx.x; i < (int)tsz; i += kThreads) {
+    float2 v = __ldg(Ti + i);
+    for (int p = 1; p < nsplit; ++p) v = cadd(v, __ldg(Ti + p * tsz + i));
+    Ts[i] = v;
   }
-  for (int i = threadIdx.x; i < g.nty; i += kThreads) ph[i] = expi2pi_frac((long long)(i - 2 * g.Ny) * s, g.Ly);
-  for (int i = threadIdx.x; i < g.J * QP; i += kThreads) Qs[i] = make_float2(0.f, 0.f);
+  for (int i = threadIdx.x; i < NBM * V; i += kThreads) twi[i] = __ldg(tx + i);
+  for (int i = threadIdx.x; i < g.nty; i += kThreads) ph[i] = __ldg(ty + (size_t)s * g.nty + i);
+  for (int i = threadIdx.x; i < J * QP; i += kThreads) Qs[i] = make_float2(0.f, 0.f);
   __syncthreads();
 
   // rows of the strip: Q[y = s + nS j][b] = sum_a T[a][b] e^{2 pi i a y / Ly}
@@ -375,7 +440,7 @@ __global__ void __launch_bounds__(kThreads) k_socs_inverse(const float2* __restr
     for (int j = 0; j < RJ; ++j) {
       const int n = lane + 32 * j;
       float2 f = make_float2(0.f, 0.f);
-      for (int a = n - g.J * ((n + A) / g.J); a <= A; a += g.J)
+      for (int a = n - J * ((n + A) / J); a <= A; a += J)
         f = cfma(Ts[(a + A) * g.ntx + b], ph[a + A], f);
       vv[j] = f;
     }
@@ -387,21 +452,27 @@ __global__ void __launch_bounds__(kThreads) k_socs_inverse(const float2* __restr
   __syncthreads();
 
   float* out = images + (size_t)img * g.Lx * g.Ly;
-  const int nv = g.V / 32;
-  for (int jj = warp; jj < g.J; jj += kWarps) {
-    float* row = out + (size_t)(s + g.nS * jj) * g.Lx;
+  for (int jj = warp; jj < J; jj += kWarps) {
+    float* row = out + (size_t)(s + g.nS * jj) * (V * P);
     const float2* q = Qs + jj * QP;
-    for (int c = 0; c < nv; ++c) {
+#pragma unroll 1
+    for (int c = 0; c < V / 32; ++c) {
       const int lp = lane + 32 * c;
       float2 Z[P];
 #pragma unroll
       for (int i = 0; i < P; ++i) Z[i] = make_float2(0.f, 0.f);
 #pragma unroll
-      for (int b = 0; b < NBM; ++b) Z[b % P] = cfma(q[b], twi[b * g.V + lp], Z[b % P]);
+      for (int b = 0; b < NBM; ++b) {
+        // Z += q[b] * conj(tw)
+        const float2 qb = q[b], w = twi[b * V + lp];
+        const int k = b % P;
+        Z[k] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Z[k].x)),
+                           fmaf(qb.y, w.x, fmaf(-qb.x, w.y, Z[k].y)));
+      }
       float o[P];
       re_idft_reg<P>(Z, o);
 #pragma unroll
-      for (int i = 0; i < P; ++i) row[lp + g.V * i] = o[i];
+      for (int i = 0; i < P; ++i) row[lp + V * i] = o[i];
     }
   }
 }
@@ -449,78 +520,87 @@ int check_launch(const char* what) {
   return KL_OK;
 }
 
-template <int P, int NFM, int RJ>
-int launch_fwd(const SocsGeom& g, const float* masks, int nclips, float2* partial, cudaStream_t st) {
-  size_t sm = sizeof(float2) * ((size_t)NFM * g.V + (size_t)g.J * NFM);
-  auto kern = k_socs_forward<P, NFM, RJ>;
+template <int P, int V, int NFM, int RJ>
+int launch_fwd(const SocsGeom& g, const float2* tx, const float2* ty, const float* masks,
+               int nclips, float2* partial, cudaStream_t st) {
+  size_t sm = sizeof(float2) * ((size_t)NFM * V + (size_t)32 * RJ * NFM);
+  auto kern = k_socs_forward<P, V, NFM, RJ>;
   int rc = set_smem(kern, sm);
   if (rc) return rc;
-  kern<<<dim3(g.nS, nclips), kThreads, sm, st>>>(masks, g, partial);
+  kern<<<dim3(g.nS, nclips), kThreads, sm, st>>>(masks, g, tx, ty, partial);
   return check_launch("k_socs_forward");
 }
 
-template <int P, int NBM, int RJ>
-int launch_inv(const SocsGeom& g, const float2* T, int nimg, float* images, cudaStream_t st) {
-  size_t sm = sizeof(float2) * ((size_t)NBM * g.V + (size_t)g.J * (NBM + 1) +
+template <int P, int V, int NBM, int RJ>
+int launch_inv(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T, int nimg,
+               int nsplit, float* images, cudaStream_t st) {
+  size_t sm = sizeof(float2) * ((size_t)NBM * V + (size_t)32 * RJ * (NBM + 1) +
                                 (size_t)g.nty * g.ntx + g.nty);
-  auto kern = k_socs_inverse<P, NBM, RJ>;
+  auto kern = k_socs_inverse<P, V, NBM, RJ>;
   int rc = set_smem(kern, sm);
   if (rc) return rc;
-  kern<<<dim3(g.nS, nimg), kThreads, sm, st>>>(T, g, images);
+  kern<<<dim3(g.nS, nimg), kThreads, sm, st>>>(T, g, tx, ty, nsplit, images);
   return check_launch("k_socs_inverse");
 }
 
 template <int RG>
 int launch_spec(const SocsGeom& g, const float2* partial, int nclips, const float2* H,
-                const float* lam, int K, int nsets, float2* T, cudaStream_t st) {
+                const float* lam, int K, int nsets, int nsplit, float2* T, cudaStream_t st) {
   constexpr int G = 32 * RG, GP = G + 1;
   size_t e1n = (size_t)g.nby * GP > (size_t)G * g.ntx ? (size_t)g.nby * GP : (size_t)G * g.ntx;
-  size_t isn = (size_t)G * GP + ((G * GP) & 1);
-  size_t sm = sizeof(float2) * ((size_t)g.nby * g.nbx + e1n) + sizeof(float) * isn +
+  size_t sm = sizeof(float2) * ((size_t)g.nby * g.nbx + e1n) + sizeof(float) * (size_t)G * GP +
               sizeof(float2) * (size_t)kWarps * G;
   auto kern = k_socs_spectral<RG>;
   int rc = set_smem(kern, sm);
   if (rc) return rc;
-  kern<<<dim3(nclips, nsets), kThreads, sm, st>>>(partial, g, H, lam, K, T);
+  kern<<<dim3(nclips, nsets, nsplit), kThreads, sm, st>>>(partial, g, H, lam, K, T);
   return check_launch("k_socs_spectral");
 }
 }  // namespace
 
-int socs_launch_forward(const SocsGeom& g, const float* masks, int nclips, float2* partial,
-                        cudaStream_t st) {
+#define KL_PV_LIST(X, A, B) \
+  X(8, 32, A, B) X(8, 96, A, B) X(16, 32, A, B) X(16, 96, A, B) X(32, 32, A, B) X(32, 64, A, B) X(32, 96, A, B)
+
+int socs_launch_forward(const SocsGeom& g, const float2* tx, const float2* ty, const float* masks,
+                        int nclips, float2* partial, cudaStream_t st) {
   if (nclips <= 0) return KL_OK;
   const int RJ = g.J / 32;
-#define KL_FWD(P_, N_, R_) \
-  if (g.P == P_ && g.NFM == N_ && RJ == R_) return launch_fwd<P_, N_, R_>(g, masks, nclips, partial, st);
-  KL_FWD(32, 16, 1) KL_FWD(32, 16, 2) KL_FWD(32, 32, 1) KL_FWD(32, 32, 2)
-  KL_FWD(16, 16, 1) KL_FWD(16, 16, 2) KL_FWD(16, 32, 1) KL_FWD(16, 32, 2)
-  KL_FWD(8, 16, 1) KL_FWD(8, 16, 2) KL_FWD(8, 32, 1) KL_FWD(8, 32, 2)
+#define KL_FWD(P_, V_, N_, R_)                               \
+  if (g.P == P_ && g.V == V_ && g.NFM == N_ && RJ == R_) \
+    return launch_fwd<P_, V_, N_, R_>(g, tx, ty, masks, nclips, partial, st);
+  KL_PV_LIST(KL_FWD, 16, 1)
+  KL_PV_LIST(KL_FWD, 16, 2)
+  KL_PV_LIST(KL_FWD, 32, 1)
+  KL_PV_LIST(KL_FWD, 32, 2)
 #undef KL_FWD
   set_error("socs_launch_forward: no kernel for this geometry");
   return KL_ERR_UNSUPPORTED;
 }
 
 int socs_launch_spectral(const SocsGeom& g, const float2* partial, int nclips, const float2* H,
-                         const float* lam, int K, int nsets, float2* T, cudaStream_t st) {
+                         const float* lam, int K, int nsets, int nsplit, float2* T,
+                         cudaStream_t st) {
   if (nclips <= 0) return KL_OK;
   switch (g.G) {
-    case 32: return launch_spec<1>(g, partial, nclips, H, lam, K, nsets, T, st);
-    case 64: return launch_spec<2>(g, partial, nclips, H, lam, K, nsets, T, st);
-    case 128: return launch_spec<4>(g, partial, nclips, H, lam, K, nsets, T, st);
+    case 32: return launch_spec<1>(g, partial, nclips, H, lam, K, nsets, nsplit, T, st);
+    case 64: return launch_spec<2>(g, partial, nclips, H, lam, K, nsets, nsplit, T, st);
+    case 128: return launch_spec<4>(g, partial, nclips, H, lam, K, nsets, nsplit, T, st);
   }
   set_error("socs_launch_spectral: unsupported spectral grid");
   return KL_ERR_UNSUPPORTED;
 }
 
-int socs_launch_inverse(const SocsGeom& g, const float2* T, int nclips, int nsets, float* images,
-                        cudaStream_t st) {
+int socs_launch_inverse(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T,
+                        int nclips, int nsets, int nsplit, float* images, cudaStream_t st) {
   if (nclips <= 0) return KL_OK;
   const int RJ = g.J / 32, nimg = nclips * nsets;
-#define KL_INV(P_, N_, R_) \
-  if (g.P == P_ && g.NBM == N_ && RJ == R_) return launch_inv<P_, N_, R_>(g, T, nimg, images, st);
-  KL_INV(32, 32, 1) KL_INV(32, 32, 2) KL_INV(32, 64, 1) KL_INV(32, 64, 2)
-  KL_INV(16, 32, 1) KL_INV(16, 32, 2) KL_INV(16, 64, 1) KL_INV(16, 64, 2)
-  KL_INV(8, 32, 1) KL_INV(8, 32, 2) KL_INV(8, 64, 1) KL_INV(8, 64, 2)
+#define KL_INV(P_, V_, N_, R_)                               \
+  if (g.P == P_ && g.V == V_ && g.NBM == N_ && RJ == R_) \
+    return launch_inv<P_, V_, N_, R_>(g, tx, ty, T, nimg, nsplit, images, st);
+  KL_PV_LIST(KL_INV, 32, 1)
+  KL_PV_LIST(KL_INV, 32, 2)
+  KL_PV_LIST(KL_INV, 64, 1)
+  KL_PV_LIST(KL_INV, 64, 2)
 #undef KL_INV
   set_error("socs_launch_inverse: no kernel for this geometry");
   return KL_ERR_UNSUPPORTED;
