@@ -138,6 +138,61 @@ int kl_socs_stage_times(kl_socs_plan plan, double* ms, int* launches);
 int kl_mask_spectrum(kl_socs_plan plan, const float* masks_dev, int nclips, float* band_dev,
                      void* stream);
 
+/* ------------------------------------------------------------------------- */
+/* TCC assembly, SOCS kernels, Hopkins image: K-Litho-TCC/klitho_tcc.cpp      */
+/* ------------------------------------------------------------------------- */
+
+#define KL_PREC_FAST 0 /* FP32 pupil factor, 3-term BF16 tensor-core TCC, FP64 Rayleigh-Ritz */
+#define KL_PREC_FP64 1 /* plain FP64 GPU path (pupil table from the host libm, FP64 TCC)    */
+
+typedef struct kl_tcc_plan_s* kl_tcc_plan;
+
+/* Optical setting of one TCC: source map (createSource output, host), NA,
+ * defocus in the reference's normalised units (argv[21], dz = defocus *
+ * lambda / NA^2, klitho_tcc.cpp:191), immersion index n_medium (1 reproduces
+ * klitho_tcc.cpp:220; NA > 1 needs n_medium >= NA), period Lx x Ly.
+ * Computes outer sigma and the band (klitho_tcc.cpp:479-486), the source
+ * points (:202-211) and the pupil factor A[f][s] = sqrt(J_s) P(f, s)
+ * (:201-228) on the current device. */
+int kl_tcc_plan_create(kl_tcc_plan* plan, const float* src_host, int srcSize, double NA,
+                       double defocus, double n_medium, int Lx, int Ly, int precision);
+int kl_tcc_plan_destroy(kl_tcc_plan plan);
+/* Band half-widths, TCC size N = (2Nx+1)(2Ny+1), source point count S, sigma_o. */
+int kl_tcc_plan_info(kl_tcc_plan plan, int* Nx, int* Ny, int* N, int* S, float* outerSigma);
+/* Copy the FP32 factor A (N x S c64, row-major) to A_dev (fast path only). */
+int kl_tcc_factor(kl_tcc_plan plan, float* A_dev, void* stream);
+
+/* calcTCC (klitho_tcc.cpp:186-267): the N x N Hermitian TCC, row-major, into
+ * tcc_dev -- c64 on the fast path (tcgen05 tensor cores, BF16x3 split, FP32
+ * accumulate), c128 on the FP64 path.  Synchronous on the fast path (reports
+ * pipeline timeouts). */
+int kl_tcc_build(kl_tcc_plan plan, void* tcc_dev, void* stream);
+/* {max re, min re, max im, min im} of a TCC built by kl_tcc_build (the
+ * "Max. TCC Real/Imag Value" lines of klitho_tcc.cpp:521-528). */
+int kl_tcc_minmax(kl_tcc_plan plan, const void* tcc_dev, double* out4, void* stream);
+/* Build the TCC into library-owned device memory, return its min/max as above
+ * and release it (what klitho_tcc prints; the TCC itself is not an output of
+ * the reference program). */
+int kl_tcc_build_minmax(kl_tcc_plan plan, double* out4);
+
+/* calcKernels (klitho_tcc.cpp:300-377): top-nk eigenpairs of the TCC by
+ * blocked subspace iteration (block `block`, 0 = automatic) with FP64
+ * CholeskyQR2 and Rayleigh-Ritz, in descending order; kernels in the
+ * reference layout krn[k][j] = v_k[N-1-j] as float planes (nk x N each),
+ * scales = eigenvalues as float, evals_host (optional) in double.
+ * Returns KL_ERR_NOT_CONVERGED if the iteration cap is reached. */
+int kl_topk_eig(kl_tcc_plan plan, int nk, int block, float* krn_re_host, float* krn_im_host,
+                float* scales_host, double* evals_host, int* iterations);
+
+/* Hopkins image (calcImage + FT_c2r, klitho_tcc.cpp:269-290, :150-183) of
+ * nclips masks: sum_s J_s |IFFT(P(.,s) conj . M)|^2, the source-point form
+ * of the TCC contraction (identical in exact arithmetic), computed by the
+ * fused SOCS pipeline with the columns of A as kernels.  Fast path only. */
+int kl_hopkins_image(kl_tcc_plan plan, const float* masks_dev, int nclips, float* images_dev,
+                     void* stream);
+/* One Hopkins image from and to host memory (Lx*Ly floats each); synchronous. */
+int kl_hopkins_image_host(kl_tcc_plan plan, const float* mask_host, float* image_host);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,3 +79,9 @@ int socs_launch_band(const SocsGeom& g, const float2* partial, int nclips, float
                      cudaStream_t st);
 
 }  // namespace kl
+
+// Internal: upload kernel set `set` of a SOCS plan from device memory
+// (H_dev: nk x band complex64, lam_dev: nk floats; device-to-device copies).
+extern "C" int kl_socs_set_kernels_device(struct kl_socs_plan_s* plan, int set,
+                                          const float2* H_dev, const float* lam_dev,
+                                          cudaStream_t st);

@@ -152,6 +152,18 @@ int kl_socs_set_kernels(kl_socs_plan p, int set, const float* re, const float* i
   return KL_OK;
 }
 
+int kl_socs_set_kernels_device(kl_socs_plan p, int set, const float2* H_dev, const float* lam_dev,
+                               cudaStream_t st) {
+  KL_CHECK_ARG(p && H_dev && lam_dev, "kl_socs_set_kernels_device: NULL argument");
+  KL_CHECK_ARG(set >= 0 && set < p->nsets, "kl_socs_set_kernels_device: set out of range");
+  const size_t nb2 = (size_t)p->g.nby * p->g.nbx;
+  KL_CUDA_TRY(cudaMemcpyAsync(p->H + (size_t)set * p->K * nb2, H_dev, sizeof(float2) * nb2 * p->K,
+                              cudaMemcpyDeviceToDevice, st));
+  KL_CUDA_TRY(cudaMemcpyAsync(p->lam + (size_t)set * p->K, lam_dev, sizeof(float) * p->K,
+                              cudaMemcpyDeviceToDevice, st));
+  return KL_OK;
+}
+
 int kl_socs_forward(kl_socs_plan p, const float* masks, int nclips, float* images, void* stream) {
   KL_CHECK_ARG(p && masks && images, "kl_socs_forward: NULL argument");
   KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_socs_forward: nclips exceeds the plan");

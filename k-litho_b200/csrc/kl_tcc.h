@@ -1,0 +1,97 @@
+// kl_tcc.h -- internal interfaces of the TCC assembly and eigen-decomposition
+// (K-Litho-TCC/klitho_tcc.cpp:186-267 calcTCC, :300-377 calcKernels).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+namespace kl {
+
+// One active source pixel, in the reference's raster order
+// (klitho_tcc.cpp:202-205), with its shifted-pupil loop bounds (:206-211).
+struct SrcPoint {
+  float sx, sy, J;
+  int nxmin, nxmax, nymin, nymax;
+  int src_id;
+};
+
+// Scalars of the pupil evaluation, computed on the host with the reference's
+// float arithmetic (klitho_tcc.cpp:189-197).
+struct PupilParams {
+  int Nx, Ny, N, S;
+  float Lx_norm, Ly_norm;  // L*NA/lambda
+  float dzk;               // (defocus / (NA^2/lambda)) * (2 pi / lambda), float product
+  float NA;
+  double n_medium2;        // n_medium^2 (1 reproduces the reference)
+};
+
+// Host: enumerate the TCC's source points; fills pp (except N/S sizes derived).
+void tcc_source_points(const float* src, int srcSize, float outerSigma, float lambda, float NA,
+                       float defocus, double n_medium, int Lx, int Ly, int Nx, int Ny,
+                       std::vector<SrcPoint>& pts, PupilParams& pp);
+
+// Host: pupil table P[f][s] (N x S complex128) with the host libm's cosf/sinf,
+// bit-identical to the reference's table (used by the FP64 path).
+void tcc_pupil_host(const std::vector<SrcPoint>& pts, const PupilParams& pp, double* P);
+
+// Device: A[f][s] = sqrt(J_s) P(f, s) in FP32 (N x S complex64, row-major).
+int tcc_build_A(const SrcPoint* pts_dev, const PupilParams& pp, float2* A, cudaStream_t st);
+
+// Device: bf16 split operands for TCC = A A^H on the tensor cores.
+// X1, X2, Y are N x Kp bf16, Kp = round_up(6 S, 64).
+int tcc_split_operands(const float2* A, int N, int S, int Kp, void* X1, void* X2, void* Y,
+                       cudaStream_t st);
+int tcc_kp(int S);
+
+// Device: Hermitian TCC (N x N complex64) = X1 Y^T + i X2 Y^T by tcgen05 MMA,
+// upper tiles computed, lower tiles mirrored.  err_dev receives a nonzero code
+// if a pipeline wait gave up.
+int tcc_gemm_tc(const void* X1, const void* X2, const void* Y, int N, int Kp, float2* tcc,
+                int* err_dev, cudaStream_t st);
+
+// Device: FP64 TCC by direct accumulation over source points (the plain FP64
+// path): tcc[i][j] = sum_s J_s P[i][s] conj(P[j][s]).  P is N x S complex128.
+int tcc_direct_fp64(const double2* P, const float* J, int N, int S, double2* tcc, cudaStream_t st);
+
+// Device: SOCS-layout kernels of the Abbe (source-point) form of the Hopkins
+// image: H_s[f] = conj A[f][s] (S x N complex64), lam = 1.
+int tcc_factor_kernels(const float2* A, int N, int S, float2* H, float* lam, cudaStream_t st);
+
+// Device: min/max of the real and imaginary parts of a complex64/128 matrix
+// (klitho_tcc.cpp:521-528 prints the maxima).  out4 = {max re, min re, max im, min im}.
+int tcc_minmax_c64(const float2* m, size_t n, double* out4_host, cudaStream_t st);
+int tcc_minmax_c128(const double2* m, size_t n, double* out4_host, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// Eigen-decomposition by blocked subspace iteration (FP64 Rayleigh-Ritz)
+// ---------------------------------------------------------------------------
+struct EigenOptions {
+  int K;          // kernels wanted
+  int B;          // block size (>= K)
+  int max_iter;   // iteration cap (KL_ERR_NOT_CONVERGED beyond it)
+  double tol;     // relative change of the top-K Ritz values between checks
+  uint64_t seed;  // start block
+};
+
+struct EigenResult {
+  int iterations;
+  double residual;  // max relative Ritz-value change at the last check
+};
+
+// Operator TCC = A A^H given by its FP32 factor A (N x S).
+int eig_topk_factor(const float2* A, int N, int S, const EigenOptions& opt, double2* U,
+                    double* evals, EigenResult* res, cudaStream_t st);
+// Operator given by a materialised FP64 TCC (N x N).
+int eig_topk_dense(const double2* tcc, int N, const EigenOptions& opt, double2* U, double* evals,
+                   EigenResult* res, cudaStream_t st);
+// Operator given by a materialised FP32 TCC (N x N).
+int eig_topk_dense_c64(const float2* tcc, int N, const EigenOptions& opt, double2* U,
+                       double* evals, EigenResult* res, cudaStream_t st);
+
+// Kernels in the reference layout: krn[k][j] = U[n-1-j][k] (klitho_tcc.cpp:358-362),
+// as separate float32 planes.
+int eig_to_kernels(const double2* U, int N, int K, float* re, float* im, cudaStream_t st);
+
+}  // namespace kl

@@ -1,0 +1,333 @@
+// kl_tcc_api.cpp -- C ABI of TCC assembly, top-K SOCS kernels and the
+// Hopkins image (see include/klitho_gpu.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kl_internal.h"
+#include "kl_tcc.h"
+
+struct kl_tcc_plan_s {
+  int precision = KL_PREC_FAST;
+  int Lx = 0, Ly = 0, srcSize = 0;
+  float outerSigma = 0.f;
+  kl::PupilParams pp{};
+  std::vector<kl::SrcPoint> pts;
+  kl::SrcPoint* pts_dev = nullptr;
+  float2* A = nullptr;        // fast path: N x S FP32 factor
+  double2* P = nullptr;       // FP64 path: N x S pupil table (host libm)
+  float* J = nullptr;         // FP64 path: S weights
+  double2* tcc64 = nullptr;   // FP64 path: TCC (built on demand)
+  int* err = nullptr;
+  kl_socs_plan hopkins = nullptr;  // SOCS plan of the Abbe form (lazy)
+  int hopkins_clips = 0;
+};
+
+namespace {
+void free_plan(kl_tcc_plan p) {
+  if (!p) return;
+  cudaFree(p->pts_dev);
+  cudaFree(p->A);
+  cudaFree(p->P);
+  cudaFree(p->J);
+  cudaFree(p->tcc64);
+  cudaFree(p->err);
+  if (p->hopkins) kl_socs_plan_destroy(p->hopkins);
+  delete p;
+}
+
+int dalloc(void** ptr, size_t bytes, const char* what) {
+  if (cudaMalloc(ptr, bytes ? bytes : 16) != cudaSuccess) {
+    cudaGetLastError();
+    kl::set_error(std::string("cudaMalloc(") + what + ") failed");
+    return KL_ERR_NOMEM;
+  }
+  return KL_OK;
+}
+
+int ensure_tcc64(kl_tcc_plan p, cudaStream_t st) {
+  if (p->tcc64) return KL_OK;
+  const size_t N = (size_t)p->pp.N;
+  int rc = dalloc((void**)&p->tcc64, sizeof(double2) * N * N, "FP64 TCC");
+  if (rc) return rc;
+  return kl::tcc_direct_fp64(p->P, p->J, p->pp.N, p->pp.S, p->tcc64, st);
+}
+}  // namespace
+
+extern "C" {
+
+int kl_tcc_plan_create(kl_tcc_plan* plan, const float* src, int srcSize, double NA, double defocus,
+                       double n_medium, int Lx, int Ly, int precision) {
+  KL_CHECK_ARG(plan, "kl_tcc_plan_create: plan is NULL");
+  *plan = nullptr;
+  KL_CHECK_ARG(src && srcSize > 2 && Lx > 0 && Ly > 0 && NA > 0 && n_medium > 0,
+               "kl_tcc_plan_create: bad arguments");
+  KL_CHECK_ARG(precision == KL_PREC_FAST || precision == KL_PREC_FP64,
+               "kl_tcc_plan_create: unknown precision");
+  kl_tcc_plan p = new (std::nothrow) kl_tcc_plan_s;
+  if (!p) return KL_ERR_NOMEM;
+  p->precision = precision;
+  p->Lx = Lx;
+  p->Ly = Ly;
+  p->srcSize = srcSize;
+  float sig = kl_outer_sigma(src, srcSize);
+  if (sig > 1.0f) sig = 1.0f;  // klitho_tcc.cpp:480-483
+  p->outerSigma = sig;
+  int Nx = 0, Ny = 0;
+  kl_band_size(NA, Lx, Ly, sig, &Nx, &Ny);
+  kl::tcc_source_points(src, srcSize, sig, 193.0f, (float)NA, (float)defocus, n_medium, Lx, Ly,
+                        Nx, Ny, p->pts, p->pp);
+  const kl::PupilParams& pp = p->pp;
+  if (pp.S == 0) {
+    free_plan(p);
+    kl::set_error("kl_tcc_plan_create: the source has no points inside the pupil");
+    return KL_ERR_INVALID;
+  }
+  if (n_medium * n_medium < NA * NA) {
+    free_plan(p);
+    kl::set_error("kl_tcc_plan_create: NA exceeds n_medium; the defocus phase is undefined");
+    return KL_ERR_INVALID;
+  }
+  int rc;
+  if ((rc = dalloc((void**)&p->err, sizeof(int), "status"))) {
+    free_plan(p);
+    return rc;
+  }
+  cudaMemset(p->err, 0, sizeof(int));
+  const size_t NS = (size_t)pp.N * pp.S;
+  if (precision == KL_PREC_FAST) {
+    if ((rc = dalloc((void**)&p->pts_dev, sizeof(kl::SrcPoint) * pp.S, "source points")) ||
+        (rc = dalloc((void**)&p->A, sizeof(float2) * NS, "TCC factor"))) {
+      free_plan(p);
+      return rc;
+    }
+    cudaMemcpy(p->pts_dev, p->pts.data(), sizeof(kl::SrcPoint) * pp.S, cudaMemcpyHostToDevice);
+    if ((rc = kl::tcc_build_A(p->pts_dev, pp, p->A, nullptr))) {
+      free_plan(p);
+      return rc;
+    }
+  } else {
+    std::vector<double> P(2 * NS);
+    kl::tcc_pupil_host(p->pts, pp, P.data());
+    std::vector<float> J(pp.S);
+    for (int s = 0; s < pp.S; ++s) J[s] = p->pts[s].J;
+    if ((rc = dalloc((void**)&p->P, sizeof(double2) * NS, "pupil table")) ||
+        (rc = dalloc((void**)&p->J, sizeof(float) * pp.S, "source weights"))) {
+      free_plan(p);
+      return rc;
+    }
+    cudaMemcpy(p->P, P.data(), sizeof(double2) * NS, cudaMemcpyHostToDevice);
+    cudaMemcpy(p->J, J.data(), sizeof(float) * pp.S, cudaMemcpyHostToDevice);
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    kl::set_error(std::string("kl_tcc_plan_create: ") + cudaGetErrorString(cudaGetLastError()));
+    free_plan(p);
+    return KL_ERR_CUDA;
+  }
+  *plan = p;
+  return KL_OK;
+}
+
+int kl_tcc_plan_destroy(kl_tcc_plan plan) {
+  free_plan(plan);
+  return KL_OK;
+}
+
+int kl_tcc_plan_info(kl_tcc_plan p, int* Nx, int* Ny, int* N, int* S, float* outerSigma) {
+  KL_CHECK_ARG(p, "kl_tcc_plan_info: NULL plan");
+  if (Nx) *Nx = p->pp.Nx;
+  if (Ny) *Ny = p->pp.Ny;
+  if (N) *N = p->pp.N;
+  if (S) *S = p->pp.S;
+  if (outerSigma) *outerSigma = p->outerSigma;
+  return KL_OK;
+}
+
+int kl_tcc_factor(kl_tcc_plan p, float* A_dev, void* stream) {
+  KL_CHECK_ARG(p && A_dev, "kl_tcc_factor: NULL argument");
+  KL_CHECK_ARG(p->precision == KL_PREC_FAST, "kl_tcc_factor: FP32 factor exists on the fast path only");
+  KL_CUDA_TRY(cudaMemcpyAsync(A_dev, p->A, sizeof(float2) * (size_t)p->pp.N * p->pp.S,
+                              cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return KL_OK;
+}
+
+int kl_tcc_build(kl_tcc_plan p, void* tcc_dev, void* stream) {
+  KL_CHECK_ARG(p && tcc_dev, "kl_tcc_build: NULL argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int N = p->pp.N, S = p->pp.S;
+  if (p->precision == KL_PREC_FP64) {
+    int rc = kl::tcc_direct_fp64(p->P, p->J, N, S, (double2*)tcc_dev, st);
+    if (rc) return rc;
+    return KL_OK;
+  }
+  const int Kp = kl::tcc_kp(S);
+  void *X1 = nullptr, *X2 = nullptr, *Y = nullptr;
+  const size_t ob = sizeof(uint16_t) * (size_t)N * Kp;
+  int rc;
+  if ((rc = dalloc(&X1, ob, "split operand")) || (rc = dalloc(&X2, ob, "split operand")) ||
+      (rc = dalloc(&Y, ob, "split operand"))) {
+    cudaFree(X1);
+    cudaFree(X2);
+    return rc;
+  }
+  KL_CUDA_TRY(cudaMemsetAsync(p->err, 0, sizeof(int), st));
+  rc = kl::tcc_split_operands(p->A, N, S, Kp, X1, X2, Y, st);
+  if (!rc) rc = kl::tcc_gemm_tc(X1, X2, Y, N, Kp, (float2*)tcc_dev, p->err, st);
+  int herr = 0;
+  if (!rc) {
+    cudaMemcpyAsync(&herr, p->err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+      kl::set_error(std::string("kl_tcc_build: ") + cudaGetErrorString(cudaGetLastError()));
+      rc = KL_ERR_CUDA;
+    } else if (herr) {
+      kl::set_error("kl_tcc_build: tensor-core pipeline wait timed out (code " + std::to_string(herr) + ")");
+      rc = KL_ERR_CUDA;
+    }
+  }
+  cudaFree(X1);
+  cudaFree(X2);
+  cudaFree(Y);
+  return rc;
+}
+
+int kl_tcc_minmax(kl_tcc_plan p, const void* tcc_dev, double* out4, void* stream) {
+  KL_CHECK_ARG(p && tcc_dev && out4, "kl_tcc_minmax: NULL argument");
+  const size_t n = (size_t)p->pp.N * p->pp.N;
+  if (p->precision == KL_PREC_FP64)
+    return kl::tcc_minmax_c128((const double2*)tcc_dev, n, out4, (cudaStream_t)stream);
+  return kl::tcc_minmax_c64((const float2*)tcc_dev, n, out4, (cudaStream_t)stream);
+}
+
+int kl_tcc_build_minmax(kl_tcc_plan p, double* out4) {
+  KL_CHECK_ARG(p && out4, "kl_tcc_build_minmax: NULL argument");
+  const size_t n = (size_t)p->pp.N * p->pp.N;
+  void* tcc = nullptr;
+  int rc = dalloc(&tcc, (p->precision == KL_PREC_FP64 ? sizeof(double2) : sizeof(float2)) * n, "TCC");
+  if (rc) return rc;
+  rc = kl_tcc_build(p, tcc, nullptr);
+  if (!rc) rc = kl_tcc_minmax(p, tcc, out4, nullptr);
+  cudaFree(tcc);
+  return rc;
+}
+
+int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn_im_host,
+                float* scales_host, double* evals_host, int* iterations) {
+  KL_CHECK_ARG(p && krn_re_host && krn_im_host && scales_host, "kl_topk_eig: NULL argument");
+  const int N = p->pp.N, S = p->pp.S;
+  KL_CHECK_ARG(nk > 0 && nk <= N, "kl_topk_eig: nk must be in [1, N]");
+  cudaStream_t st = nullptr;
+  // kernels beyond the TCC's rank (<= S) have eigenvalue 0: the solver
+  // returns the nonzero part, the rest are zero kernels
+  const int K = std::min(nk, std::min(N, S));
+  kl::EigenOptions opt;
+  opt.K = K;
+  opt.B = block > 0 ? block : std::min(K + std::max(16, K / 2), std::max(K, 2 * K));
+  opt.max_iter = 400;
+  opt.tol = 1e-13;
+  opt.seed = 0x6b6c697468ull;
+  double2* U = nullptr;
+  double* ev = nullptr;
+  float *re = nullptr, *im = nullptr;
+  int rc;
+  if ((rc = dalloc((void**)&U, sizeof(double2) * (size_t)N * K, "eigenvectors")) ||
+      (rc = dalloc((void**)&ev, sizeof(double) * K, "eigenvalues")) ||
+      (rc = dalloc((void**)&re, sizeof(float) * (size_t)N * K, "kernels")) ||
+      (rc = dalloc((void**)&im, sizeof(float) * (size_t)N * K, "kernels"))) {
+    cudaFree(U);
+    cudaFree(ev);
+    cudaFree(re);
+    return rc;
+  }
+  kl::EigenResult res{};
+  if (p->precision == KL_PREC_FAST) {
+    rc = kl::eig_topk_factor(p->A, N, S, opt, U, ev, &res, st);
+  } else {
+    rc = ensure_tcc64(p, st);
+    if (!rc) rc = kl::eig_topk_dense(p->tcc64, N, opt, U, ev, &res, st);
+  }
+  if (!rc) rc = kl::eig_to_kernels(U, N, K, re, im, st);
+  std::vector<double> evh(K);
+  if (!rc) {
+    cudaMemcpy(krn_re_host, re, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
+    cudaMemcpy(krn_im_host, im, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
+    cudaMemcpy(evh.data(), ev, sizeof(double) * K, cudaMemcpyDeviceToHost);
+    if (cudaDeviceSynchronize() != cudaSuccess) {
+      kl::set_error(std::string("kl_topk_eig: ") + cudaGetErrorString(cudaGetLastError()));
+      rc = KL_ERR_CUDA;
+    }
+  }
+  if (!rc) {
+    for (int k = 0; k < nk; ++k) {
+      const double v = k < K ? evh[k] : 0.0;
+      scales_host[k] = (float)v;
+      if (evals_host) evals_host[k] = v;
+    }
+    for (int k = K; k < nk; ++k) {
+      std::memset(krn_re_host + (size_t)k * N, 0, sizeof(float) * N);
+      std::memset(krn_im_host + (size_t)k * N, 0, sizeof(float) * N);
+    }
+    if (iterations) *iterations = res.iterations;
+  }
+  cudaFree(U);
+  cudaFree(ev);
+  cudaFree(re);
+  cudaFree(im);
+  return rc;
+}
+
+int kl_hopkins_image(kl_tcc_plan p, const float* masks_dev, int nclips, float* images_dev,
+                     void* stream) {
+  KL_CHECK_ARG(p && masks_dev && images_dev, "kl_hopkins_image: NULL argument");
+  KL_CHECK_ARG(p->precision == KL_PREC_FAST, "kl_hopkins_image: FP64 imaging is kl_fp64_hopkins_image");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int N = p->pp.N, S = p->pp.S;
+  if (!p->hopkins || nclips > p->hopkins_clips) {
+    if (p->hopkins) kl_socs_plan_destroy(p->hopkins);
+    p->hopkins = nullptr;
+    int rc = kl_socs_plan_create(&p->hopkins, p->Lx, p->Ly, p->pp.Nx, p->pp.Ny, S, 1,
+                                 std::max(1, nclips));
+    if (rc) return rc;
+    p->hopkins_clips = std::max(1, nclips);
+    float2* H = nullptr;
+    float* lam = nullptr;
+    if ((rc = dalloc((void**)&H, sizeof(float2) * (size_t)N * S, "Abbe kernels")) ||
+        (rc = dalloc((void**)&lam, sizeof(float) * S, "Abbe weights"))) {
+      cudaFree(H);
+      return rc;
+    }
+    rc = kl::tcc_factor_kernels(p->A, N, S, H, lam, st);
+    if (!rc) rc = kl_socs_set_kernels_device(p->hopkins, 0, H, lam, st);
+    cudaStreamSynchronize(st);
+    cudaFree(H);
+    cudaFree(lam);
+    if (rc) return rc;
+  }
+  return kl_socs_forward(p->hopkins, masks_dev, nclips, images_dev, stream);
+}
+
+int kl_hopkins_image_host(kl_tcc_plan p, const float* mask_host, float* image_host) {
+  KL_CHECK_ARG(p && mask_host && image_host, "kl_hopkins_image_host: NULL argument");
+  const size_t bytes = sizeof(float) * (size_t)p->Lx * p->Ly;
+  float *md = nullptr, *id = nullptr;
+  int rc;
+  if ((rc = dalloc((void**)&md, bytes, "mask")) || (rc = dalloc((void**)&id, bytes, "image"))) {
+    cudaFree(md);
+    return rc;
+  }
+  cudaMemcpy(md, mask_host, bytes, cudaMemcpyHostToDevice);
+  rc = kl_hopkins_image(p, md, 1, id, nullptr);
+  if (!rc && cudaMemcpy(image_host, id, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    kl::set_error(std::string("kl_hopkins_image_host: ") + cudaGetErrorString(cudaGetLastError()));
+    rc = KL_ERR_CUDA;
+  }
+  cudaFree(md);
+  cudaFree(id);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,608 @@
+// tcc.cu -- TCC assembly (K-Litho-TCC/klitho_tcc.cpp:186-267 calcTCC).
+//
+// The reference accumulates TCC[f1][f2] += J(s) P(f1,s) conj P(f2,s) over
+// source points.  That is the Hermitian product TCC = A A^H with
+// A[f][s] = sqrt(J_s) P(f, s).  Fast path: A is sampled in FP32 on the GPU and
+// the product runs on the 5th-generation tensor cores as real GEMMs on a
+// 3-term BF16 split (hi*hi + hi*lo + lo*hi), FP32 accumulation in TMEM:
+//     TCC_re = [Ar Ai](hi,hi,lo) . [Ar Ai](hi,lo,hi)^T
+//     TCC_im = [Ai -Ar](hi,hi,lo) . [Ar Ai](hi,lo,hi)^T
+// One CTA per 128 x 128 upper tile: a TMA producer thread streams 128 x 64
+// bf16 tiles (128-byte swizzle) through a 4-stage mbarrier pipeline, one
+// thread issues tcgen05.mma into two TMEM accumulators (re, im), and four
+// warps drain TMEM with tcgen05.ld, writing the tile and its conjugate
+// transpose (coalesced) so the result is exactly Hermitian.
+// FP64 path: the same sum accumulated in FP64 on the CUDA cores from the
+// reference-identical pupil table.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "kl_internal.h"
+#include "kl_tcc.h"
+
+namespace kl {
+
+// ---------------------------------------------------------------------------
+// host: source points and the reference pupil table
+// ---------------------------------------------------------------------------
+void tcc_source_points(const float* src, int srcSize, float outerSigma, float lambda, float NA,
+                       float defocus, double n_medium, int Lx, int Ly, int Nx, int Ny,
+                       std::vector<SrcPoint>& pts, PupilParams& pp) {
+  // float arithmetic of klitho_tcc.cpp:189-197 and :202-211
+  const int sh = (int)((srcSize - 1) / 2.0);
+  const float sig = outerSigma > 1.0f ? 1.0f : outerSigma;
+  const int oSgm = (int)std::ceil((float)sh * sig);
+  const float dz = defocus / (NA * NA / lambda);
+  const float k = (float)(2 * M_PI / lambda);
+  const float Lxn = (float)Lx * NA / lambda, Lyn = (float)Ly * NA / lambda;
+  pts.clear();
+  for (int q = -oSgm; q <= oSgm; ++q)
+    for (int p = -oSgm; p <= oSgm; ++p) {
+      const int id = (q + sh) * srcSize + p + sh;
+      if (src[id] != 0.0f && p * p + q * q <= sh * sh) {
+        SrcPoint t;
+        t.sx = (float)p / (float)sh;
+        t.sy = (float)q / (float)sh;
+        t.J = src[id];
+        t.nxmin = (int)((-1.0f - t.sx) * Lxn);
+        t.nxmax = (int)((1.0f - t.sx) * Lxn);
+        t.nymin = (int)((-1.0f - t.sy) * Lyn);
+        t.nymax = (int)((1.0f - t.sy) * Lyn);
+        t.src_id = id;
+        pts.push_back(t);
+      }
+    }
+  pp.Nx = Nx;
+  pp.Ny = Ny;
+  pp.N = (2 * Nx + 1) * (2 * Ny + 1);
+  pp.S = (int)pts.size();
+  pp.Lx_norm = Lxn;
+  pp.Ly_norm = Lyn;
+  pp.dzk = dz * k;
+  pp.NA = NA;
+  pp.n_medium2 = n_medium * n_medium;
+}
+
+void tcc_pupil_host(const std::vector<SrcPoint>& pts, const PupilParams& pp, double* P) {
+  const int N = pp.N, S = pp.S, bw = 2 * pp.Nx + 1;
+  std::memset(P, 0, sizeof(double) * 2 * (size_t)N * S);
+  for (int s = 0; s < S; ++s) {
+    const SrcPoint& t = pts[s];
+    for (int ny = t.nymin; ny <= t.nymax; ++ny) {
+      const float fy = (float)ny / pp.Ly_norm + t.sy;
+      if (!(fy * fy <= 1.0f)) continue;
+      for (int nx = t.nxmin; nx <= t.nxmax; ++nx) {
+        const float fx = (float)nx / pp.Lx_norm + t.sx;
+        const float rho2 = fx * fx + fy * fy;
+        if (!(rho2 <= 1.0f)) continue;
+        if (ny < -pp.Ny || ny > pp.Ny || nx < -pp.Nx || nx > pp.Nx) continue;
+        const float ph = (float)((double)pp.dzk * std::sqrt(pp.n_medium2 - (double)(rho2 * pp.NA * pp.NA)));
+        const size_t f = (size_t)((ny + pp.Ny) * bw + nx + pp.Nx);
+        P[2 * (f * S + s)] = (double)cosf(ph);
+        P[2 * (f * S + s) + 1] = (double)sinf(ph);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// device: A = sqrt(J) P in FP32, same float roundings as the reference
+// ---------------------------------------------------------------------------
+__global__ void k_build_A(const SrcPoint* __restrict__ pts, const PupilParams pp,
+                          float2* __restrict__ A) {
+  const int bw = 2 * pp.Nx + 1;
+  const size_t n = (size_t)pp.N * pp.S;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(i / pp.S), s = (int)(i % pp.S);
+    const int ny = f / bw - pp.Ny, nx = f % bw - pp.Nx;
+    const SrcPoint t = pts[s];
+    float2 v = make_float2(0.f, 0.f);
+    if (ny >= t.nymin && ny <= t.nymax && nx >= t.nxmin && nx <= t.nxmax) {
+      const float fy = __fadd_rn(__fdiv_rn((float)ny, pp.Ly_norm), t.sy);
+      const float fx = __fadd_rn(__fdiv_rn((float)nx, pp.Lx_norm), t.sx);
+      const float rho2 = __fadd_rn(__fmul_rn(fx, fx), __fmul_rn(fy, fy));
+      if (__fmul_rn(fy, fy) <= 1.0f && rho2 <= 1.0f) {
+        const float r2na = __fmul_rn(__fmul_rn(rho2, pp.NA), pp.NA);
+        const double arg = __dsub_rn(pp.n_medium2, (double)r2na);
+        const float ph = __double2float_rn(__dmul_rn((double)pp.dzk, sqrt(arg)));
+        float sn, cs;
+        sincosf(ph, &sn, &cs);
+        const float a = sqrtf(t.J);
+        v = make_float2(a * cs, a * sn);
+      }
+    }
+    A[i] = v;
+  }
+}
+
+int tcc_build_A(const SrcPoint* pts_dev, const PupilParams& pp, float2* A, cudaStream_t st) {
+  const size_t n = (size_t)pp.N * pp.S;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_build_A<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(pts_dev, pp, A);
+  KL_CUDA_TRY(cudaGetLastError());
+  return KL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// bf16 split operands
+// ---------------------------------------------------------------------------
+int tcc_kp(int S) { return ((6 * S + 63) / 64) * 64; }
+
+__global__ void k_tcc_split(const float2* __restrict__ A, int N, int S, int Kp,
+                            __nv_bfloat16* __restrict__ X1, __nv_bfloat16* __restrict__ X2,
+                            __nv_bfloat16* __restrict__ Y) {
+  const size_t n = (size_t)N * Kp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int f = (int)(i / Kp), k = (int)(i % Kp);
+    float x1 = 0.f, x2 = 0.f, y = 0.f;
+    if (k < 6 * S) {
+      const int seg = k / S, s = k - seg * S;
+      const float2 a = A[(size_t)f * S + s];
+      const __nv_bfloat16 rh = __float2bfloat16_rn(a.x), ih = __float2bfloat16_rn(a.y);
+      const float rhf = __bfloat162float(rh), ihf = __bfloat162float(ih);
+      const float rl = __bfloat162float(__float2bfloat16_rn(a.x - rhf));
+      const float il = __bfloat162float(__float2bfloat16_rn(a.y - ihf));
+      switch (seg) {
+        case 0: x1 = rhf; x2 = ihf; y = rhf; break;
+        case 1: x1 = ihf; x2 = -rhf; y = ihf; break;
+        case 2: x1 = rhf; x2 = ihf; y = rl; break;
+        case 3: x1 = ihf; x2 = -rhf; y = il; break;
+        case 4: x1 = rl; x2 = il; y = rhf; break;
+        default: x1 = il; x2 = -rl; y = ihf; break;
+      }
+    }
+    X1[i] = __float2bfloat16_rn(x1);
+    X2[i] = __float2bfloat16_rn(x2);
+    Y[i] = __float2bfloat16_rn(y);
+  }
+}
+
+int tcc_split_operands(const float2* A, int N, int S, int Kp, void* X1, void* X2, void* Y,
+                       cudaStream_t st) {
+  const size_t n = (size_t)N * Kp;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  k_tcc_split<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(A, N, S, Kp, (__nv_bfloat16*)X1,
+                                                       (__nv_bfloat16*)X2, (__nv_bfloat16*)Y);
+  KL_CUDA_TRY(cudaGetLastError());
+  return KL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 Hermitian GEMM
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int TM = 128, TN = 128, TK = 64, STAGES = 4;
+constexpr int TILE_BYTES = TM * TK * 2;         // 16 KB, one 128 x 64 bf16 tile
+constexpr int STAGE_BYTES = 3 * TILE_BYTES;     // X1, X2, Y
+constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
+constexpr uint32_t TMEM_COLS = 256;             // re: [0,128), im: [128,256)
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s bound on any pipeline wait
+
+// instruction descriptor: dense, f32 accumulate, bf16 A/B, both K-major, M=128, N=128
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                           ((uint32_t)(TM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait; returns false (and records `code`) if the phase never completes
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  while (true) {
+    if (mbar_try(bar, parity)) return true;
+    if (now_ns() - t0 > WAIT_NS) {
+      atomicExch(err, code);
+      return false;
+    }
+    __nanosleep(128);
+  }
+}
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+// K-major, 128-byte swizzle, 8-row core groups 1024 B apart
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(IDESC), "r"(accum), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+}
+}  // namespace
+
+__global__ void __launch_bounds__(128, 1)
+    k_tcc_gemm(const __grid_constant__ CUtensorMap tmX1, const __grid_constant__ CUtensorMap tmX2,
+               const __grid_constant__ CUtensorMap tmY, int N, int nkb, int nt,
+               float2* __restrict__ tcc, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
+  uint64_t* empty = full + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+  // upper-triangular tile (ib <= jb) of this CTA
+  int t = blockIdx.x, ib = 0, rowlen = nt;
+  while (t >= rowlen) {
+    t -= rowlen;
+    ++ib;
+    --rowlen;
+  }
+  const int jb = ib + t;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);
+      mbar_init(smem_u32(&empty[s]), 1);
+    }
+    mbar_init(smem_u32(done), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (threadIdx.x == 0) {
+    // TMA producer
+    int armed[STAGES];
+    for (int s = 0; s < STAGES; ++s) armed[s] = -1;
+    bool ok = true;
+    for (int kb = 0; kb < nkb && ok; ++kb) {
+      const int s = kb % STAGES, use = kb / STAGES;
+      if (use > 0) ok = mbar_wait(smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 1);
+      if (!ok) break;
+      const uint32_t bar = smem_u32(&full[s]);
+      mbar_expect_tx(bar, STAGE_BYTES);
+      uint8_t* st = smem + s * STAGE_BYTES;
+      tma_load_2d(smem_u32(st), &tmX1, kb * TK, ib * TM, bar);
+      tma_load_2d(smem_u32(st + TILE_BYTES), &tmX2, kb * TK, ib * TM, bar);
+      tma_load_2d(smem_u32(st + 2 * TILE_BYTES), &tmY, kb * TK, jb * TN, bar);
+      armed[s] = use;
+    }
+    if (!ok) {
+      // let copies already issued land before the CTA can retire
+      for (int s = 0; s < STAGES; ++s)
+        if (armed[s] >= 0) mbar_wait(smem_u32(&full[s]), (uint32_t)(armed[s] & 1), err, 4);
+    }
+  } else if (threadIdx.x == 32) {
+    // MMA issuer
+    bool ok = true;
+    for (int kb = 0; kb < nkb && ok; ++kb) {
+      const int s = kb % STAGES, use = kb / STAGES;
+      ok = mbar_wait(smem_u32(&full[s]), (uint32_t)(use & 1), err, 2);
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a1 = smem_u32(smem + s * STAGE_BYTES);
+      const uint32_t a2 = a1 + TILE_BYTES, b = a1 + 2 * TILE_BYTES;
+#pragma unroll
+      for (int k = 0; k < TK / 16; ++k) {
+        const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+        const uint32_t off = (uint32_t)(k * 32);  // 16 bf16 along K inside the swizzle atom
+        mma_bf16(tmem, smem_desc(a1 + off), smem_desc(b + off), acc);
+        mma_bf16(tmem + 128, smem_desc(a2 + off), smem_desc(b + off), acc);
+      }
+      mma_commit(smem_u32(&empty[s]));
+    }
+    mma_commit(smem_u32(done));
+  }
+  __syncwarp();
+
+  // epilogue: four warps, warp w owns TMEM lanes (tile rows) [32w, 32w+32)
+  const bool ready = mbar_wait(smem_u32(done), 0u, err, 3);
+  __syncwarp();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ready) {
+    const int r = warp * 32 + lane;
+    const int i = ib * TM + r;
+    const bool diag = ib == jb;
+#pragma unroll 1
+    for (int c0 = 0; c0 < TN; c0 += 32) {
+      uint32_t re[32], im[32];
+      const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16);
+      tmem_ld32(base + (uint32_t)c0, re);
+      tmem_ld32(base + 128u + (uint32_t)c0, im);
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      // direct tile: row i, columns j0 + c0 + c
+      if (i < N) {
+        float2* row = tcc + (size_t)i * N;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+          const int j = jb * TN + c0 + c;
+          if (j < N && (!diag || c0 + c >= r)) {
+            float2 v = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
+            if (diag && c0 + c == r) v.y = 0.f;
+            row[j] = v;
+          }
+        }
+      }
+      // conjugate transpose: tcc[j][i], consecutive lanes write consecutive i
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        const int j = jb * TN + c0 + c;
+        if (j < N && i < N && (!diag || c0 + c > r))
+          tcc[(size_t)j * N + i] = make_float2(__uint_as_float(re[c]), -__uint_as_float(im[c]));
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+                 : "memory");
+  }
+}
+
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+int make_map(CUtensorMap* m, const void* base, int rows, int Kp) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is unavailable");
+    return KL_ERR_CUDA;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
+  const cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)TM};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
+                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return KL_ERR_CUDA;
+  }
+  return KL_OK;
+}
+}  // namespace
+
+int tcc_gemm_tc(const void* X1, const void* X2, const void* Y, int N, int Kp, float2* tcc,
+                int* err_dev, cudaStream_t st) {
+  KL_CHECK_ARG(N > 0 && Kp > 0 && Kp % TK == 0, "tcc_gemm_tc: bad sizes");
+  KL_CHECK_ARG(((uintptr_t)X1 | (uintptr_t)X2 | (uintptr_t)Y) % 16 == 0, "tcc_gemm_tc: operands must be 16-byte aligned");
+  CUtensorMap m1, m2, my;
+  int rc;
+  if ((rc = make_map(&m1, X1, N, Kp)) || (rc = make_map(&m2, X2, N, Kp)) || (rc = make_map(&my, Y, N, Kp))) return rc;
+  const int nt = (N + TM - 1) / TM;
+  const int tiles = nt * (nt + 1) / 2;
+  KL_CUDA_TRY(cudaFuncSetAttribute(k_tcc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
+  k_tcc_gemm<<<tiles, 128, SMEM_BYTES, st>>>(m1, m2, my, N, Kp / TK, nt, tcc, err_dev);
+  KL_CUDA_TRY(cudaGetLastError());
+  return KL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 direct TCC: tcc[i][j] = sum_s J_s P[i][s] conj P[j][s], upper tiles + mirror
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_tcc_direct(const double2* __restrict__ P,
+                                                    const float* __restrict__ J, int N, int S,
+                                                    int nt, double2* __restrict__ tcc) {
+  constexpr int T = 32, TKS = 16;
+  __shared__ double2 sa[TKS][T + 1];
+  __shared__ double2 sb[TKS][T + 1];
+  int t = blockIdx.x, ib = 0, rowlen = nt;
+  while (t >= rowlen) {
+    t -= rowlen;
+    ++ib;
+    --rowlen;
+  }
+  const int jb = ib + t;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double2 acc[2][2] = {};
+  for (int s0 = 0; s0 < S; s0 += TKS) {
+    for (int i = threadIdx.x; i < TKS * T; i += 256) {
+      const int kk = i / T, r = i - kk * T, s = s0 + kk;
+      const int gi = ib * T + r, gj = jb * T + r;
+      double2 a = make_double2(0, 0), b = make_double2(0, 0);
+      if (s < S && gi < N) {
+        const double2 p = P[(size_t)gi * S + s];
+        const double w = (double)J[s];
+        a = make_double2(p.x * w, p.y * w);
+      }
+      if (s < S && gj < N) {
+        const double2 p = P[(size_t)gj * S + s];
+        b = make_double2(p.x, -p.y);
+      }
+      sa[kk][r] = a;
+      sb[kk][r] = b;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TKS; ++kk) {
+      const double2 a0 = sa[kk][ty], a1 = sa[kk][ty + 16], b0 = sb[kk][tx], b1 = sb[kk][tx + 16];
+      acc[0][0] = make_double2(fma(a0.x, b0.x, fma(-a0.y, b0.y, acc[0][0].x)), fma(a0.x, b0.y, fma(a0.y, b0.x, acc[0][0].y)));
+      acc[0][1] = make_double2(fma(a0.x, b1.x, fma(-a0.y, b1.y, acc[0][1].x)), fma(a0.x, b1.y, fma(a0.y, b1.x, acc[0][1].y)));
+      acc[1][0] = make_double2(fma(a1.x, b0.x, fma(-a1.y, b0.y, acc[1][0].x)), fma(a1.x, b0.y, fma(a1.y, b0.x, acc[1][0].y)));
+      acc[1][1] = make_double2(fma(a1.x, b1.x, fma(-a1.y, b1.y, acc[1][1].x)), fma(a1.x, b1.y, fma(a1.y, b1.x, acc[1][1].y)));
+    }
+    __syncthreads();
+  }
+  for (int a = 0; a < 2; ++a)
+    for (int b = 0; b < 2; ++b) {
+      const int i = ib * T + ty + 16 * a, j = jb * T + tx + 16 * b;
+      if (i < N && j < N && j >= i) {
+        double2 v = acc[a][b];
+        if (i == j) v.y = 0.0;
+        tcc[(size_t)i * N + j] = v;
+        if (j > i) tcc[(size_t)j * N + i] = make_double2(v.x, -v.y);
+      }
+    }
+}
+
+int tcc_direct_fp64(const double2* P, const float* J, int N, int S, double2* tcc, cudaStream_t st) {
+  const int nt = (N + 31) / 32;
+  k_tcc_direct<<<nt * (nt + 1) / 2, 256, 0, st>>>(P, J, N, S, nt, tcc);
+  KL_CUDA_TRY(cudaGetLastError());
+  return KL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Hopkins image through the factor: H_s[f] = conj A[f][s], weight 1
+// ---------------------------------------------------------------------------
+__global__ void k_factor_kernels(const float2* __restrict__ A, int N, int S, float2* __restrict__ H,
+                                 float* __restrict__ lam) {
+  const size_t n = (size_t)N * S;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int s = (int)(i / N), f = (int)(i % N);
+    const float2 a = A[(size_t)f * S + s];
+    H[i] = make_float2(a.x, -a.y);
+    if (f == 0) lam[s] = 1.0f;
+  }
+}
+
+int tcc_factor_kernels(const float2* A, int N, int S, float2* H, float* lam, cudaStream_t st) {
+  k_factor_kernels<<<296, 256, 0, st>>>(A, N, S, H, lam);
+  KL_CUDA_TRY(cudaGetLastError());
+  return KL_OK;
+}
+
+// ---------------------------------------------------------------------------
+// min / max of the real and imaginary parts
+// ---------------------------------------------------------------------------
+template <typename C>
+__global__ void k_minmax(const C* __restrict__ m, size_t n, double* __restrict__ out) {
+  double mxr = -1e300, mnr = 1e300, mxi = -1e300, mni = 1e300;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double r = (double)m[i].x, im = (double)m[i].y;
+    mxr = fmax(mxr, r);
+    mnr = fmin(mnr, r);
+    mxi = fmax(mxi, im);
+    mni = fmin(mni, im);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mxr = fmax(mxr, __shfl_xor_sync(0xffffffffu, mxr, o));
+    mnr = fmin(mnr, __shfl_xor_sync(0xffffffffu, mnr, o));
+    mxi = fmax(mxi, __shfl_xor_sync(0xffffffffu, mxi, o));
+    mni = fmin(mni, __shfl_xor_sync(0xffffffffu, mni, o));
+  }
+  __shared__ double sm[4][32];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    sm[0][w] = mxr;
+    sm[1][w] = mnr;
+    sm[2][w] = mxi;
+    sm[3][w] = mni;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+      mxr = fmax(mxr, sm[0][k]);
+      mnr = fmin(mnr, sm[1][k]);
+      mxi = fmax(mxi, sm[2][k]);
+      mni = fmin(mni, sm[3][k]);
+    }
+    out[4 * blockIdx.x + 0] = fmax(mxr, sm[0][0]);
+    out[4 * blockIdx.x + 1] = fmin(mnr, sm[1][0]);
+    out[4 * blockIdx.x + 2] = fmax(mxi, sm[2][0]);
+    out[4 * blockIdx.x + 3] = fmin(mni, sm[3][0]);
+  }
+}
+
+template <typename C>
+int minmax(const C* m, size_t n, double* out4, cudaStream_t st) {
+  const int blocks = 296;
+  double* d = nullptr;
+  KL_CUDA_TRY(cudaMalloc(&d, sizeof(double) * 4 * blocks));
+  k_minmax<C><<<blocks, 256, 0, st>>>(m, n, d);
+  std::vector<double> h(4 * blocks);
+  cudaError_t e = cudaMemcpyAsync(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    set_error(std::string("minmax: ") + cudaGetErrorString(e));
+    return KL_ERR_CUDA;
+  }
+  out4[0] = -1e300;
+  out4[1] = 1e300;
+  out4[2] = -1e300;
+  out4[3] = 1e300;
+  for (int b = 0; b < blocks; ++b) {
+    out4[0] = std::fmax(out4[0], h[4 * b]);
+    out4[1] = std::fmin(out4[1], h[4 * b + 1]);
+    out4[2] = std::fmax(out4[2], h[4 * b + 2]);
+    out4[3] = std::fmin(out4[3], h[4 * b + 3]);
+  }
+  return KL_OK;
+}
+
+int tcc_minmax_c64(const float2* m, size_t n, double* out4, cudaStream_t st) { return minmax(m, n, out4, st); }
+int tcc_minmax_c128(const double2* m, size_t n, double* out4, cudaStream_t st) { return minmax(m, n, out4, st); }
+
+}  // namespace kl

@@ -75,6 +75,17 @@ def lib() -> ctypes.CDLL:
         L.kl_socs_forward.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
         L.kl_socs_forward_host.argtypes = [_vp, _c_float_p, ctypes.c_int, _c_float_p, _vp]
         L.kl_mask_spectrum.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+        L.kl_tcc_plan_create.argtypes = [ctypes.POINTER(_vp), _c_float_p, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.kl_tcc_plan_destroy.argtypes = [_vp]
+        L.kl_tcc_plan_info.argtypes = [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_float_p]
+        L.kl_tcc_factor.argtypes = [_vp, _vp, _vp]
+        L.kl_tcc_build.argtypes = [_vp, _vp, _vp]
+        L.kl_tcc_minmax.argtypes = [_vp, _vp, ctypes.POINTER(ctypes.c_double), _vp]
+        L.kl_topk_eig.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _c_float_p, _c_float_p,
+                                  _c_float_p, ctypes.POINTER(ctypes.c_double), _c_int_p]
+        L.kl_hopkins_image.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
         L.kl_socs_enable_timing.argtypes = [_vp, ctypes.c_int]
         L.kl_socs_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), _c_int_p]
         _LIB = L
@@ -241,3 +252,81 @@ class SocsPlan:
         n = masks_dev.shape[0] if nclips is None else nclips
         check(lib().kl_mask_spectrum(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(band_dev),
                                      _stream_ptr(stream)), "kl_mask_spectrum")
+
+
+# ---------------------------------------------------------------------------
+# TCC, SOCS kernels and the Hopkins image (klitho_tcc's numerics)
+# ---------------------------------------------------------------------------
+
+PREC_FAST = 0
+PREC_FP64 = 1
+
+
+class TccPlan:
+    """GPU TCC of one optical setting (calcTCC / calcKernels / calcImage)."""
+
+    def __init__(self, src: np.ndarray, NA: float, defocus: float, Lx: int, Ly: int,
+                 n_medium: float = 1.0, precision: int = PREC_FAST):
+        s = np.ascontiguousarray(src, dtype=np.float32)
+        h = _vp()
+        check(lib().kl_tcc_plan_create(ctypes.byref(h), _fp(s), int(s.shape[0]), float(NA),
+                                       float(defocus), float(n_medium), int(Lx), int(Ly),
+                                       int(precision)), "kl_tcc_plan_create")
+        self._h = h
+        self.precision = precision
+        self.Lx, self.Ly = int(Lx), int(Ly)
+        nx, ny, n, S = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        sig = ctypes.c_float()
+        check(lib().kl_tcc_plan_info(h, ctypes.byref(nx), ctypes.byref(ny), ctypes.byref(n),
+                                     ctypes.byref(S), ctypes.byref(sig)), "kl_tcc_plan_info")
+        self.Nx, self.Ny, self.N, self.S = nx.value, ny.value, n.value, S.value
+        self.outer_sigma = sig.value
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().kl_tcc_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def factor(self, stream=None):
+        import torch
+        A = torch.empty((self.N, self.S, 2), dtype=torch.float32, device="cuda")
+        check(lib().kl_tcc_factor(self._h, _dev_ptr(A), _stream_ptr(stream)), "kl_tcc_factor")
+        return A
+
+    def build(self, stream=None):
+        """The N x N TCC as a torch tensor (..., 2) of float32 (fast) or float64 (FP64)."""
+        import torch
+        dt = torch.float32 if self.precision == PREC_FAST else torch.float64
+        T = torch.empty((self.N, self.N, 2), dtype=dt, device="cuda")
+        check(lib().kl_tcc_build(self._h, _dev_ptr(T), _stream_ptr(stream)), "kl_tcc_build")
+        return T
+
+    def minmax(self, T, stream=None):
+        out = (ctypes.c_double * 4)()
+        check(lib().kl_tcc_minmax(self._h, _dev_ptr(T), out, _stream_ptr(stream)), "kl_tcc_minmax")
+        return list(out)
+
+    def topk(self, nk: int, block: int = 0):
+        """(kernels nk x N complex64 in the reference layout, scales float32,
+        eigenvalues float64, iterations)."""
+        re = np.zeros(nk * self.N, dtype=np.float32)
+        im = np.zeros(nk * self.N, dtype=np.float32)
+        sc = np.zeros(nk, dtype=np.float32)
+        ev = np.zeros(nk, dtype=np.float64)
+        it = ctypes.c_int()
+        check(lib().kl_topk_eig(self._h, int(nk), int(block), _fp(re), _fp(im), _fp(sc),
+                                ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                ctypes.byref(it)), "kl_topk_eig")
+        k = (re + 1j * im).astype(np.complex64).reshape(nk, self.N)
+        return k, sc, ev, it.value
+
+    def hopkins(self, masks_dev, images_dev, nclips: int | None = None, stream=None) -> None:
+        n = masks_dev.shape[0] if nclips is None else nclips
+        check(lib().kl_hopkins_image(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(images_dev),
+                                     _stream_ptr(stream)), "kl_hopkins_image")

@@ -1,0 +1,148 @@
+"""Drop-in CLIs (klitho_tcc, klitho_socs) against the reference programs.
+
+CPU tests: argument validation and error messages (these paths exit before
+any GPU work).  GPU tests: the same command lines run through the reference
+build (oracle/_ref, FFT shim + LAPACK forwarder) and through k-litho_b200/bin,
+output files compared -- image.bin within 1e-5 of clear field, kernel_info.txt
+format identical, kernels compared as weighted projectors.
+"""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+import klitho as K
+import synth
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BIN = os.path.join(REPO, "k-litho_b200", "bin")
+REFBIN = os.path.join(REPO, "oracle", "_ref")
+GOLDEN = os.path.join(REPO, "tests", "golden")
+
+
+def run(exe, args, cwd, env=None):
+    e = dict(os.environ)
+    if env:
+        e.update(env)
+    return subprocess.run([exe] + [str(a) for a in args], cwd=cwd, capture_output=True, text=True,
+                          env=e, timeout=600)
+
+
+def workdir(tmp_path, name):
+    d = tmp_path / name
+    (d / "out" / "kernels" / "png").mkdir(parents=True)
+    return d
+
+
+def tcc_args(Lx, msx, maskfile, srcType="Annular", NA=0.8, defocus=0.2, nk=8, srcSize=41):
+    return [Lx, Lx, msx, msx, "Import", 128, 128, 0, maskfile, srcSize, srcType, 0.6, 0.9, 0.1,
+            0.5, 1, 0.6, 0.2, "none", NA, defocus, nk]
+
+
+@pytest.mark.parametrize("args,msg", [
+    ([1, 2, 3], "Expected 23 arguments"),
+    (tcc_args(256, 512, "m.bin"), "Invalid input parameters"),
+    (tcc_args(256, 128, "m.bin", NA=1.2), "NA must be in the range [0, 1]"),
+])
+def test_tcc_cli_rejects_bad_arguments(tmp_path, args, msg):
+    r = run(os.path.join(BIN, "klitho_tcc"), args, tmp_path)
+    assert r.returncode == 1 and msg in r.stderr
+
+
+@pytest.mark.parametrize("args,msg", [
+    ([1, 2], "Expected 11 arguments"),
+    ([256, 256, 300, 300, "LineSpace", 10, 10, 0, "x", "k/"], "Invalid input parameters"),
+])
+def test_socs_cli_rejects_bad_arguments(tmp_path, args, msg):
+    r = run(os.path.join(BIN, "klitho_socs"), args, tmp_path)
+    assert r.returncode == 1 and msg in r.stderr
+
+
+def test_socs_cli_even_kernel_size_is_an_error(tmp_path):
+    kd = tmp_path / "k"
+    kd.mkdir()
+    K.writeKernelInfo(str(kd / "kernel_info.txt"), 32, 33, [1.0])
+    r = run(os.path.join(BIN, "klitho_socs"),
+            [256, 256, 128, 128, "LineSpace", 10, 10, 0, "x", str(kd) + "/"], tmp_path)
+    assert r.returncode == 1 and "Kernel size must be odd" in r.stderr
+
+
+def read_kernel_dir(d):
+    kx, ky, nk, sc = K.readKernelInfo(os.path.join(d, "kernel_info.txt"))
+    n = kx * ky
+    ks = []
+    for i in range(nk):
+        re = np.fromfile(os.path.join(d, f"krn_{i}_r.bin"), dtype=np.float32)
+        im = np.fromfile(os.path.join(d, f"krn_{i}_i.bin"), dtype=np.float32)
+        assert re.size == n and im.size == n
+        ks.append(re.astype(np.complex128) + 1j * im)
+    return kx, ky, np.array(ks), sc
+
+
+@pytest.mark.gpu
+def test_tcc_cli_matches_reference_program(tmp_path, ref_built):
+    L, ms = 512, 256
+    mask = synth.rect_mask(ms, 12, seed=21)
+    mfile = tmp_path / "mask.bin"
+    mask.astype(np.float32).tofile(mfile)
+    args = tcc_args(L, ms, str(mfile))
+    dref, dours = workdir(tmp_path, "ref"), workdir(tmp_path, "ours")
+    rr = run(os.path.join(REFBIN, "klitho_tcc"), args, dref)
+    ro = run(os.path.join(BIN, "klitho_tcc"), args, dours)
+    assert rr.returncode == 0, rr.stderr
+    assert ro.returncode == 0, ro.stderr
+    # console: same parameter block and the same TCC band
+    for key in ("Nx: ", "TCC Size: ", "Number of Kernels: ", "Wavelength: ", "NA: "):
+        lr = [l for l in rr.stdout.splitlines() if l.startswith(key)]
+        lo = [l for l in ro.stdout.splitlines() if l.startswith(key)]
+        assert lr == lo, (key, lr, lo)
+    ir = np.fromfile(dref / "out" / "image.bin", dtype=np.float32)
+    io = np.fromfile(dours / "out" / "image.bin", dtype=np.float32)
+    assert ir.size == io.size == L * L
+    assert np.abs(ir - io).max() <= 1e-5
+    kxr, kyr, kr, sr = read_kernel_dir(dref / "out" / "kernels")
+    kxo, kyo, ko, so = read_kernel_dir(dours / "out" / "kernels")
+    assert (kxr, kyr) == (kxo, kyo) and len(sr) == len(so)
+    assert np.allclose(so, sr, rtol=2e-5, atol=1e-6 * sr[0])
+    Vr, Vo = kr.T, ko.T
+    Pr = (Vr * sr[None, :].astype(np.float64)) @ Vr.conj().T
+    Po = (Vo * so[None, :].astype(np.float64)) @ Vo.conj().T
+    assert np.linalg.norm(Po - Pr) / np.linalg.norm(Pr) <= 1e-5
+    # kernel_info.txt: identical layout line by line, eigenvalues to print precision
+    tr = (dref / "out" / "kernels" / "kernel_info.txt").read_text().splitlines()
+    to = (dours / "out" / "kernels" / "kernel_info.txt").read_text().splitlines()
+    assert len(tr) == len(to) and tr[:5] == to[:5]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kdir", ["shipped", "generated"])
+def test_socs_cli_matches_reference_program(tmp_path, ref_built, kdir):
+    L, ms = 512, 384
+    mask = synth.rect_mask(ms, 20, seed=5)
+    mfile = tmp_path / "mask.bin"
+    mask.astype(np.float32).tofile(mfile)
+    if kdir == "shipped":
+        kd = os.path.join(GOLDEN, "shipped_kernels")
+    else:
+        src = K.createSource(41, "Annular", 0.6, 0.9)
+        plan = K.TccPlan(src, 1.35, synth.defocus_arg(25.0), L, L, n_medium=1.44)
+        krn, sc, ev, _ = plan.topk(12)
+        kd = str(tmp_path / "kgen")
+        os.makedirs(kd)
+        for i in range(12):
+            krn[i].real.astype(np.float32).tofile(os.path.join(kd, f"krn_{i}_r.bin"))
+            krn[i].imag.astype(np.float32).tofile(os.path.join(kd, f"krn_{i}_i.bin"))
+        K.writeKernelInfo(os.path.join(kd, "kernel_info.txt"), 2 * plan.Nx + 1, 2 * plan.Ny + 1, sc)
+    args = [L, L, ms, ms, "Import", 128, 128, 0, str(mfile), kd + "/"]
+    dref, dours = workdir(tmp_path, "ref"), workdir(tmp_path, "ours")
+    rr = run(os.path.join(REFBIN, "klitho_socs"), args, dref)
+    ro = run(os.path.join(BIN, "klitho_socs"), args, dours)
+    assert rr.returncode == 0, rr.stderr
+    assert ro.returncode == 0, ro.stderr
+    ir = np.fromfile(dref / "out" / "image.bin", dtype=np.float32)
+    io = np.fromfile(dours / "out" / "image.bin", dtype=np.float32)
+    _, _, _, sc = K.readKernelInfo(os.path.join(kd, "kernel_info.txt"))
+    cf = float(np.abs(ir).max())
+    assert np.abs(ir - io).max() <= 1e-5 * max(cf, 1.0)
