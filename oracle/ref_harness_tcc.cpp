@@ -21,6 +21,19 @@
 using namespace std;
 typedef complex<double> Complex;
 
+// calcKernels (klitho_tcc.cpp:312) allocates zheevr's W with m entries while
+// LAPACK documents W as length N; inside a long-lived test process the
+// difference corrupts the heap.  Array allocations made by the reference code
+// in this library get slack at the end so such writes stay inside them.
+// Results are unaffected.
+void* operator new[](size_t n) {
+  void* p = std::malloc(n + (1u << 20));
+  if (!p) throw std::bad_alloc();
+  return p;
+}
+void operator delete[](void* p) noexcept { std::free(p); }
+void operator delete[](void* p, size_t) noexcept { std::free(p); }
+
 // Prototypes of functions defined in K-Litho-TCC/klitho_tcc.cpp (line of
 // definition in parentheses); the signatures must match to link.
 void FT_r2c(vector<float>& in, vector<Complex>& out, int sizeX, int sizeY, fftw_plan& fwd,
@@ -55,7 +68,9 @@ int kref_create_source(int srcSize, const char* type, float innerR, float outerR
   pt.y = ptY;
   stringstream ss;
   createSource(src, srcSize, string(type), an, di, cq, pt, string(file ? file : ""), ss);
-  memcpy(out, src.data(), sizeof(float) * src.size());
+  // an imported file can leave the vector longer than srcSize^2
+  // (readFloatArrayFromBinary sizes it by the byte count, file_io.cpp:245)
+  memcpy(out, src.data(), sizeof(float) * (size_t)srcSize * srcSize);
   return 0;
 }
 
@@ -115,7 +130,10 @@ int kref_hopkins_image(const float* mask, const double* tcc_in, int Lx, int Ly, 
   vector<Complex> tcc((size_t)N * N);
   memcpy(tcc.data(), tcc_in, sizeof(Complex) * tcc.size());
   vector<double> realDataLxy(Lxy, 0);
-  vector<Complex> complexDataLxy(Ly * (Lx / 2 + 1), 0);
+  // FT_c2r (klitho_tcc.cpp:162-167) stores the nx = -1 column one row ahead,
+  // which for the last row is Lx/2-2 elements past the buffer: the slack
+  // keeps that (zero-valued) store inside this allocation
+  vector<Complex> complexDataLxy(Ly * (Lx / 2 + 1) + Lx, 0);
   fftw_plan r2c = fftw_plan_dft_r2c_2d(Ly, Lx, realDataLxy.data(),
                                        reinterpret_cast<fftw_complex*>(complexDataLxy.data()),
                                        FFTW_ESTIMATE);
