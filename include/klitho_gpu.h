@@ -95,6 +95,7 @@ int kl_read_kernel_info(const char* path, int* krnSizeX, int* krnSizeY, int* nk,
 /* ------------------------------------------------------------------------- */
 
 typedef struct kl_socs_plan_s* kl_socs_plan;
+typedef struct kl_tcc_plan_s* kl_tcc_plan; /* see the TCC section below */
 
 /* Plan for clips of period Lx x Ly imaged with `nsets` kernel sets (e.g. one
  * per focus) of `nk` kernels of band (2Nx+1) x (2Ny+1), for batches of up to
@@ -122,6 +123,33 @@ int kl_socs_forward(kl_socs_plan plan, const float* masks_dev, int nclips, float
 int kl_socs_forward_host(kl_socs_plan plan, const float* masks_host, int nclips,
                          float* images_host, void* stream);
 
+/* ------------------------------------------------------------------------- */
+/* Adjoint (VJP) of SOCS imaging under a sigmoid resist and an L2 loss.       */
+/* No counterpart in the reference.                                            */
+/* ------------------------------------------------------------------------- */
+
+/* A SOCS plan that also supports kl_socs_vjp (taller strips so the band of
+ * dL/dI fits; clips up to 1024^2 at NA 1.35).  Its kl_socs_forward gives the
+ * same images as kl_socs_plan_create's. */
+int kl_socs_plan_create_adjoint(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk,
+                                int nsets, int max_clips);
+
+/* loss[c*nsets+s] = sum_x (sigmoid(alpha (I - threshold)) - target)^2 for the
+ * SOCS image I of clip c under kernel set s, and grad_dev[c] = dL/dmask
+ * summed over the sets (nclips x Ly x Lx float32).  images_dev may be NULL
+ * (the image is then not written).  The K coherent fields are recomputed on
+ * chip, never stored.  Stream-ordered; loss_dev is device memory. */
+int kl_socs_vjp(kl_socs_plan plan, const float* masks_dev, const float* targets_dev, int nclips,
+                float alpha, float threshold, float* images_dev, float* grad_dev,
+                double* loss_dev, void* stream);
+
+/* dL/dJ for the source map of `tcc` (srcSize^2 float32, zero where the map
+ * has no TCC source point), from the last kl_socs_vjp on this plan, summed
+ * over its clips.  Defined through the TCC factor A = sqrt(J) P (the Hopkins
+ * model): dL/dJ_s = sum_x dL/dI(x) |E_s(x)|^2.  One kernel set per plan;
+ * synchronous. */
+int kl_socs_vjp_source(kl_socs_plan plan, kl_tcc_plan tcc, float* grad_src_dev, void* stream);
+
 /* Stage timing for diagnostics and roofline accounting.  While enabled, every
  * kl_socs_forward records CUDA events on its stream around its three kernels
  * (mask forward transform, spectral core, image synthesis).
@@ -144,8 +172,6 @@ int kl_mask_spectrum(kl_socs_plan plan, const float* masks_dev, int nclips, floa
 
 #define KL_PREC_FAST 0 /* FP32 pupil factor, 3-term BF16 tensor-core TCC, FP64 Rayleigh-Ritz */
 #define KL_PREC_FP64 1 /* plain FP64 GPU path (pupil table from the host libm, FP64 TCC)    */
-
-typedef struct kl_tcc_plan_s* kl_tcc_plan;
 
 /* Optical setting of one TCC: source map (createSource output, host), NA,
  * defocus in the reference's normalised units (argv[21], dz = defocus *

@@ -52,8 +52,10 @@ struct SocsGeom {
 // Largest number of kernel slices the spectral stage splits a (clip, set) into.
 constexpr int kSocsMaxSplit = 8;
 
-// Fill geometry; returns KL_OK or KL_ERR_UNSUPPORTED with a message.
-int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g);
+// Fill geometry; returns KL_OK or KL_ERR_UNSUPPORTED with a message.  With
+// `adjoint`, strips are tall enough (J >= 4Ny+1) to carry the band of the
+// loss gradient dL/dI as well.
+int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g, bool adjoint = false);
 
 // Device workspace sizes.
 size_t socs_partial_bytes(const SocsGeom& g, int nclips);

@@ -1,0 +1,67 @@
+// kl_plans.h -- plan objects behind the opaque handles of include/klitho_gpu.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "kl_internal.h"
+#include "kl_tcc.h"
+
+struct kl_socs_plan_s {
+  kl::SocsGeom g{};
+  int K = 0, nsets = 0, max_clips = 0;
+  int device = 0;
+  bool adjoint = false;
+  float2* H = nullptr;       // nsets x K x nby x nbx
+  float* lam = nullptr;      // nsets x K
+  float2* partial = nullptr; // max_clips strip partials
+  float2* T = nullptr;       // intensity spectra (clip x set x kernel slice)
+  float2* tx = nullptr;      // plan-time twiddle tables
+  float2* ty = nullptr;
+  float* stage_in = nullptr; // host-entry staging (lazily allocated)
+  float* stage_out = nullptr;
+  size_t stage_clips = 0;
+  // adjoint state (kl_socs_plan_create_adjoint)
+  float2* gpart = nullptr;   // strip partials of the spectrum of dL/dI
+  float2* gam = nullptr;     // per-slice Gam partials
+  float2* Tg = nullptr;      // half-plane spectrum of dL/dm
+  int last_vjp_clips = 0;
+  // optional stage timing: 4 events per kl_socs_forward
+  bool timing = false;
+  std::vector<cudaEvent_t> events;
+};
+
+struct kl_tcc_plan_s {
+  int precision = KL_PREC_FAST;
+  int Lx = 0, Ly = 0, srcSize = 0;
+  float outerSigma = 0.f;
+  kl::PupilParams pp{};
+  std::vector<kl::SrcPoint> pts;
+  kl::SrcPoint* pts_dev = nullptr;
+  float2* A = nullptr;        // fast path: N x S FP32 factor
+  double2* P = nullptr;       // FP64 path: N x S pupil table (host libm)
+  float* J = nullptr;         // S weights (both paths)
+  int* src_id = nullptr;      // S source-map indices (both paths)
+  double2* tcc64 = nullptr;   // FP64 path: TCC (built on demand)
+  int* err = nullptr;
+  struct kl_socs_plan_s* hopkins = nullptr;  // SOCS plan of the Abbe form (lazy)
+  int hopkins_clips = 0;
+};
+
+namespace kl {
+// adjoint launchers (socs_vjp.cu)
+int vjp_supported(const SocsGeom& g);
+size_t vjp_gpart_bytes(const SocsGeom& g, int nimg);
+int vjp_launch_inverse(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T,
+                       int nclips, int nsets, int nsplit, const float* targets, float alpha,
+                       float thr, float* images, double* loss, float2* gpart, cudaStream_t st);
+int vjp_launch_spectral(const SocsGeom& g, const float2* partial, const float2* gpart, int nclips,
+                        const float2* H, const float* lam, int K, int nsets, int nsplit,
+                        float2* gam_out, cudaStream_t st);
+int vjp_launch_gradT(const SocsGeom& g, const float2* gam, int nclips, int nparts, float2* T,
+                     cudaStream_t st);
+int vjp_launch_source(const SocsGeom& g, const float2* partial, const float2* gpart, int nimg,
+                      int nsets, const float2* Hs, const float* Jw, const int* src_id, int S,
+                      int nsplit, float* grad_src, cudaStream_t st);
+}  // namespace kl

@@ -7,25 +7,7 @@
 #include <vector>
 
 #include "kl_internal.h"
-
-struct kl_socs_plan_s {
-  kl::SocsGeom g{};
-  int K = 0, nsets = 0, max_clips = 0;
-  int device = 0;
-  float2* H = nullptr;       // nsets x K x nby x nbx
-  float* lam = nullptr;      // nsets x K
-  float2* partial = nullptr; // max_clips strip partials
-  float2* T = nullptr;       // intensity spectra (clip x set x kernel slice)
-  float2* tx = nullptr;      // plan-time twiddle tables
-  float2* ty = nullptr;
-  float* stage_in = nullptr; // host-entry staging (lazily allocated)
-  float* stage_out = nullptr;
-  size_t stage_clips = 0;
-  // optional stage timing: 4 events per kl_socs_forward (start, after the
-  // forward, spectral and inverse kernels)
-  bool timing = false;
-  std::vector<cudaEvent_t> events;
-};
+#include "kl_plans.h"
 
 namespace {
 void drop_events(kl_socs_plan p) {
@@ -44,6 +26,9 @@ void free_plan(kl_socs_plan p) {
   cudaFree(p->ty);
   cudaFree(p->stage_in);
   cudaFree(p->stage_out);
+  cudaFree(p->gpart);
+  cudaFree(p->gam);
+  cudaFree(p->Tg);
   delete p;
 }
 
@@ -80,19 +65,17 @@ int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, c
   if (rc) return rc;
   return mark(p, st);
 }
-}  // namespace
-
-extern "C" {
-
-int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
-                        int max_clips) {
+int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
+                int max_clips, bool adjoint) {
   KL_CHECK_ARG(plan != nullptr, "kl_socs_plan_create: plan is NULL");
   *plan = nullptr;
   KL_CHECK_ARG(nk > 0 && nsets > 0 && max_clips > 0, "kl_socs_plan_create: nk, nsets, max_clips must be positive");
   kl::SocsGeom g;
-  int rc = kl::socs_geometry(Lx, Ly, Nx, Ny, &g);
+  int rc = kl::socs_geometry(Lx, Ly, Nx, Ny, &g, adjoint);
   if (rc) return rc;
+  if (adjoint && (rc = kl::vjp_supported(g))) return rc;
   kl_socs_plan p = new (std::nothrow) kl_socs_plan_s;
+  if (p) p->adjoint = adjoint;
   if (!p) {
     kl::set_error("kl_socs_plan_create: out of host memory");
     return KL_ERR_NOMEM;
@@ -122,6 +105,15 @@ int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int 
     free_plan(p);
     return rc;
   }
+  if (adjoint) {
+    const size_t nb2s = (size_t)g.nby * g.nbx;
+    if ((rc = alloc((void**)&p->gpart, kl::vjp_gpart_bytes(g, max_clips * nsets), "dL/dI partials")) ||
+        (rc = alloc((void**)&p->gam, sizeof(float2) * nb2s * tcap * nsets, "adjoint partials")) ||
+        (rc = alloc((void**)&p->Tg, sizeof(float2) * (size_t)max_clips * g.nty * g.ntx, "gradient spectra"))) {
+      free_plan(p);
+      return rc;
+    }
+  }
   if (cudaStreamSynchronize(nullptr) != cudaSuccess) {
     kl::set_error(std::string("kl_socs_plan_create: ") + cudaGetErrorString(cudaGetLastError()));
     free_plan(p);
@@ -130,6 +122,46 @@ int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int 
   cudaMemset(p->H, 0, sizeof(float2) * nb2 * nk * nsets);
   cudaMemset(p->lam, 0, sizeof(float) * (size_t)nk * nsets);
   *plan = p;
+  return KL_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
+                        int max_clips) {
+  return create_plan(plan, Lx, Ly, Nx, Ny, nk, nsets, max_clips, false);
+}
+
+int kl_socs_plan_create_adjoint(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk,
+                                int nsets, int max_clips) {
+  return create_plan(plan, Lx, Ly, Nx, Ny, nk, nsets, max_clips, true);
+}
+
+int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nclips, float alpha,
+                float threshold, float* images, float* grad, double* loss, void* stream) {
+  KL_CHECK_ARG(p && masks && targets && grad && loss, "kl_socs_vjp: NULL argument");
+  KL_CHECK_ARG(p->adjoint, "kl_socs_vjp: the plan was not created by kl_socs_plan_create_adjoint");
+  KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_socs_vjp: nclips exceeds the plan");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (nclips == 0) return KL_OK;
+  const kl::SocsGeom& g = p->g;
+  int rc;
+  const int ns1 = kl::socs_choose_split(g, nclips, p->nsets, p->K);
+  if ((rc = kl::socs_launch_forward(g, p->tx, p->ty, masks, nclips, p->partial, st))) return rc;
+  if ((rc = kl::socs_launch_spectral(g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, ns1, p->T, st)))
+    return rc;
+  KL_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(double) * (size_t)nclips * p->nsets, st));
+  if ((rc = kl::vjp_launch_inverse(g, p->tx, p->ty, p->T, nclips, p->nsets, ns1, targets, alpha,
+                                   threshold, images, loss, p->gpart, st)))
+    return rc;
+  const int ns2 = kl::socs_choose_split(g, nclips, p->nsets, p->K);
+  if ((rc = kl::vjp_launch_spectral(g, p->partial, p->gpart, nclips, p->H, p->lam, p->K, p->nsets,
+                                    ns2, p->gam, st)))
+    return rc;
+  if ((rc = kl::vjp_launch_gradT(g, p->gam, nclips, p->nsets * ns2, p->Tg, st))) return rc;
+  if ((rc = kl::socs_launch_inverse(g, p->tx, p->ty, p->Tg, nclips, 1, 1, grad, st))) return rc;
+  p->last_vjp_clips = nclips;
   return KL_OK;
 }
 

@@ -10,23 +10,8 @@
 #include <vector>
 
 #include "kl_internal.h"
+#include "kl_plans.h"
 #include "kl_tcc.h"
-
-struct kl_tcc_plan_s {
-  int precision = KL_PREC_FAST;
-  int Lx = 0, Ly = 0, srcSize = 0;
-  float outerSigma = 0.f;
-  kl::PupilParams pp{};
-  std::vector<kl::SrcPoint> pts;
-  kl::SrcPoint* pts_dev = nullptr;
-  float2* A = nullptr;        // fast path: N x S FP32 factor
-  double2* P = nullptr;       // FP64 path: N x S pupil table (host libm)
-  float* J = nullptr;         // FP64 path: S weights
-  double2* tcc64 = nullptr;   // FP64 path: TCC (built on demand)
-  int* err = nullptr;
-  kl_socs_plan hopkins = nullptr;  // SOCS plan of the Abbe form (lazy)
-  int hopkins_clips = 0;
-};
 
 namespace {
 void free_plan(kl_tcc_plan p) {
@@ -35,6 +20,7 @@ void free_plan(kl_tcc_plan p) {
   cudaFree(p->A);
   cudaFree(p->P);
   cudaFree(p->J);
+  cudaFree(p->src_id);
   cudaFree(p->tcc64);
   cudaFree(p->err);
   if (p->hopkins) kl_socs_plan_destroy(p->hopkins);
@@ -100,6 +86,21 @@ int kl_tcc_plan_create(kl_tcc_plan* plan, const float* src, int srcSize, double 
   }
   cudaMemset(p->err, 0, sizeof(int));
   const size_t NS = (size_t)pp.N * pp.S;
+  {
+    std::vector<float> Jh(pp.S);
+    std::vector<int> ids(pp.S);
+    for (int s = 0; s < pp.S; ++s) {
+      Jh[s] = p->pts[s].J;
+      ids[s] = p->pts[s].src_id;
+    }
+    if ((rc = dalloc((void**)&p->J, sizeof(float) * pp.S, "source weights")) ||
+        (rc = dalloc((void**)&p->src_id, sizeof(int) * pp.S, "source indices"))) {
+      free_plan(p);
+      return rc;
+    }
+    cudaMemcpy(p->J, Jh.data(), sizeof(float) * pp.S, cudaMemcpyHostToDevice);
+    cudaMemcpy(p->src_id, ids.data(), sizeof(int) * pp.S, cudaMemcpyHostToDevice);
+  }
   if (precision == KL_PREC_FAST) {
     if ((rc = dalloc((void**)&p->pts_dev, sizeof(kl::SrcPoint) * pp.S, "source points")) ||
         (rc = dalloc((void**)&p->A, sizeof(float2) * NS, "TCC factor"))) {
@@ -114,15 +115,11 @@ int kl_tcc_plan_create(kl_tcc_plan* plan, const float* src, int srcSize, double 
   } else {
     std::vector<double> P(2 * NS);
     kl::tcc_pupil_host(p->pts, pp, P.data());
-    std::vector<float> J(pp.S);
-    for (int s = 0; s < pp.S; ++s) J[s] = p->pts[s].J;
-    if ((rc = dalloc((void**)&p->P, sizeof(double2) * NS, "pupil table")) ||
-        (rc = dalloc((void**)&p->J, sizeof(float) * pp.S, "source weights"))) {
+    if ((rc = dalloc((void**)&p->P, sizeof(double2) * NS, "pupil table"))) {
       free_plan(p);
       return rc;
     }
     cudaMemcpy(p->P, P.data(), sizeof(double2) * NS, cudaMemcpyHostToDevice);
-    cudaMemcpy(p->J, J.data(), sizeof(float) * pp.S, cudaMemcpyHostToDevice);
   }
   if (cudaDeviceSynchronize() != cudaSuccess) {
     kl::set_error(std::string("kl_tcc_plan_create: ") + cudaGetErrorString(cudaGetLastError()));
@@ -308,6 +305,37 @@ int kl_hopkins_image(kl_tcc_plan p, const float* masks_dev, int nclips, float* i
     if (rc) return rc;
   }
   return kl_socs_forward(p->hopkins, masks_dev, nclips, images_dev, stream);
+}
+
+int kl_socs_vjp_source(kl_socs_plan sp, kl_tcc_plan tp, float* grad_src, void* stream) {
+  KL_CHECK_ARG(sp && tp && grad_src, "kl_socs_vjp_source: NULL argument");
+  KL_CHECK_ARG(sp->adjoint && sp->last_vjp_clips > 0, "kl_socs_vjp_source: run kl_socs_vjp first");
+  KL_CHECK_ARG(sp->nsets == 1, "kl_socs_vjp_source: one kernel set (one optical setting) per plan");
+  KL_CHECK_ARG(tp->precision == KL_PREC_FAST, "kl_socs_vjp_source: needs the fast-path TCC plan");
+  KL_CHECK_ARG(tp->pp.Nx == sp->g.Nx && tp->pp.Ny == sp->g.Ny && tp->Lx == sp->g.Lx && tp->Ly == sp->g.Ly,
+               "kl_socs_vjp_source: TCC plan and SOCS plan describe different bands");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int N = tp->pp.N, S = tp->pp.S, nimg = sp->last_vjp_clips;
+  float2* H = nullptr;
+  float* lam = nullptr;
+  int rc;
+  if ((rc = dalloc((void**)&H, sizeof(float2) * (size_t)N * S, "source kernels")) ||
+      (rc = dalloc((void**)&lam, sizeof(float) * S, "source weights"))) {
+    cudaFree(H);
+    return rc;
+  }
+  KL_CUDA_TRY(cudaMemsetAsync(grad_src, 0, sizeof(float) * (size_t)tp->srcSize * tp->srcSize, st));
+  rc = kl::tcc_factor_kernels(tp->A, N, S, H, lam, st);
+  int nsplit = 1;
+  while (nsplit < S && nimg * nsplit < 2 * 148) nsplit *= 2;
+  if (nsplit > S) nsplit = S;
+  if (!rc)
+    rc = kl::vjp_launch_source(sp->g, sp->partial, sp->gpart, nimg, sp->nsets, H, tp->J, tp->src_id,
+                               S, nsplit, grad_src, st);
+  cudaStreamSynchronize(st);
+  cudaFree(H);
+  cudaFree(lam);
+  return rc;
 }
 
 int kl_hopkins_image_host(kl_tcc_plan p, const float* mask_host, float* image_host) {

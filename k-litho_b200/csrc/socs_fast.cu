@@ -49,7 +49,7 @@ __host__ __device__ inline int pow2_at_least(int v) {
 }
 }  // namespace
 
-int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g) {
+int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g, bool adjoint) {
   if (Lx <= 0 || Ly <= 0 || Nx < 0 || Ny < 0) {
     set_error("socs_geometry: invalid sizes");
     return KL_ERR_INVALID;
@@ -90,10 +90,11 @@ int socs_geometry(int Lx, int Ly, int Nx, int Ny, SocsGeom* g) {
   }
   r.NBM = r.ntx <= 32 ? 32 : 64;
   r.KX = r.NBM > r.NFM ? r.NBM : r.NFM;
-  r.J = pow2_at_least(r.nby);
+  r.J = pow2_at_least(adjoint ? r.nty : r.nby);
   if (r.J < 32) r.J = 32;
-  if (r.J > 64 || Ly % r.J != 0) {
-    set_error("fast SOCS path needs Ly divisible by " + std::to_string(r.J) + " and Ny <= 31");
+  if (r.J > (adjoint ? 128 : 64) || Ly % r.J != 0) {
+    set_error("fast SOCS path needs Ly divisible by " + std::to_string(r.J) +
+              (adjoint ? " and 4Ny+1 <= 128" : " and Ny <= 31"));
     return KL_ERR_UNSUPPORTED;
   }
   r.nS = Ly / r.J;

@@ -86,6 +86,10 @@ def lib() -> ctypes.CDLL:
         L.kl_topk_eig.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _c_float_p, _c_float_p,
                                   _c_float_p, ctypes.POINTER(ctypes.c_double), _c_int_p]
         L.kl_hopkins_image.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+        L.kl_socs_plan_create_adjoint.argtypes = L.kl_socs_plan_create.argtypes
+        L.kl_socs_vjp.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                  _vp, _vp, _vp, _vp]
+        L.kl_socs_vjp_source.argtypes = [_vp, _vp, _vp, _vp]
         L.kl_socs_enable_timing.argtypes = [_vp, ctypes.c_int]
         L.kl_socs_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), _c_int_p]
         _LIB = L
@@ -194,13 +198,13 @@ class SocsPlan:
     """GPU SOCS imaging for clips of one period (calcSOCS + FI on device)."""
 
     def __init__(self, Lx: int, Ly: int, Nx: int, Ny: int, nk: int, nsets: int = 1,
-                 max_clips: int = 1):
+                 max_clips: int = 1, adjoint: bool = False):
         self.Lx, self.Ly, self.Nx, self.Ny = int(Lx), int(Ly), int(Nx), int(Ny)
         self.nk, self.nsets, self.max_clips = int(nk), int(nsets), int(max_clips)
         h = _vp()
-        check(lib().kl_socs_plan_create(ctypes.byref(h), self.Lx, self.Ly, self.Nx, self.Ny,
-                                        self.nk, self.nsets, self.max_clips),
-              "kl_socs_plan_create")
+        create = lib().kl_socs_plan_create_adjoint if adjoint else lib().kl_socs_plan_create
+        check(create(ctypes.byref(h), self.Lx, self.Ly, self.Nx, self.Ny, self.nk, self.nsets,
+                     self.max_clips), "kl_socs_plan_create")
         self._h = h
 
     def close(self) -> None:
@@ -237,6 +241,20 @@ class SocsPlan:
         check(lib().kl_socs_forward_host(self._h, _fp(m), int(n), _fp(images),
                                          _stream_ptr(stream)), "kl_socs_forward_host")
         return images
+
+    def vjp(self, masks_dev, targets_dev, grad_dev, loss_dev, images_dev=None, alpha=50.0,
+            threshold=0.225, nclips: int | None = None, stream=None) -> None:
+        """Adjoint of imaging + sigmoid resist + L2 loss (kl_socs_vjp)."""
+        n = masks_dev.shape[0] if nclips is None else nclips
+        check(lib().kl_socs_vjp(self._h, _dev_ptr(masks_dev), _dev_ptr(targets_dev), int(n),
+                                float(alpha), float(threshold),
+                                _dev_ptr(images_dev) if images_dev is not None else None,
+                                _dev_ptr(grad_dev), _dev_ptr(loss_dev), _stream_ptr(stream)),
+              "kl_socs_vjp")
+
+    def vjp_source(self, tcc_plan, grad_src_dev, stream=None) -> None:
+        check(lib().kl_socs_vjp_source(self._h, tcc_plan._h, _dev_ptr(grad_src_dev),
+                                       _stream_ptr(stream)), "kl_socs_vjp_source")
 
     def enable_timing(self, on: bool = True) -> None:
         check(lib().kl_socs_enable_timing(self._h, int(bool(on))), "kl_socs_enable_timing")

@@ -353,3 +353,85 @@ def ref_socs_image(mask, krn_r, krn_i, scales, Nx, Ny) -> np.ndarray:
     ref_socs().kref_socs_image(_fp(m), Lx, Ly, _fp(kr), _fp(ki), _fp(sc), len(sc), int(Nx),
                                int(Ny), _fp(out))
     return out
+
+
+# ---------------------------------------------------------------------------
+# FP64 reference of the SOCS adjoint (no counterpart in the reference):
+# the forward model restated with torch complex128 FFTs on the CPU, the loss
+# L = sum (sigmoid(alpha (I - c)) - t)^2, gradients by autograd.
+# ---------------------------------------------------------------------------
+
+def _band_index(L, N):
+    import torch
+    return torch.arange(-N, N + 1) % L
+
+
+def socs_fields_torch(mask, krn, Nx, Ny):
+    """Coherent fields E_k on the full Lx x Ly grid (complex128), the
+    band-limited evaluation the reference's calcSOCS + FI produces."""
+    import torch
+    m = mask if isinstance(mask, torch.Tensor) else torch.as_tensor(mask, dtype=torch.float64)
+    Ly, Lx = m.shape
+    D = torch.fft.fft2(m.to(torch.float64))
+    iy, ix = _band_index(Ly, Ny), _band_index(Lx, Nx)
+    M = D[iy][:, ix] / (Lx * Ly)
+    H = torch.as_tensor(np.asarray(krn, dtype=np.complex128)).reshape(-1, 2 * Ny + 1, 2 * Nx + 1)
+    # odd periods: the reference's shifts place the image one pixel later
+    dy, dx = 2 * ((Ly + 1) // 2) - Ly, 2 * ((Lx + 1) // 2) - Lx
+    fy = torch.arange(-Ny, Ny + 1, dtype=torch.float64)[:, None]
+    fx = torch.arange(-Nx, Nx + 1, dtype=torch.float64)[None, :]
+    ph = torch.exp(-2j * np.pi * (fy * dy / Ly + fx * dx / Lx))
+    C = H * (M * ph)[None]
+    full = torch.zeros((H.shape[0], Ly, Lx), dtype=torch.complex128)
+    full[:, iy[:, None], ix[None, :]] = C
+    return torch.fft.ifft2(full) * (Lx * Ly)
+
+
+def socs_image_torch(mask, krn, scales, Nx, Ny):
+    import torch
+    E = socs_fields_torch(mask, krn, Nx, Ny)
+    lam = torch.as_tensor(np.asarray(scales, dtype=np.float64))
+    return (lam[:, None, None] * (E.real ** 2 + E.imag ** 2)).sum(0)
+
+
+def resist_loss_torch(I, target, alpha=50.0, thr=0.225):
+    import torch
+    t = torch.as_tensor(np.asarray(target, dtype=np.float64))
+    s = torch.sigmoid(alpha * (I - thr))
+    return ((s - t) ** 2).sum()
+
+
+def socs_vjp_reference(mask, target, krn, scales, Nx, Ny, alpha=50.0, thr=0.225):
+    """(loss, dL/dmask, image, dL/dI) in FP64."""
+    import torch
+    m = torch.as_tensor(np.asarray(mask, dtype=np.float64)).clone().requires_grad_(True)
+    I = socs_image_torch(m, krn, scales, Nx, Ny)
+    I.retain_grad()
+    L = resist_loss_torch(I, target, alpha, thr)
+    L.backward()
+    return float(L.detach()), m.grad.numpy(), I.detach().numpy(), I.grad.numpy()
+
+
+def socs_loss(mask, target, krn, scales, Nx, Ny, alpha=50.0, thr=0.225):
+    import torch
+    with torch.no_grad():
+        I = socs_image_torch(torch.as_tensor(np.asarray(mask, dtype=np.float64)), krn, scales, Nx, Ny)
+        return float(resist_loss_torch(I, target, alpha, thr))
+
+
+def source_gradient_reference(mask, dLdI, P, J, Nx, Ny):
+    """dL/dJ_s = sum_x dL/dI(x) |E_s(x)|^2 with E_s from conj(P[:, s]) (the
+    Hopkins/Abbe fields of calcImage's convention)."""
+    E = socs_fields_torch(mask, np.conj(P).T, Nx, Ny).numpy()
+    return np.einsum("yx,syx->s", dLdI, E.real ** 2 + E.imag ** 2)
+
+
+def hopkins_loss(mask, target, P, J, Nx, Ny, alpha=50.0, thr=0.225):
+    """Loss of the full Hopkins image sum_s J_s |E_s|^2 (for finite differences
+    of the source weights)."""
+    import torch
+    with torch.no_grad():
+        E = socs_fields_torch(mask, np.conj(P).T, Nx, Ny)
+        I = (torch.as_tensor(np.asarray(J, dtype=np.float64))[:, None, None] *
+             (E.real ** 2 + E.imag ** 2)).sum(0)
+        return float(resist_loss_torch(I, target, alpha, thr))
