@@ -160,6 +160,23 @@ int kl_socs_vjp_source(kl_socs_plan plan, kl_tcc_plan tcc, float* grad_src_dev, 
 int kl_socs_enable_timing(kl_socs_plan plan, int enable);
 int kl_socs_stage_times(kl_socs_plan plan, double* ms, int* launches);
 
+/* SOCS images without any memory allocation.  No counterpart in the
+ * reference.  For callers that may not allocate device memory at run time
+ * (a fixed memory budget handed over at start-up, a framework that owns the
+ * allocator, code where cudaMalloc would synchronise or fail): the caller
+ * passes every buffer -- masks (nclips x Ly x Lx float32), kernels in the
+ * kernel layout as interleaved c64 (nk x (2Ny+1)(2Nx+1)), nk float scales,
+ * images (nclips x Ly x Lx float32), all device memory -- and the scratch
+ * comes from one static 8 MiB device array inside the library (about 38 clips
+ * of 1024^2 per call; larger requests return KL_ERR_INVALID with the sizes in
+ * kl_last_error).  The first call on each device looks up that array's
+ * device address; make it before any stream capture.  Calls share the array,
+ * so calls that overlap on the GPU race and must be serialised by the
+ * caller.  Same results as kl_socs_forward with one kernel set. */
+int kl_socs_forward_noalloc(const float* masks_dev, int nclips, int Lx, int Ly, int Nx, int Ny,
+                            const float* kernels_dev, const float* scales_dev, int nk,
+                            float* images_dev, void* stream);
+
 /* The band of FT_r2c (K-Litho-TCC/klitho_tcc.cpp:97-148): centred spectrum
  * scaled by 1/(Lx Ly), cropped to the kernel band; band_dev receives nclips
  * c64 arrays in the kernel layout.  Stream-ordered. */
