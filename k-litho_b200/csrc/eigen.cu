@@ -41,12 +41,22 @@ enum GemmMode {
   G_DX = 2,    // a = T64[m][k] (double2),                   b = X[k][n]
   G_FX = 3,    // a = T32[m][k] (float2),                    b = X[k][n]
   G_HH = 4,    // a = conj(W[k][m]),                         b = V[k][n]   (W^H V)
-  G_NN = 5     // a = W[m][k],                               b = R[k][n]
+  G_NN = 5,    // a = W[m][k],                               b = R[k][n]
+  G_AHA = 6    // a = conj(A32[k][m]),                       b = A32[k][n] (FP64 Gram of A)
 };
 
 template <int MODE>
+__device__ __forceinline__ double2 load_b(const void* B, int ldb, int k, int n) {
+  if (MODE == G_AHA) {
+    const float2 v = reinterpret_cast<const float2*>(B)[(size_t)k * ldb + n];
+    return make_double2(v.x, v.y);
+  }
+  return reinterpret_cast<const double2*>(B)[(size_t)k * ldb + n];
+}
+
+template <int MODE>
 __device__ __forceinline__ double2 load_a(const void* A, int lda, int m, int k) {
-  if (MODE == G_AHX) {
+  if (MODE == G_AHX || MODE == G_AHA) {
     float2 v = reinterpret_cast<const float2*>(A)[(size_t)k * lda + m];
     return make_double2(v.x, -v.y);
   } else if (MODE == G_AY || MODE == G_FX) {
@@ -62,7 +72,7 @@ __device__ __forceinline__ double2 load_a(const void* A, int lda, int m, int k) 
 
 template <int MODE>
 __global__ void __launch_bounds__(256) k_zgemm(const void* __restrict__ A, int lda,
-                                               const double2* __restrict__ Bm, int ldb,
+                                               const void* __restrict__ Bm, int ldb,
                                                double2* __restrict__ C, int ldc, int M, int N,
                                                int K, int accumulate) {
   constexpr int TM = 32, TN = 32, TK = 16;
@@ -84,7 +94,7 @@ __global__ void __launch_bounds__(256) k_zgemm(const void* __restrict__ A, int l
     for (int i = threadIdx.x; i < TK * TN; i += 256) {
       const int kk = i / TN, nn = i - kk * TN;
       const int n = n0 + nn, k = k0 + kk;
-      sb[kk][nn] = (n < N && k < kend) ? Bm[(size_t)k * ldb + n] : make_double2(0.0, 0.0);
+      sb[kk][nn] = (n < N && k < kend) ? load_b<MODE>(Bm, ldb, k, n) : make_double2(0.0, 0.0);
     }
     __syncthreads();
 #pragma unroll
@@ -116,7 +126,7 @@ __global__ void __launch_bounds__(256) k_zgemm(const void* __restrict__ A, int l
 }
 
 template <int MODE>
-int zgemm(const void* A, int lda, const double2* Bm, int ldb, double2* C, int ldc, int M, int N,
+int zgemm(const void* A, int lda, const void* Bm, int ldb, double2* C, int ldc, int M, int N,
           int K, cudaStream_t st) {
   const int gx = (M + 31) / 32, gy = (N + 31) / 32;
   int gz = 1;
@@ -204,134 +214,301 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double2* __restrict__ G,
 }
 
 // Hermitian eigensolve H = Q diag(w) Q^H by cyclic Jacobi with the
-// round-robin (tournament) ordering: B/2 disjoint rotations per step.
-// H row-major B x B (overwritten), Q row-major B x B (columns = vectors,
-// kept in global memory), w descending on return (vectors permuted).
-__global__ void __launch_bounds__(256) k_jacobi(double2* __restrict__ Hg, int B,
-                                                double2* __restrict__ Q, double* __restrict__ w,
-                                                int max_sweeps, int* __restrict__ sweeps_out) {
-  extern __shared__ double2 sm[];
-  const int Bp = B + (B & 1);
-  double2* H = sm;                                        // Bp x Bp
-  int* pr = reinterpret_cast<int*>(H + (size_t)Bp * Bp);  // Bp ring
-  double* pc = reinterpret_cast<double*>(pr + Bp + (Bp & 1));  // per pair: c, s, phase re, im
-  __shared__ double s_off, s_diag;
-  __shared__ int s_done;
-  for (int t = threadIdx.x; t < Bp * Bp; t += blockDim.x) {
-    const int i = t / Bp, j = t % Bp;
-    H[t] = (i < B && j < B) ? Hg[(size_t)i * B + j] : make_double2(0.0, 0.0);
+// round-robin (circle) ordering: Bp/2 disjoint rotations per step, pairs in
+// closed form.  One CTA per matrix keeps H in shared memory (or works on it in
+// place in global memory when it is too large) and applies each step as
+// independent two-sided 2 x 2 block updates U_a^H H[a, b] U_b over all pairs
+// of pairs, writing the rotations to a log.  The eigenvectors Q = prod U are
+// formed afterwards from the log by k_jacobi_vectors, one warp per row of Q,
+// so the sequential sweep loop touches only H.  A launch takes a batch of
+// independent matrices (one CTA each), e.g. the TCCs of several focus values.
+constexpr int kJacobiThreads = 1024;
+constexpr int kJacobiMaxSweeps = 40;
+constexpr int kJacobiMaxJobs = 16;
+constexpr int kGramMaxS = 128;  // factor widths solved by one Gram eigensolve
+
+struct JacobiJob {
+  double2* H;    // B x B Hermitian input (overwritten when worked in place)
+  double4* rot;  // rotation log, jacobi_log_elems(B)
+  double2* Q;    // B x B output, column j = eigenvector j
+  double* w;     // B eigenvalues, descending
+  int* jst;      // [0] steps applied, [1 + i] rank of diagonal entry i
+  int B;
+};
+struct JacobiJobs {
+  JacobiJob j[kJacobiMaxJobs];
+};
+
+__device__ __forceinline__ void jacobi_pair(int t, int i, int Bp, int& p, int& q) {
+  const int m = Bp - 1;
+  if (i == 0) {
+    p = 0;
+    q = 1 + t % m;
+  } else {
+    p = 1 + (t + i) % m;
+    q = 1 + (t - i + m) % m;
   }
-  for (int t = threadIdx.x; t < Bp * Bp; t += blockDim.x) {
-    const int i = t / Bp, j = t % Bp;
-    if (i < B && j < B) Q[(size_t)i * B + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  if (p > q) {
+    const int x = p;
+    p = q;
+    q = x;
   }
-  for (int i = threadIdx.x; i < Bp; i += blockDim.x) pr[i] = i;
-  __syncthreads();
+}
+
+// the (p, q) of pair t at step i of a sweep, for all steps (bytes: B <= 128)
+__device__ void jacobi_pair_table(uchar2* tab, int Bp) {
   const int npairs = Bp / 2;
-  int sweep = 0;
+  for (int i = threadIdx.x; i < (Bp - 1) * npairs; i += blockDim.x) {
+    const int step = i / npairs, t = i - step * npairs;
+    int p, q;
+    jacobi_pair(step, t, Bp, p, q);
+    tab[i] = make_uchar2((unsigned char)p, (unsigned char)q);
+  }
+}
+
+struct JacobiSmem {
+  int npairs, nblocks;
+  size_t pc, pt, bt, h, total_no_h;
+  __host__ __device__ explicit JacobiSmem(int B) {
+    const int Bp = B + (B & 1);
+    npairs = Bp / 2;
+    nblocks = npairs * (npairs + 1) / 2;
+    pc = 0;                                                   // npairs double4
+    pt = pc + sizeof(double4) * npairs;                       // (Bp - 1) x npairs uchar2
+    bt = pt + sizeof(uchar2) * (Bp - 1) * npairs;             // nblocks ushort
+    h = (bt + sizeof(unsigned short) * nblocks + 15) & ~size_t(15);
+    total_no_h = h;
+  }
+};
+
+// rotation zeroing b = H[p][q] given a = H[p][p], d = H[q][q]:
+// (c, s, Re e, Im e) with e = b / |b|, t = s / c = sgn(th) / (|th| + sqrt(th^2 + 1)),
+// th = (d - a) / (2 |b|); *tb = t |b| moves the diagonal (a - t|b|, d + t|b|)
+__device__ __forceinline__ double4 jacobi_rotation(double a, double d, double2 b, double* tb) {
+  const double b2 = b.x * b.x + b.y * b.y;
+  if (b2 > 1e-300 && b2 > 1e-36 * fabs(a * d)) {
+    const double r = rsqrt(b2);
+    const double th = 0.5 * (d - a) * r;
+    const double tt = copysign(1.0, th) / (fabs(th) + sqrt(fma(th, th, 1.0)));
+    const double c = rsqrt(fma(tt, tt, 1.0));
+    *tb = tt * (b2 * r);
+    return make_double4(c, tt * c, b.x * r, b.y * r);
+  }
+  *tb = 0.0;
+  return make_double4(1.0, 0.0, 1.0, 0.0);
+}
+
+// rows (p1, q1) rotated by u1 from the left (U1^H .), columns (p2, q2) by u2
+__device__ __forceinline__ void rot_block(double2& x00, double2& x01, double2& x10, double2& x11, double4 u1,
+                                          double4 u2) {
+  // right: Y[:,0] = c2 X[:,0] - s2 conj(e2) X[:,1];  Y[:,1] = s2 X[:,0] + c2 conj(e2) X[:,1]
+  const double2 e2c = make_double2(u2.z, -u2.w);
+  const double2 a1 = zmul(x01, e2c), b1 = zmul(x11, e2c);
+  const double2 y00 = make_double2(u2.x * x00.x - u2.y * a1.x, u2.x * x00.y - u2.y * a1.y);
+  const double2 y01 = make_double2(u2.y * x00.x + u2.x * a1.x, u2.y * x00.y + u2.x * a1.y);
+  const double2 y10 = make_double2(u2.x * x10.x - u2.y * b1.x, u2.x * x10.y - u2.y * b1.y);
+  const double2 y11 = make_double2(u2.y * x10.x + u2.x * b1.x, u2.y * x10.y + u2.x * b1.y);
+  // left: Z[0,:] = c1 Y[0,:] - s1 e1 Y[1,:];  Z[1,:] = s1 Y[0,:] + c1 e1 Y[1,:]
+  const double2 e1 = make_double2(u1.z, u1.w);
+  const double2 g0 = zmul(y10, e1), g1 = zmul(y11, e1);
+  x00 = make_double2(u1.x * y00.x - u1.y * g0.x, u1.x * y00.y - u1.y * g0.y);
+  x01 = make_double2(u1.x * y01.x - u1.y * g1.x, u1.x * y01.y - u1.y * g1.y);
+  x10 = make_double2(u1.y * y00.x + u1.x * g0.x, u1.y * y00.y + u1.x * g0.y);
+  x11 = make_double2(u1.y * y01.x + u1.x * g1.x, u1.y * y01.y + u1.x * g1.y);
+}
+
+// one 2 x 2 block (pair t1 rows, pair t2 columns, t1 <= t2) of a step; the
+// rotated entries are left in x.. for the caller
+__device__ __forceinline__ void jacobi_block(double2* H, int B, uchar2 pr, uchar2 pcl, bool diag, double4 u1,
+                                             double4 u2, double2& x00, double2& x01, double2& x10,
+                                             double2& x11) {
+  const int rx = pr.x, ry = pr.y, cx = pcl.x, cy = pcl.y;
+  const bool rq = ry < B, cq = cy < B;
+  const double2 z = make_double2(0.0, 0.0);
+  x00 = H[rx * B + cx];
+  x01 = cq ? H[rx * B + cy] : z;
+  x10 = rq ? H[ry * B + cx] : z;
+  x11 = (rq && cq) ? H[ry * B + cy] : z;
+  rot_block(x00, x01, x10, x11, u1, u2);
+  if (diag) {
+    H[rx * B + rx] = make_double2(x00.x, 0.0);
+    if (rq) {
+      H[rx * B + ry] = z;
+      H[ry * B + rx] = z;
+      H[ry * B + ry] = make_double2(x11.x, 0.0);
+    }
+  } else {
+    H[rx * B + cx] = x00;
+    H[cx * B + rx] = zconj(x00);
+    if (cq) {
+      H[rx * B + cy] = x01;
+      H[cy * B + rx] = zconj(x01);
+    }
+    if (rq) {
+      H[ry * B + cx] = x10;
+      H[cx * B + ry] = zconj(x10);
+    }
+    if (rq && cq) {
+      H[ry * B + cy] = x11;
+      H[cy * B + ry] = zconj(x11);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiJobs jobs, int h_in_smem, int max_sweeps) {
+  extern __shared__ __align__(16) unsigned char jsm[];
+  const JacobiJob job = jobs.j[blockIdx.x];
+  const int B = job.B;
+  double4* __restrict__ rot = job.rot;
+  const JacobiSmem L(B);
+  const int Bp = B + (B & 1), npairs = L.npairs, nblocks = L.nblocks;
+  double4* pc = reinterpret_cast<double4*>(jsm + L.pc);
+  const uchar2* ptab = reinterpret_cast<const uchar2*>(jsm + L.pt);
+  unsigned short* bt = reinterpret_cast<unsigned short*>(jsm + L.bt);
+  double2* H = h_in_smem ? reinterpret_cast<double2*>(jsm + L.h) : job.H;
+  __shared__ double s_red[2][kJacobiThreads / 32];
+  __shared__ int s_done;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (h_in_smem)
+    for (int t = threadIdx.x; t < B * B; t += blockDim.x) H[t] = job.H[t];
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    // b -> (t1 <= t2) over the upper triangle of the npairs x npairs block grid
+    int t1 = 0, rem = b;
+    while (rem >= npairs - t1) {
+      rem -= npairs - t1;
+      ++t1;
+    }
+    bt[b] = (unsigned short)(t1 | ((t1 + rem) << 8));
+  }
+  jacobi_pair_table(reinterpret_cast<uchar2*>(jsm + L.pt), Bp);
+  __syncthreads();
+  int sweep = 0, nsteps = 0;
   for (; sweep < max_sweeps; ++sweep) {
+    double off = 0.0, dg = 0.0;
+    for (int t = threadIdx.x; t < B * B; t += blockDim.x) {
+      const double2 h = H[t];
+      if ((t / B) == (t % B)) dg += h.x * h.x; else off += h.x * h.x + h.y * h.y;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_xor_sync(0xffffffffu, off, o);
+      dg += __shfl_xor_sync(0xffffffffu, dg, o);
+    }
+    if (lane == 0) {
+      s_red[0][warp] = off;
+      s_red[1][warp] = dg;
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
-      double off = 0.0, dg = 0.0;
-      for (int i = 0; i < B; ++i)
-        for (int j = 0; j < B; ++j) {
-          const double2 h = H[i * Bp + j];
-          if (i == j) dg += h.x * h.x; else off += h.x * h.x + h.y * h.y;
-        }
-      s_off = off;
-      s_diag = dg;
-      s_done = !(off > 1e-30 * dg) || dg == 0.0;
+      double a = 0.0, b = 0.0;
+      for (int k = 0; k < nw; ++k) {
+        a += s_red[0][k];
+        b += s_red[1][k];
+      }
+      s_done = !(a > 1e-28 * b) || b == 0.0;
     }
     __syncthreads();
     if (s_done) break;
-    for (int step = 0; step < Bp - 1; ++step) {
-      // rotation parameters for pair (pr[t], pr[Bp-1-t])
+    for (int step = 0; step < Bp - 1; ++step, ++nsteps) {
+      const uchar2* pairs = ptab + step * npairs;
       for (int t = threadIdx.x; t < npairs; t += blockDim.x) {
-        int p = pr[t], q = pr[Bp - 1 - t];
-        if (p > q) { const int tmp = p; p = q; q = tmp; }
-        double c = 1.0, s = 0.0, er = 1.0, ei = 0.0;
+        const int p = pairs[t].x, q = pairs[t].y;
+        double4 u = make_double4(1.0, 0.0, 1.0, 0.0);
         if (q < B) {
-          const double2 b = H[p * Bp + q];
-          const double ab = sqrt(b.x * b.x + b.y * b.y);
-          const double a = H[p * Bp + p].x, d = H[q * Bp + q].x;
-          if (ab > 1e-300 && ab > 1e-18 * sqrt(fabs(a * d))) {
-            const double th = (d - a) / (2.0 * ab);
-            const double tt = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1.0));
-            c = 1.0 / sqrt(tt * tt + 1.0);
-            s = tt * c;
-            er = b.x / ab;
-            ei = b.y / ab;  // e^{i phi} = b/|b|
-          }
+          double tb;
+          u = jacobi_rotation(H[p * B + p].x, H[q * B + q].x, H[p * B + q], &tb);
         }
-        pc[4 * t] = c;
-        pc[4 * t + 1] = s;
-        pc[4 * t + 2] = er;
-        pc[4 * t + 3] = ei;
+        pc[t] = u;
+        rot[(size_t)nsteps * npairs + t] = u;
       }
       __syncthreads();
-      // columns: H <- H U with U = [[c, s],[-s e^{-i phi}, c e^{-i phi}]] on (p, q)
-      for (int idx = threadIdx.x; idx < npairs * Bp; idx += blockDim.x) {
-        const int t = idx / Bp, k = idx % Bp;
-        int p = pr[t], q = pr[Bp - 1 - t];
-        if (p > q) { const int tmp = p; p = q; q = tmp; }
-        if (q >= B) continue;
-        const double c = pc[4 * t], s = pc[4 * t + 1];
-        const double2 em = make_double2(pc[4 * t + 2], -pc[4 * t + 3]);  // e^{-i phi}
-        const double2 hp = H[k * Bp + p], hq = H[k * Bp + q];
-        const double2 hqe = zmul(hq, em);
-        H[k * Bp + p] = make_double2(c * hp.x - s * hqe.x, c * hp.y - s * hqe.y);
-        H[k * Bp + q] = make_double2(s * hp.x + c * hqe.x, s * hp.y + c * hqe.y);
-        if (k < B) {
-          const double2 qp = Q[(size_t)k * B + p], qq = Q[(size_t)k * B + q];
-          const double2 qqe = zmul(qq, em);
-          Q[(size_t)k * B + p] = make_double2(c * qp.x - s * qqe.x, c * qp.y - s * qqe.y);
-          Q[(size_t)k * B + q] = make_double2(s * qp.x + c * qqe.x, s * qp.y + c * qqe.y);
-        }
-      }
-      __syncthreads();
-      // rows: H <- U^H H
-      for (int idx = threadIdx.x; idx < npairs * Bp; idx += blockDim.x) {
-        const int t = idx / Bp, k = idx % Bp;
-        int p = pr[t], q = pr[Bp - 1 - t];
-        if (p > q) { const int tmp = p; p = q; q = tmp; }
-        if (q >= B) continue;
-        const double c = pc[4 * t], s = pc[4 * t + 1];
-        const double2 ep = make_double2(pc[4 * t + 2], pc[4 * t + 3]);  // e^{+i phi}
-        const double2 hp = H[p * Bp + k], hq = H[q * Bp + k];
-        const double2 hqe = zmul(hq, ep);
-        H[p * Bp + k] = make_double2(c * hp.x - s * hqe.x, c * hp.y - s * hqe.y);
-        H[q * Bp + k] = make_double2(s * hp.x + c * hqe.x, s * hp.y + c * hqe.y);
-      }
-      __syncthreads();
-      // advance the tournament: keep pr[0], rotate the rest
-      if (threadIdx.x == 0) {
-        const int last = pr[Bp - 1];
-        for (int i = Bp - 1; i > 1; --i) pr[i] = pr[i - 1];
-        pr[1] = last;
+      for (int bi = threadIdx.x; bi < nblocks; bi += blockDim.x) {
+        const int t1 = bt[bi] & 0xff, t2 = bt[bi] >> 8;
+        double2 x00, x01, x10, x11;
+        jacobi_block(H, B, pairs[t1], pairs[t2], t1 == t2, pc[t1], pc[t2], x00, x01, x10, x11);
       }
       __syncthreads();
     }
   }
-  // eigenvalues, sorted descending (selection by rank; B is small)
+  // eigenvalues sorted descending (rank by comparison; B is small)
   for (int i = threadIdx.x; i < B; i += blockDim.x) {
-    const double vi = H[i * Bp + i].x;
-    int rank = 0;
+    const double vi = H[i * B + i].x;
+    int r = 0;
     for (int j = 0; j < B; ++j) {
-      const double vj = H[j * Bp + j].x;
-      rank += (vj > vi) || (vj == vi && j < i);
+      const double vj = H[j * B + j].x;
+      r += (vj > vi) || (vj == vi && j < i);
     }
-    w[rank] = vi;
-    pr[i] = rank;  // reuse: destination column of vector i
+    job.w[r] = vi;
+    job.jst[1 + i] = r;
   }
-  __syncthreads();
-  // permute the vectors through shared memory, one row of Q at a time
-  double2* row = H;  // reuse
-  for (int r = 0; r < B; ++r) {
-    for (int i = threadIdx.x; i < B; i += blockDim.x) row[pr[i]] = Q[(size_t)r * B + i];
+  if (threadIdx.x == 0) job.jst[0] = nsteps;
+}
+
+// Q[k][rank[p]] = (prod of the logged rotations)[k][p]: row k of Q evolves
+// independently (entries p, q of the row mix under pair (p, q)), so each warp
+// replays the log on one row held in shared memory, two pairs per lane.
+constexpr int kVecWarps = 8;
+constexpr int kVecChunk = 32;  // logged steps staged per pass
+
+size_t jacobi_vectors_smem(int B) {
+  const int Bp = B + (B & 1), npairs = Bp / 2;
+  return sizeof(double4) * kVecChunk * npairs + sizeof(double2) * kVecWarps * B +
+         ((sizeof(uchar2) * (Bp - 1) * npairs + 15) & ~size_t(15));
+}
+
+__global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jobs) {
+  extern __shared__ __align__(16) unsigned char vsm[];
+  const JacobiJob job = jobs.j[blockIdx.y];
+  const int B = job.B;
+  if (blockIdx.x * kVecWarps >= B) return;  // uniform over the CTA
+  const double4* __restrict__ rot = job.rot;
+  const int* __restrict__ jst = job.jst;
+  double2* __restrict__ Q = job.Q;
+  const int Bp = B + (B & 1), npairs = Bp / 2;
+  double4* lg = reinterpret_cast<double4*>(vsm);                       // kVecChunk x npairs
+  double2* rows = reinterpret_cast<double2*>(lg + kVecChunk * npairs);  // kVecWarps x B
+  uchar2* ptab = reinterpret_cast<uchar2*>(rows + kVecWarps * B);       // (Bp - 1) x npairs
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int k = blockIdx.x * kVecWarps + warp;
+  double2* row = rows + warp * B;
+  for (int p = lane; p < B; p += 32) row[p] = make_double2(p == k ? 1.0 : 0.0, 0.0);
+  jacobi_pair_table(ptab, Bp);
+  const int nsteps = jst[0];
+  const bool two = lane + 32 < npairs;
+  int step = 0;
+  for (int s0 = 0; s0 < nsteps; s0 += kVecChunk) {
+    const int ns = min(kVecChunk, nsteps - s0);
     __syncthreads();
-    for (int i = threadIdx.x; i < B; i += blockDim.x) Q[(size_t)r * B + i] = row[i];
+    for (int i = threadIdx.x; i < ns * npairs; i += blockDim.x) lg[i] = rot[(size_t)s0 * npairs + i];
     __syncthreads();
+    if (k >= B) continue;
+    for (int j = 0; j < ns; ++j) {
+      const uchar2* pr = ptab + step * npairs;
+      const double4* uj = lg + j * npairs;
+      if (lane < npairs) {
+        const int p0 = pr[lane].x, q0 = pr[lane].y;
+        const int p1 = two ? pr[lane + 32].x : p0, q1 = two ? pr[lane + 32].y : q0;
+        const bool ok0 = q0 < B, ok1 = two && q1 < B;
+        const double4 u0 = uj[lane];
+        const double4 u1 = two ? uj[lane + 32] : u0;
+        const double2 vp0 = row[p0], vq0 = ok0 ? row[q0] : vp0;
+        const double2 vp1 = row[p1], vq1 = ok1 ? row[q1] : vp1;
+        const double2 e0 = zmul(vq0, make_double2(u0.z, -u0.w));
+        const double2 e1 = zmul(vq1, make_double2(u1.z, -u1.w));
+        if (ok0) {
+          row[p0] = make_double2(u0.x * vp0.x - u0.y * e0.x, u0.x * vp0.y - u0.y * e0.y);
+          row[q0] = make_double2(u0.y * vp0.x + u0.x * e0.x, u0.y * vp0.y + u0.x * e0.y);
+        }
+        if (ok1) {
+          row[p1] = make_double2(u1.x * vp1.x - u1.y * e1.x, u1.x * vp1.y - u1.y * e1.y);
+          row[q1] = make_double2(u1.y * vp1.x + u1.x * e1.x, u1.y * vp1.y + u1.x * e1.y);
+        }
+      }
+      __syncwarp();
+      if (++step == Bp - 1) step = 0;
+    }
   }
-  if (threadIdx.x == 0 && sweeps_out) sweeps_out[0] = sweep;
+  if (k < B)
+    for (int p = lane; p < B; p += 32) Q[(size_t)k * B + jst[1 + p]] = row[p];
 }
 
 // krn[k][j] = U[N-1-j][k] as float planes (klitho_tcc.cpp:358-362)
@@ -348,8 +525,9 @@ __global__ void k_to_kernels(const double2* __restrict__ U, int N, int ldu, int 
 
 struct Workspace {
   double2 *X = nullptr, *W = nullptr, *Z = nullptr, *G = nullptr, *Rinv = nullptr, *Q = nullptr;
+  double4* rot = nullptr;
   double* w = nullptr;
-  int* status = nullptr;
+  int *status = nullptr, *jst = nullptr;
   ~Workspace() {
     cudaFree(X);
     cudaFree(W);
@@ -357,14 +535,19 @@ struct Workspace {
     cudaFree(G);
     cudaFree(Rinv);
     cudaFree(Q);
+    cudaFree(rot);
+    cudaFree(jst);
     cudaFree(w);
     cudaFree(status);
   }
 };
 
-size_t jacobi_smem(int B) {
+// k_jacobi keeps H in shared memory up to this size, else works in place
+constexpr size_t kJacobiSmemCap = 220 * 1024;
+bool jacobi_h_in_smem(int B) { return JacobiSmem(B).total_no_h + sizeof(double2) * (size_t)B * B <= kJacobiSmemCap; }
+size_t jacobi_log_elems(int B) {
   const int Bp = B + (B & 1);
-  return sizeof(double2) * (size_t)Bp * Bp + sizeof(int) * (Bp + 1) + sizeof(double) * 4 * (Bp / 2 + 1) + 64;
+  return (size_t)kJacobiMaxSweeps * (Bp - 1) * (Bp / 2) + 1;
 }
 
 // X (N x B) <- orth(X) by CholeskyQR2; the first pass shifted for safety
@@ -382,12 +565,35 @@ int cholqr2(double2* X, int N, int B, Workspace& ws, cudaStream_t st) {
   return KL_OK;
 }
 
-int jacobi(double2* H, int B, Workspace& ws, cudaStream_t st) {
-  const size_t sm = jacobi_smem(B);
-  if (sm > 48 * 1024) KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  k_jacobi<<<1, 256, sm, st>>>(H, B, ws.Q, ws.w, 60, nullptr);
-  KL_CUDA_TRY(cudaGetLastError());
+// Eigen-decompositions of a batch of Hermitian matrices, one CTA each (see
+// JacobiJob); H is overwritten when it does not fit in shared memory.
+int jacobi_batch(const std::vector<JacobiJob>& all, cudaStream_t st) {
+  for (size_t j0 = 0; j0 < all.size(); j0 += kJacobiMaxJobs) {
+    const int nj = (int)std::min(all.size() - j0, (size_t)kJacobiMaxJobs);
+    JacobiJobs jobs{};
+    int bmax = 1;
+    for (int j = 0; j < nj; ++j) {
+      jobs.j[j] = all[j0 + j];
+      bmax = std::max(bmax, jobs.j[j].B);
+    }
+    const bool in_smem = jacobi_h_in_smem(bmax);
+    const size_t sm = JacobiSmem(bmax).total_no_h + (in_smem ? sizeof(double2) * (size_t)bmax * bmax : 0);
+    if (sm > 48 * 1024)
+      KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_jacobi<<<nj, kJacobiThreads, sm, st>>>(jobs, in_smem ? 1 : 0, kJacobiMaxSweeps);
+    KL_CUDA_TRY(cudaGetLastError());
+    const size_t vsm = jacobi_vectors_smem(bmax);
+    if (vsm > 48 * 1024)
+      KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
+    k_jacobi_vectors<<<dim3((bmax + kVecWarps - 1) / kVecWarps, nj), 32 * kVecWarps, vsm, st>>>(jobs);
+    KL_CUDA_TRY(cudaGetLastError());
+  }
   return KL_OK;
+}
+
+// Q (B x B, column j = eigenvector j) and w (descending) of the Hermitian H
+int jacobi(double2* H, int B, double4* rot, int* jst, double2* Q, double* w, cudaStream_t st) {
+  return jacobi_batch({JacobiJob{H, rot, Q, w, jst, B}}, st);
 }
 
 // Generic driver.  apply(X, W): W = TCC X (N x B); project(X, H): H = X^H TCC X (B x B).
@@ -398,7 +604,8 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   const int K = opt.K;
   if (cudaMalloc(&ws.X, sizeof(double2) * (size_t)N * B) || cudaMalloc(&ws.W, sizeof(double2) * (size_t)N * B) ||
       cudaMalloc(&ws.G, sizeof(double2) * (size_t)B * B) || cudaMalloc(&ws.Rinv, sizeof(double2) * (size_t)B * B) ||
-      cudaMalloc(&ws.Q, sizeof(double2) * (size_t)B * B) || cudaMalloc(&ws.w, sizeof(double) * B) ||
+      cudaMalloc(&ws.Q, sizeof(double2) * (size_t)B * B) || cudaMalloc(&ws.rot, sizeof(double4) * jacobi_log_elems(B)) ||
+      cudaMalloc(&ws.jst, sizeof(int) * (B + 1)) || cudaMalloc(&ws.w, sizeof(double) * B) ||
       cudaMalloc(&ws.status, sizeof(int))) {
     cudaGetLastError();
     set_error("subspace iteration: device allocation failed");
@@ -424,7 +631,7 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   for (it = 1; it <= opt.max_iter; ++it) {
     if (it % check_every == 0) {
       if ((rc = project(ws.X, ws.G))) return rc;
-      if ((rc = jacobi(ws.G, B, ws, st))) return rc;
+      if ((rc = jacobi(ws.G, B, ws.rot, ws.jst, ws.Q, ws.w, st))) return rc;
       KL_CUDA_TRY(cudaMemcpyAsync(cur.data(), ws.w, sizeof(double) * B, cudaMemcpyDeviceToHost, st));
       KL_CUDA_TRY(cudaStreamSynchronize(st));
       change = 0.0;
@@ -445,7 +652,7 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   // final Rayleigh-Ritz on the current block (G holds the eigvecs in Q)
   if (!converged) {
     if ((rc = project(ws.X, ws.G))) return rc;
-    if ((rc = jacobi(ws.G, B, ws, st))) return rc;
+    if ((rc = jacobi(ws.G, B, ws.rot, ws.jst, ws.Q, ws.w, st))) return rc;
   }
   // U = X Q[:, :K] (N x K, row-major), eigenvalues
   if ((rc = zgemm<G_NN>(ws.X, B, ws.Q, B, ws.W, B, N, B, B, st))) return rc;
@@ -478,9 +685,76 @@ int block_size(const EigenOptions& opt, int N, int rank_bound) {
 
 }  // namespace
 
+namespace {
+
+// V[s][k] = Q[s][k] / sqrt(w[k]) for k < K (zero for a numerically null w[k])
+__global__ void k_ritz_scale(const double2* __restrict__ Q, int ldq, const double* __restrict__ w,
+                             int S, int K, double2* __restrict__ V) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S * K) return;
+  const int s = i / K, k = i - s * K;
+  const double wk = w[k];
+  const double f = (wk > 1e-15 * fabs(w[0]) && wk > 0.0) ? 1.0 / sqrt(wk) : 0.0;
+  const double2 q = Q[(size_t)s * ldq + k];
+  V[i] = make_double2(q.x * f, q.y * f);
+}
+
+// TCC = A A^H with S <= kGramMaxS columns: the TCC's range is span(A), so the
+// Rayleigh-Ritz step on that span is exact.  G = A^H A (S x S, FP64 products
+// of the FP32 factor), G = V diag(w) V^H by Jacobi, U = A V diag(w)^{-1/2}.
+// The Jacobi eigensolves of all problems run in one launch, one CTA each.
+int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
+  const size_t n = pr.size();
+  std::vector<Workspace> ws(n);
+  std::vector<JacobiJob> jobs(n);
+  for (size_t i = 0; i < n; ++i) {
+    const int S = pr[i].S, K = pr[i].K;
+    Workspace& w = ws[i];
+    if (cudaMalloc(&w.G, sizeof(double2) * (size_t)S * S) || cudaMalloc(&w.Q, sizeof(double2) * (size_t)S * S) ||
+        cudaMalloc(&w.rot, sizeof(double4) * jacobi_log_elems(S)) || cudaMalloc(&w.jst, sizeof(int) * (S + 1)) ||
+        cudaMalloc(&w.W, sizeof(double2) * (size_t)S * K) || cudaMalloc(&w.w, sizeof(double) * S)) {
+      cudaGetLastError();
+      set_error("eig_topk_factor: device allocation failed");
+      return KL_ERR_NOMEM;
+    }
+    int rc = zgemm<G_AHA>(pr[i].A, S, pr[i].A, S, w.G, S, S, S, pr[i].N, st);
+    if (rc) return rc;
+    jobs[i] = JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S};
+  }
+  int rc = jacobi_batch(jobs, st);
+  if (rc) return rc;
+  std::vector<int> nsteps(n, 0);
+  for (size_t i = 0; i < n; ++i) {
+    const int S = pr[i].S, K = pr[i].K;
+    k_ritz_scale<<<(S * K + 255) / 256, 256, 0, st>>>(ws[i].Q, S, ws[i].w, S, K, ws[i].W);
+    KL_CUDA_TRY(cudaGetLastError());
+    if ((rc = zgemm<G_AY>(pr[i].A, S, ws[i].W, K, pr[i].U, K, pr[i].N, K, S, st))) return rc;
+    KL_CUDA_TRY(cudaMemcpyAsync(pr[i].evals, ws[i].w, sizeof(double) * K, cudaMemcpyDeviceToDevice, st));
+    KL_CUDA_TRY(cudaMemcpyAsync(&nsteps[i], ws[i].jst, sizeof(int), cudaMemcpyDeviceToHost, st));
+  }
+  KL_CUDA_TRY(cudaStreamSynchronize(st));
+  for (size_t i = 0; i < n; ++i) {
+    const int S = pr[i].S;
+    const int sweeps = nsteps[i] / (S + (S & 1) - 1);
+    if (sweeps >= kJacobiMaxSweeps) {
+      set_error("eig_topk_factor: Jacobi eigensolve of the Gram matrix did not converge in " +
+                std::to_string(kJacobiMaxSweeps) + " sweeps");
+      return KL_ERR_NOT_CONVERGED;
+    }
+    if (pr[i].res) {
+      pr[i].res->iterations = sweeps;  // Jacobi sweeps of the single Rayleigh-Ritz step
+      pr[i].res->residual = 0.0;
+    }
+  }
+  return KL_OK;
+}
+
+}  // namespace
+
 int eig_topk_factor(const float2* A, int N, int S, const EigenOptions& opt, double2* U,
                     double* evals, EigenResult* res, cudaStream_t st) {
   KL_CHECK_ARG(opt.K > 0 && opt.K <= N, "eig_topk_factor: K out of range");
+  if (S <= kGramMaxS && opt.K <= S) return eig_topk_gram({FactorProblem{A, N, S, opt.K, U, evals, res}}, st);
   const int B = block_size(opt, N, S);
   KL_CHECK_ARG(opt.K <= B, "eig_topk_factor: K exceeds the block size");
   double2* Z = nullptr;
@@ -502,6 +776,22 @@ int eig_topk_factor(const float2* A, int N, int S, const EigenOptions& opt, doub
   int rc = subspace_iteration(N, opt, B, apply, project, U, evals, res, st);
   cudaFree(Z);
   return rc;
+}
+
+int eig_topk_factor_batch(const std::vector<FactorProblem>& pr, const EigenOptions& opt, cudaStream_t st) {
+  bool gram = true;
+  for (const FactorProblem& f : pr) {
+    KL_CHECK_ARG(f.K > 0 && f.K <= f.N, "eig_topk_factor: K out of range");
+    gram = gram && f.S <= kGramMaxS && f.K <= f.S;
+  }
+  if (gram) return eig_topk_gram(pr, st);
+  for (const FactorProblem& f : pr) {
+    EigenOptions o = opt;
+    o.K = f.K;
+    const int rc = eig_topk_factor(f.A, f.N, f.S, o, f.U, f.evals, f.res, st);
+    if (rc) return rc;
+  }
+  return KL_OK;
 }
 
 int eig_topk_dense(const double2* tcc, int N, const EigenOptions& opt, double2* U, double* evals,

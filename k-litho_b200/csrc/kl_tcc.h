@@ -76,9 +76,24 @@ struct EigenOptions {
 };
 
 struct EigenResult {
-  int iterations;
+  int iterations;   // subspace iterations, or Jacobi sweeps of a one-step Gram solve
   double residual;  // max relative Ritz-value change at the last check
 };
+
+// One top-K problem on a TCC factor A (N x S), for the batched solver.
+struct FactorProblem {
+  const float2* A;
+  int N, S, K;
+  double2* U;      // N x K eigenvectors (row-major)
+  double* evals;   // K eigenvalues, descending
+  EigenResult* res;
+};
+
+// Top-K eigenpairs of several TCC = A A^H at once (e.g. one per focus value):
+// factors with S <= 128 columns share one batched Gram eigensolve launch; the
+// rest are solved one after another by subspace iteration.
+int eig_topk_factor_batch(const std::vector<FactorProblem>& problems, const EigenOptions& opt,
+                          cudaStream_t st);
 
 // Operator TCC = A A^H given by its FP32 factor A (N x S).
 int eig_topk_factor(const float2* A, int N, int S, const EigenOptions& opt, double2* U,

@@ -212,6 +212,70 @@ int kl_tcc_build_minmax(kl_tcc_plan p, double* out4) {
   return rc;
 }
 
+namespace {
+
+// device buffers of one top-K solve
+struct TopkBuffers {
+  double2* U = nullptr;
+  double* ev = nullptr;
+  float *re = nullptr, *im = nullptr;
+  kl::EigenResult res{};
+  int alloc(int N, int K) {
+    int rc;
+    if ((rc = dalloc((void**)&U, sizeof(double2) * (size_t)N * K, "eigenvectors")) ||
+        (rc = dalloc((void**)&ev, sizeof(double) * K, "eigenvalues")) ||
+        (rc = dalloc((void**)&re, sizeof(float) * (size_t)N * K, "kernels")) ||
+        (rc = dalloc((void**)&im, sizeof(float) * (size_t)N * K, "kernels")))
+      return rc;
+    return KL_OK;
+  }
+  ~TopkBuffers() {
+    cudaFree(U);
+    cudaFree(ev);
+    cudaFree(re);
+    cudaFree(im);
+  }
+};
+
+kl::EigenOptions topk_options(int K, int block) {
+  kl::EigenOptions opt;
+  opt.K = K;
+  opt.B = block > 0 ? block : std::min(K + std::max(16, K / 2), std::max(K, 2 * K));
+  opt.max_iter = 400;
+  opt.tol = 1e-13;
+  opt.seed = 0x6b6c697468ull;
+  return opt;
+}
+
+// kernels (reference layout) and eigenvalues to the host; the nk - K kernels
+// beyond the TCC's rank are zero
+int topk_finish(TopkBuffers& b, int N, int K, int nk, float* krn_re_host, float* krn_im_host,
+                float* scales_host, double* evals_host, int* iterations, cudaStream_t st) {
+  int rc = kl::eig_to_kernels(b.U, N, K, b.re, b.im, st);
+  if (rc) return rc;
+  std::vector<double> evh(K);
+  cudaMemcpy(krn_re_host, b.re, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
+  cudaMemcpy(krn_im_host, b.im, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
+  cudaMemcpy(evh.data(), b.ev, sizeof(double) * K, cudaMemcpyDeviceToHost);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    kl::set_error(std::string("kl_topk_eig: ") + cudaGetErrorString(cudaGetLastError()));
+    return KL_ERR_CUDA;
+  }
+  for (int k = 0; k < nk; ++k) {
+    const double v = k < K ? evh[k] : 0.0;
+    scales_host[k] = (float)v;
+    if (evals_host) evals_host[k] = v;
+  }
+  for (int k = K; k < nk; ++k) {
+    std::memset(krn_re_host + (size_t)k * N, 0, sizeof(float) * N);
+    std::memset(krn_im_host + (size_t)k * N, 0, sizeof(float) * N);
+  }
+  if (iterations) *iterations = b.res.iterations;
+  return KL_OK;
+}
+
+}  // namespace
+
 int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn_im_host,
                 float* scales_host, double* evals_host, int* iterations) {
   KL_CHECK_ARG(p && krn_re_host && krn_im_host && scales_host, "kl_topk_eig: NULL argument");
@@ -221,60 +285,62 @@ int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn
   // kernels beyond the TCC's rank (<= S) have eigenvalue 0: the solver
   // returns the nonzero part, the rest are zero kernels
   const int K = std::min(nk, std::min(N, S));
-  kl::EigenOptions opt;
-  opt.K = K;
-  opt.B = block > 0 ? block : std::min(K + std::max(16, K / 2), std::max(K, 2 * K));
-  opt.max_iter = 400;
-  opt.tol = 1e-13;
-  opt.seed = 0x6b6c697468ull;
-  double2* U = nullptr;
-  double* ev = nullptr;
-  float *re = nullptr, *im = nullptr;
-  int rc;
-  if ((rc = dalloc((void**)&U, sizeof(double2) * (size_t)N * K, "eigenvectors")) ||
-      (rc = dalloc((void**)&ev, sizeof(double) * K, "eigenvalues")) ||
-      (rc = dalloc((void**)&re, sizeof(float) * (size_t)N * K, "kernels")) ||
-      (rc = dalloc((void**)&im, sizeof(float) * (size_t)N * K, "kernels"))) {
-    cudaFree(U);
-    cudaFree(ev);
-    cudaFree(re);
-    return rc;
-  }
-  kl::EigenResult res{};
+  const kl::EigenOptions opt = topk_options(K, block);
+  TopkBuffers b;
+  int rc = b.alloc(N, K);
+  if (rc) return rc;
   if (p->precision == KL_PREC_FAST) {
-    rc = kl::eig_topk_factor(p->A, N, S, opt, U, ev, &res, st);
+    rc = kl::eig_topk_factor(p->A, N, S, opt, b.U, b.ev, &b.res, st);
   } else {
     rc = ensure_tcc64(p, st);
-    if (!rc) rc = kl::eig_topk_dense(p->tcc64, N, opt, U, ev, &res, st);
+    if (!rc) rc = kl::eig_topk_dense(p->tcc64, N, opt, b.U, b.ev, &b.res, st);
   }
-  if (!rc) rc = kl::eig_to_kernels(U, N, K, re, im, st);
-  std::vector<double> evh(K);
-  if (!rc) {
-    cudaMemcpy(krn_re_host, re, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
-    cudaMemcpy(krn_im_host, im, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
-    cudaMemcpy(evh.data(), ev, sizeof(double) * K, cudaMemcpyDeviceToHost);
-    if (cudaDeviceSynchronize() != cudaSuccess) {
-      kl::set_error(std::string("kl_topk_eig: ") + cudaGetErrorString(cudaGetLastError()));
-      rc = KL_ERR_CUDA;
-    }
+  if (rc) return rc;
+  return topk_finish(b, N, K, nk, krn_re_host, krn_im_host, scales_host, evals_host, iterations, st);
+}
+
+int kl_topk_eig_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, float* krn_re_host,
+                      float* krn_im_host, float* scales_host, double* evals_host, int* iterations) {
+  KL_CHECK_ARG(plans && nplans > 0 && krn_re_host && krn_im_host && scales_host,
+               "kl_topk_eig_batch: NULL argument or empty batch");
+  const int N = plans[0] ? plans[0]->pp.N : 0;
+  bool fast = true;
+  for (int i = 0; i < nplans; ++i) {
+    KL_CHECK_ARG(plans[i], "kl_topk_eig_batch: NULL plan");
+    KL_CHECK_ARG(plans[i]->pp.N == N, "kl_topk_eig_batch: plans must share the pupil band (same N)");
+    fast = fast && plans[i]->precision == KL_PREC_FAST;
   }
-  if (!rc) {
-    for (int k = 0; k < nk; ++k) {
-      const double v = k < K ? evh[k] : 0.0;
-      scales_host[k] = (float)v;
-      if (evals_host) evals_host[k] = v;
+  KL_CHECK_ARG(nk > 0 && nk <= N, "kl_topk_eig_batch: nk must be in [1, N]");
+  const size_t kstride = (size_t)nk * N;
+  if (!fast) {  // the FP64 path solves one plan after another
+    for (int i = 0; i < nplans; ++i) {
+      const int rc = kl_topk_eig(plans[i], nk, block, krn_re_host + i * kstride, krn_im_host + i * kstride,
+                                 scales_host + (size_t)i * nk, evals_host ? evals_host + (size_t)i * nk : nullptr,
+                                 iterations ? iterations + i : nullptr);
+      if (rc) return rc;
     }
-    for (int k = K; k < nk; ++k) {
-      std::memset(krn_re_host + (size_t)k * N, 0, sizeof(float) * N);
-      std::memset(krn_im_host + (size_t)k * N, 0, sizeof(float) * N);
-    }
-    if (iterations) *iterations = res.iterations;
+    return KL_OK;
   }
-  cudaFree(U);
-  cudaFree(ev);
-  cudaFree(re);
-  cudaFree(im);
-  return rc;
+  cudaStream_t st = nullptr;
+  std::vector<TopkBuffers> bufs(nplans);
+  std::vector<kl::FactorProblem> pr(nplans);
+  int kmax = 1;
+  for (int i = 0; i < nplans; ++i) {
+    const int K = std::min(nk, std::min(N, plans[i]->pp.S));
+    kmax = std::max(kmax, K);
+    int rc = bufs[i].alloc(N, K);
+    if (rc) return rc;
+    pr[i] = kl::FactorProblem{plans[i]->A, N, plans[i]->pp.S, K, bufs[i].U, bufs[i].ev, &bufs[i].res};
+  }
+  int rc = kl::eig_topk_factor_batch(pr, topk_options(kmax, block), st);
+  if (rc) return rc;
+  for (int i = 0; i < nplans; ++i) {
+    rc = topk_finish(bufs[i], N, pr[i].K, nk, krn_re_host + i * kstride, krn_im_host + i * kstride,
+                     scales_host + (size_t)i * nk, evals_host ? evals_host + (size_t)i * nk : nullptr,
+                     iterations ? iterations + i : nullptr, st);
+    if (rc) return rc;
+  }
+  return KL_OK;
 }
 
 int kl_hopkins_image(kl_tcc_plan p, const float* masks_dev, int nclips, float* images_dev,

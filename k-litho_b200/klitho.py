@@ -85,6 +85,9 @@ def lib() -> ctypes.CDLL:
         L.kl_tcc_minmax.argtypes = [_vp, _vp, ctypes.POINTER(ctypes.c_double), _vp]
         L.kl_topk_eig.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _c_float_p, _c_float_p,
                                   _c_float_p, ctypes.POINTER(ctypes.c_double), _c_int_p]
+        L.kl_topk_eig_batch.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        _c_float_p, _c_float_p, _c_float_p,
+                                        ctypes.POINTER(ctypes.c_double), _c_int_p]
         L.kl_hopkins_image.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
         L.kl_socs_plan_create_adjoint.argtypes = L.kl_socs_plan_create.argtypes
         L.kl_socs_vjp.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
@@ -343,6 +346,24 @@ class TccPlan:
                                 ctypes.byref(it)), "kl_topk_eig")
         k = (re + 1j * im).astype(np.complex64).reshape(nk, self.N)
         return k, sc, ev, it.value
+
+    @staticmethod
+    def topk_batch(plans, nk: int, block: int = 0):
+        """kl_topk_eig over several plans sharing N (e.g. a focus sweep) in one
+        call: lists of (kernels, scales, eigenvalues, iterations) per plan."""
+        n, N = len(plans), plans[0].N
+        re = np.zeros(n * nk * N, dtype=np.float32)
+        im = np.zeros(n * nk * N, dtype=np.float32)
+        sc = np.zeros(n * nk, dtype=np.float32)
+        ev = np.zeros(n * nk, dtype=np.float64)
+        it = np.zeros(n, dtype=np.int32)
+        hs = (_vp * n)(*[p._h for p in plans])
+        check(lib().kl_topk_eig_batch(hs, n, int(nk), int(block), _fp(re), _fp(im), _fp(sc),
+                                      ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                      it.ctypes.data_as(_c_int_p)), "kl_topk_eig_batch")
+        k = (re + 1j * im).astype(np.complex64).reshape(n, nk, N)
+        return ([k[i] for i in range(n)], list(sc.reshape(n, nk)), list(ev.reshape(n, nk)),
+                [int(x) for x in it])
 
     def hopkins(self, masks_dev, images_dev, nclips: int | None = None, stream=None) -> None:
         n = masks_dev.shape[0] if nclips is None else nclips

@@ -134,3 +134,49 @@ def test_topk_beyond_rank_is_zero(cuda):
     plan = K.TccPlan(src, 0.8, 0.0, 256, 256)
     krn, sc, ev, it = plan.topk(3)
     assert ev[0] > 0 and np.all(ev[1:] == 0) and np.all(krn[1:] == 0)
+
+
+def test_topk_batch_focus_sweep(cuda):
+    # one plan per focus value, solved in one call; each must agree with its
+    # single-plan solve and with zheevr on the oracle TCC
+    L, nk = 512, 32
+    src = K.createSource(61, "Dipole", radius=0.15, offset=0.7, onXAxis=1)
+    focus = [-50.0, 0.0, 35.0]
+    plans = [K.TccPlan(src, 1.35, synth.defocus_arg(f), L, L, n_medium=1.44) for f in focus]
+    kb, sb, eb, itb = K.TccPlan.topk_batch(plans, nk)
+    sig = O.outer_sigma(src)
+    Nx, Ny = O.band(1.35, L, L, sig)
+    for i, f in enumerate(focus):
+        k1, s1, e1, _ = plans[i].topk(nk)
+        assert np.abs(eb[i] - e1).max() <= 1e-12 * np.abs(e1).max()
+        assert np.linalg.norm(weighted_projector(kb[i], eb[i]) - weighted_projector(k1, e1)) <= \
+            1e-6 * np.linalg.norm(weighted_projector(k1, e1))
+        tcc = O.calc_tcc(src, sig, 1.35, synth.defocus_arg(f), L, L, Nx, Ny, n_medium=1.44)
+        kr, _, er = O.calc_kernels(tcc, nk)
+        assert np.abs(eb[i] - er).max() <= 1e-6 * np.abs(er).max()
+        Pr = weighted_projector(kr, er)
+        assert np.linalg.norm(weighted_projector(kb[i], eb[i]) - Pr) / np.linalg.norm(Pr) <= 1e-5
+        assert 0 < itb[i] < 40  # Jacobi sweeps of the one Gram solve
+
+
+@pytest.mark.parametrize("precision", [K.PREC_FAST, K.PREC_FP64])
+def test_topk_batch_sequential_paths(cuda, precision):
+    # more than 128 source points (subspace iteration) or FP64 plans: the batch
+    # is solved plan by plan and must equal the single-plan results
+    L, nk = 512, 16
+    src = K.createSource(41, "Annular", 0.6, 0.9)
+    plans = [K.TccPlan(src, 1.35, synth.defocus_arg(f), L, L, n_medium=1.44, precision=precision)
+             for f in (-25.0, 25.0)]
+    kb, sb, eb, itb = K.TccPlan.topk_batch(plans, nk)
+    for i in range(2):
+        k1, s1, e1, it1 = plans[i].topk(nk)
+        assert np.abs(eb[i] - e1).max() <= 1e-12 * np.abs(e1).max()
+        assert itb[i] == it1
+
+
+def test_topk_batch_rejects_mixed_band(cuda):
+    src = K.createSource(41, "Annular", 0.6, 0.9)
+    a = K.TccPlan(src, 1.35, 0.0, 512, 512, n_medium=1.44)
+    b = K.TccPlan(src, 1.35, 0.0, 1024, 1024, n_medium=1.44)
+    with pytest.raises(RuntimeError, match="same N"):
+        K.TccPlan.topk_batch([a, b], 8)
