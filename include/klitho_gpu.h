@@ -184,6 +184,32 @@ int kl_mask_spectrum(kl_socs_plan plan, const float* masks_dev, int nclips, floa
                      void* stream);
 
 /* ------------------------------------------------------------------------- */
+/* Plain FP64 path: the reference's FFT-based chain restated in FP64 on the   */
+/* GPU (full L x L FFTs, the K fields of calcSOCS materialised), for FP64      */
+/* parity and as the baseline of the fused path.  Lx, Ly powers of two.       */
+/* ------------------------------------------------------------------------- */
+
+/* FT_r2c (K-Litho-SOCS/klitho_socs.cpp:70-121) in FP64: spectrum_dev receives
+ * Lx*Ly complex128 (interleaved doubles), DC at [Ly/2][Lx/2], scaled by
+ * 1/(Lx Ly).  Synchronous. */
+int kl_fp64_mask_spectrum(const float* mask_dev, int Lx, int Ly, double* spectrum_dev, void* stream);
+/* FT_r2c + calcSOCS + FI (klitho_socs.cpp:338-343, :196-241, :158-194) in FP64
+ * for nclips masks; kernels_dev nk x (2Nx+1)(2Ny+1) complex64 interleaved (the
+ * krn_*.bin contents), scales_dev nk floats; images_dev nclips x Ly x Lx
+ * doubles (the reference's image before its float store).  Stream-ordered;
+ * allocates its scratch per call. */
+int kl_fp64_socs_forward(const float* masks_dev, int nclips, int Lx, int Ly, int Nx, int Ny,
+                         const float* kernels_dev, const float* scales_dev, int nk, double* images_dev,
+                         void* stream);
+/* kl_socs_vjp's loss and mask gradient (one kernel set) in FP64 with the
+ * fields materialised: loss_dev[c], grad_dev (nclips x Ly x Lx doubles) and,
+ * if images_dev is not NULL, the FP64 image.  The plain-path counterpart of
+ * the fused adjoint; no reference counterpart.  Stream-ordered. */
+int kl_fp64_socs_vjp(const float* masks_dev, const float* targets_dev, int nclips, int Lx, int Ly, int Nx,
+                     int Ny, const float* kernels_dev, const float* scales_dev, int nk, double alpha,
+                     double threshold, double* images_dev, double* grad_dev, double* loss_dev, void* stream);
+
+/* ------------------------------------------------------------------------- */
 /* TCC assembly, SOCS kernels, Hopkins image: K-Litho-TCC/klitho_tcc.cpp      */
 /* ------------------------------------------------------------------------- */
 
@@ -246,6 +272,12 @@ int kl_hopkins_image(kl_tcc_plan plan, const float* masks_dev, int nclips, float
                      void* stream);
 /* One Hopkins image from and to host memory (Lx*Ly floats each); synchronous. */
 int kl_hopkins_image_host(kl_tcc_plan plan, const float* mask_host, float* image_host);
+/* calcImage + FT_c2r (klitho_tcc.cpp:269-290, :150-183) in FP64 on the plan's
+ * FP64 TCC (built on first use) with full L x L FFTs: the plain FP64 path of
+ * the Hopkins image, in double (before the reference's float store).  Plans
+ * of KL_PREC_FP64 precision only. */
+int kl_fp64_hopkins_image(kl_tcc_plan plan, const float* masks_dev, int nclips, double* images_dev,
+                          void* stream);
 
 #ifdef __cplusplus
 }

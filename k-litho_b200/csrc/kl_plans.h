@@ -65,3 +65,17 @@ int vjp_launch_source(const SocsGeom& g, const float2* partial, const float2* gp
                       int nsets, const float2* Hs, const float* Jw, const int* src_id, int S,
                       int nsplit, float* grad_src, cudaStream_t st);
 }  // namespace kl
+
+namespace kl {
+namespace f64 {
+// the plain FP64 imaging path (fp64_path.cu); device pointers, one clip at a time
+int socs_forward(const float* masks, int nclips, int Lx, int Ly, int Nx, int Ny, const float2* H,
+                 const float* lam, int nk, double* images, cudaStream_t st);
+int hopkins_image(const float* masks, int nclips, int Lx, int Ly, int Nx, int Ny, const double2* tcc,
+                  double* images, cudaStream_t st);
+int mask_spectrum(const float* mask, int Lx, int Ly, double2* out, cudaStream_t st);
+int socs_vjp(const float* masks, const float* targets, int nclips, int Lx, int Ly, int Nx, int Ny,
+             const float2* H, const float* lam, int nk, double alpha, double thr, double* images, double* grad,
+             double* loss, cudaStream_t st);
+}  // namespace f64
+}  // namespace kl

@@ -264,4 +264,21 @@ int kl_mask_spectrum(kl_socs_plan p, const float* masks, int nclips, float* band
   return kl::socs_launch_band(p->g, p->partial, nclips, reinterpret_cast<float2*>(band), st);
 }
 
+int kl_fp64_socs_forward(const float* masks, int nclips, int Lx, int Ly, int Nx, int Ny, const float* kernels,
+                         const float* scales, int nk, double* images, void* stream) {
+  return kl::f64::socs_forward(masks, nclips, Lx, Ly, Nx, Ny, reinterpret_cast<const float2*>(kernels), scales,
+                               nk, images, (cudaStream_t)stream);
+}
+
+int kl_fp64_socs_vjp(const float* masks, const float* targets, int nclips, int Lx, int Ly, int Nx, int Ny,
+                     const float* kernels, const float* scales, int nk, double alpha, double threshold,
+                     double* images, double* grad, double* loss, void* stream) {
+  return kl::f64::socs_vjp(masks, targets, nclips, Lx, Ly, Nx, Ny, reinterpret_cast<const float2*>(kernels), scales,
+                           nk, alpha, threshold, images, grad, loss, (cudaStream_t)stream);
+}
+
+int kl_fp64_mask_spectrum(const float* mask, int Lx, int Ly, double* spectrum, void* stream) {
+  return kl::f64::mask_spectrum(mask, Lx, Ly, reinterpret_cast<double2*>(spectrum), (cudaStream_t)stream);
+}
+
 }  // extern "C"

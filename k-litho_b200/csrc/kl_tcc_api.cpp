@@ -343,10 +343,19 @@ int kl_topk_eig_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, f
   return KL_OK;
 }
 
+int kl_fp64_hopkins_image(kl_tcc_plan p, const float* masks_dev, int nclips, double* images_dev, void* stream) {
+  KL_CHECK_ARG(p && masks_dev && images_dev, "kl_fp64_hopkins_image: NULL argument");
+  KL_CHECK_ARG(p->precision == KL_PREC_FP64, "kl_fp64_hopkins_image: needs a plan of KL_PREC_FP64 precision");
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = ensure_tcc64(p, st);
+  if (rc) return rc;
+  return kl::f64::hopkins_image(masks_dev, nclips, p->Lx, p->Ly, p->pp.Nx, p->pp.Ny, p->tcc64, images_dev, st);
+}
+
 int kl_hopkins_image(kl_tcc_plan p, const float* masks_dev, int nclips, float* images_dev,
                      void* stream) {
   KL_CHECK_ARG(p && masks_dev && images_dev, "kl_hopkins_image: NULL argument");
-  KL_CHECK_ARG(p->precision == KL_PREC_FAST, "kl_hopkins_image: FP64 imaging is kl_fp64_hopkins_image");
+  KL_CHECK_ARG(p->precision == KL_PREC_FAST, "kl_hopkins_image: plans of FP64 precision image through kl_fp64_hopkins_image");
   cudaStream_t st = (cudaStream_t)stream;
   const int N = p->pp.N, S = p->pp.S;
   if (!p->hopkins || nclips > p->hopkins_clips) {

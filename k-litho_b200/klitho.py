@@ -89,6 +89,13 @@ def lib() -> ctypes.CDLL:
                                         _c_float_p, _c_float_p, _c_float_p,
                                         ctypes.POINTER(ctypes.c_double), _c_int_p]
         L.kl_hopkins_image.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+        L.kl_fp64_hopkins_image.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
+        L.kl_fp64_socs_forward.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_int, _vp, _vp, ctypes.c_int, _vp, _vp]
+        L.kl_fp64_mask_spectrum.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
+        L.kl_fp64_socs_vjp.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, _vp, _vp, ctypes.c_int, ctypes.c_double,
+                                       ctypes.c_double, _vp, _vp, _vp, _vp]
         L.kl_socs_plan_create_adjoint.argtypes = L.kl_socs_plan_create.argtypes
         L.kl_socs_vjp.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                   _vp, _vp, _vp, _vp]
@@ -365,7 +372,45 @@ class TccPlan:
         return ([k[i] for i in range(n)], list(sc.reshape(n, nk)), list(ev.reshape(n, nk)),
                 [int(x) for x in it])
 
+    def hopkins_fp64(self, masks_dev, images_dev, nclips: int | None = None, stream=None) -> None:
+        """Plain FP64 Hopkins image (plans of PREC_FP64); images_dev float64."""
+        n = masks_dev.shape[0] if nclips is None else nclips
+        check(lib().kl_fp64_hopkins_image(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(images_dev),
+                                          _stream_ptr(stream)), "kl_fp64_hopkins_image")
+
     def hopkins(self, masks_dev, images_dev, nclips: int | None = None, stream=None) -> None:
         n = masks_dev.shape[0] if nclips is None else nclips
         check(lib().kl_hopkins_image(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(images_dev),
                                      _stream_ptr(stream)), "kl_hopkins_image")
+
+
+def fp64_socs_forward(masks_dev, Nx: int, Ny: int, kernels_dev, scales_dev, images_dev, stream=None) -> None:
+    """Plain FP64 SOCS image (FT_r2c + calcSOCS + FI with full FFTs): masks
+    (n, Ly, Lx) float32, kernels (nk, N, 2) float32, scales (nk,) float32 on the
+    device; images_dev (n, Ly, Lx) float64."""
+    n, Ly, Lx = masks_dev.shape
+    nk = scales_dev.shape[0]
+    check(lib().kl_fp64_socs_forward(_dev_ptr(masks_dev), int(n), int(Lx), int(Ly), int(Nx), int(Ny),
+                                     _dev_ptr(kernels_dev), _dev_ptr(scales_dev), int(nk),
+                                     _dev_ptr(images_dev), _stream_ptr(stream)), "kl_fp64_socs_forward")
+
+
+def fp64_mask_spectrum(mask_dev, spectrum_dev, stream=None) -> None:
+    """FT_r2c in FP64: mask (Ly, Lx) float32 -> spectrum (Ly, Lx, 2) float64."""
+    Ly, Lx = mask_dev.shape[-2:]
+    check(lib().kl_fp64_mask_spectrum(_dev_ptr(mask_dev), int(Lx), int(Ly), _dev_ptr(spectrum_dev),
+                                      _stream_ptr(stream)), "kl_fp64_mask_spectrum")
+
+
+def fp64_socs_vjp(masks_dev, targets_dev, Nx: int, Ny: int, kernels_dev, scales_dev, grad_dev, loss_dev,
+                  images_dev=None, alpha: float = 50.0, threshold: float = 0.225, stream=None) -> None:
+    """Plain FP64 loss and dL/dmask (float64 outputs) of the sigmoid resist
+    L2 loss of the SOCS image; masks/targets (n, Ly, Lx) float32."""
+    n, Ly, Lx = masks_dev.shape
+    nk = scales_dev.shape[0]
+    check(lib().kl_fp64_socs_vjp(_dev_ptr(masks_dev), _dev_ptr(targets_dev), int(n), int(Lx), int(Ly),
+                                 int(Nx), int(Ny), _dev_ptr(kernels_dev), _dev_ptr(scales_dev), int(nk),
+                                 float(alpha), float(threshold),
+                                 None if images_dev is None else _dev_ptr(images_dev),
+                                 _dev_ptr(grad_dev), _dev_ptr(loss_dev), _stream_ptr(stream)),
+          "kl_fp64_socs_vjp")
