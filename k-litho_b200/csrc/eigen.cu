@@ -528,17 +528,19 @@ struct Workspace {
   double4* rot = nullptr;
   double* w = nullptr;
   int *status = nullptr, *jst = nullptr;
+  cudaStream_t st = nullptr;
+  std::vector<void*> owned;
+  template <typename T>
+  int get(T** p, size_t count) {
+    void* v = nullptr;
+    const int rc = scratch_alloc(&v, sizeof(T) * count, st, "eigen workspace");
+    if (rc) return rc;
+    owned.push_back(v);
+    *p = static_cast<T*>(v);
+    return KL_OK;
+  }
   ~Workspace() {
-    cudaFree(X);
-    cudaFree(W);
-    cudaFree(Z);
-    cudaFree(G);
-    cudaFree(Rinv);
-    cudaFree(Q);
-    cudaFree(rot);
-    cudaFree(jst);
-    cudaFree(w);
-    cudaFree(status);
+    for (void* v : owned) scratch_free(v, st);
   }
 };
 
@@ -601,16 +603,15 @@ template <typename Apply, typename Project>
 int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Project project,
                        double2* U, double* evals, EigenResult* res, cudaStream_t st) {
   Workspace ws;
+  ws.st = st;
   const int K = opt.K;
-  if (cudaMalloc(&ws.X, sizeof(double2) * (size_t)N * B) || cudaMalloc(&ws.W, sizeof(double2) * (size_t)N * B) ||
-      cudaMalloc(&ws.G, sizeof(double2) * (size_t)B * B) || cudaMalloc(&ws.Rinv, sizeof(double2) * (size_t)B * B) ||
-      cudaMalloc(&ws.Q, sizeof(double2) * (size_t)B * B) || cudaMalloc(&ws.rot, sizeof(double4) * jacobi_log_elems(B)) ||
-      cudaMalloc(&ws.jst, sizeof(int) * (B + 1)) || cudaMalloc(&ws.w, sizeof(double) * B) ||
-      cudaMalloc(&ws.status, sizeof(int))) {
-    cudaGetLastError();
-    set_error("subspace iteration: device allocation failed");
-    return KL_ERR_NOMEM;
-  }
+  int arc;
+  if ((arc = ws.get(&ws.X, (size_t)N * B)) || (arc = ws.get(&ws.W, (size_t)N * B)) ||
+      (arc = ws.get(&ws.G, (size_t)B * B)) || (arc = ws.get(&ws.Rinv, (size_t)B * B)) ||
+      (arc = ws.get(&ws.Q, (size_t)B * B)) || (arc = ws.get(&ws.rot, jacobi_log_elems(B))) ||
+      (arc = ws.get(&ws.jst, (size_t)B + 1)) || (arc = ws.get(&ws.w, (size_t)B)) ||
+      (arc = ws.get(&ws.status, 1)))
+    return arc;
   const size_t sm_chol = sizeof(double2) * (size_t)B * B;
   if (sm_chol > 48 * 1024)
     KL_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_chol));
@@ -710,13 +711,12 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S, K = pr[i].K;
     Workspace& w = ws[i];
-    if (cudaMalloc(&w.G, sizeof(double2) * (size_t)S * S) || cudaMalloc(&w.Q, sizeof(double2) * (size_t)S * S) ||
-        cudaMalloc(&w.rot, sizeof(double4) * jacobi_log_elems(S)) || cudaMalloc(&w.jst, sizeof(int) * (S + 1)) ||
-        cudaMalloc(&w.W, sizeof(double2) * (size_t)S * K) || cudaMalloc(&w.w, sizeof(double) * S)) {
-      cudaGetLastError();
-      set_error("eig_topk_factor: device allocation failed");
-      return KL_ERR_NOMEM;
-    }
+    w.st = st;
+    int arc;
+    if ((arc = w.get(&w.G, (size_t)S * S)) || (arc = w.get(&w.Q, (size_t)S * S)) ||
+        (arc = w.get(&w.rot, jacobi_log_elems(S))) || (arc = w.get(&w.jst, (size_t)S + 1)) ||
+        (arc = w.get(&w.W, (size_t)S * K)) || (arc = w.get(&w.w, (size_t)S)))
+      return arc;
     int rc = zgemm<G_AHA>(pr[i].A, S, pr[i].A, S, w.G, S, S, S, pr[i].N, st);
     if (rc) return rc;
     jobs[i] = JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S};
@@ -758,11 +758,7 @@ int eig_topk_factor(const float2* A, int N, int S, const EigenOptions& opt, doub
   const int B = block_size(opt, N, S);
   KL_CHECK_ARG(opt.K <= B, "eig_topk_factor: K exceeds the block size");
   double2* Z = nullptr;
-  if (cudaMalloc(&Z, sizeof(double2) * (size_t)S * B)) {
-    cudaGetLastError();
-    set_error("eig_topk_factor: device allocation failed");
-    return KL_ERR_NOMEM;
-  }
+  if (int arc = scratch_alloc((void**)&Z, sizeof(double2) * (size_t)S * B, st, "eigen workspace")) return arc;
   auto apply = [&](double2* X, double2* W) -> int {
     int rc = zgemm<G_AHX>(A, S, X, B, Z, B, S, B, N, st);  // Z = A^H X
     if (rc) return rc;
@@ -774,7 +770,7 @@ int eig_topk_factor(const float2* A, int N, int S, const EigenOptions& opt, doub
     return zgemm<G_HH>(Z, B, Z, B, H, B, B, B, S, st);      // H = Z^H Z
   };
   int rc = subspace_iteration(N, opt, B, apply, project, U, evals, res, st);
-  cudaFree(Z);
+  scratch_free(Z, st);
   return rc;
 }
 
@@ -799,11 +795,7 @@ int eig_topk_dense(const double2* tcc, int N, const EigenOptions& opt, double2* 
   KL_CHECK_ARG(opt.K > 0 && opt.K <= N, "eig_topk_dense: K out of range");
   const int B = block_size(opt, N, N);
   double2* Wt = nullptr;
-  if (cudaMalloc(&Wt, sizeof(double2) * (size_t)N * B)) {
-    cudaGetLastError();
-    set_error("eig_topk_dense: device allocation failed");
-    return KL_ERR_NOMEM;
-  }
+  if (int arc = scratch_alloc((void**)&Wt, sizeof(double2) * (size_t)N * B, st, "eigen workspace")) return arc;
   auto apply = [&](double2* X, double2* W) -> int {
     return zgemm<G_DX>(tcc, N, X, B, W, B, N, B, N, st);
   };
@@ -813,7 +805,7 @@ int eig_topk_dense(const double2* tcc, int N, const EigenOptions& opt, double2* 
     return zgemm<G_HH>(X, B, Wt, B, H, B, B, B, N, st);
   };
   int rc = subspace_iteration(N, opt, B, apply, project, U, evals, res, st);
-  cudaFree(Wt);
+  scratch_free(Wt, st);
   return rc;
 }
 
@@ -822,11 +814,7 @@ int eig_topk_dense_c64(const float2* tcc, int N, const EigenOptions& opt, double
   KL_CHECK_ARG(opt.K > 0 && opt.K <= N, "eig_topk_dense_c64: K out of range");
   const int B = block_size(opt, N, N);
   double2* Wt = nullptr;
-  if (cudaMalloc(&Wt, sizeof(double2) * (size_t)N * B)) {
-    cudaGetLastError();
-    set_error("eig_topk_dense_c64: device allocation failed");
-    return KL_ERR_NOMEM;
-  }
+  if (int arc = scratch_alloc((void**)&Wt, sizeof(double2) * (size_t)N * B, st, "eigen workspace")) return arc;
   auto apply = [&](double2* X, double2* W) -> int {
     return zgemm<G_FX>(tcc, N, X, B, W, B, N, B, N, st);
   };
@@ -836,7 +824,7 @@ int eig_topk_dense_c64(const float2* tcc, int N, const EigenOptions& opt, double
     return zgemm<G_HH>(X, B, Wt, B, H, B, B, B, N, st);
   };
   int rc = subspace_iteration(N, opt, B, apply, project, U, evals, res, st);
-  cudaFree(Wt);
+  scratch_free(Wt, st);
   return rc;
 }
 

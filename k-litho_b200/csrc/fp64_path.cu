@@ -12,6 +12,7 @@
 // does nothing clever: full-size spectra, every field written to memory.
 #include <algorithm>
 #include <string>
+#include <vector>
 
 #include "kl_internal.h"
 #include "kl_plans.h"
@@ -357,33 +358,21 @@ struct Fp64Work {
   double2 *D = nullptr, *T = nullptr, *wx = nullptr, *wy = nullptr;  // L^2 data, transpose, twiddles
   double2 *X = nullptr, *E = nullptr, *wg = nullptr, *wgy = nullptr;  // K g^2 fields, grid twiddles
   double* acc = nullptr;
-  double2* Y = nullptr;  // adjoint: 2 g^2 (band of dL/dI, scratch)
+  double2* Y = nullptr;               // adjoint: 2 g^2 (band of dL/dI, scratch)
   double *I = nullptr, *G = nullptr;  // adjoint: image and dL/dI, L^2
+  cudaStream_t st = nullptr;
+  std::vector<void*> owned;
   ~Fp64Work() {
-    cudaFree(Y);
-    cudaFree(I);
-    cudaFree(G);
-    cudaFree(D);
-    cudaFree(T);
-    cudaFree(wx);
-    cudaFree(wy);
-    cudaFree(X);
-    cudaFree(E);
-    cudaFree(wg);
-    cudaFree(wgy);
-    cudaFree(acc);
+    for (void* v : owned) scratch_free(v, st);
   }
 };
 
 namespace {
 
-int alloc(void** p, size_t bytes, const char* what) {
-  if (cudaMalloc(p, bytes) != cudaSuccess) {
-    cudaGetLastError();
-    set_error(std::string("FP64 path: device allocation failed (") + what + ")");
-    return KL_ERR_NOMEM;
-  }
-  return KL_OK;
+int alloc(Fp64Work& w, void** p, size_t bytes, const char* what) {
+  const int rc = scratch_alloc(p, bytes, w.st, what);
+  if (!rc) w.owned.push_back(*p);
+  return rc;
 }
 
 int fft_rows(double2* d, int nrows, int n, const double2* w, int sign, double scale, cudaStream_t st) {
@@ -430,6 +419,7 @@ int prepare(Fp64Work& w, int Lx, int Ly, int gx, int gy, int nk, cudaStream_t st
   KL_CHECK_ARG(ilog2_exact(Lx) > 0 && ilog2_exact(Ly) > 0 && ilog2_exact(Lx) <= kMaxFftLog2 &&
                    ilog2_exact(Ly) <= kMaxFftLog2,
                "FP64 path: Lx and Ly must be powers of two in [2, 8192]");
+  w.st = st;
   w.Lx = Lx;
   w.Ly = Ly;
   w.gx = gx;
@@ -437,21 +427,21 @@ int prepare(Fp64Work& w, int Lx, int Ly, int gx, int gy, int nk, cudaStream_t st
   w.nk = nk;
   const size_t nL = (size_t)Lx * Ly;
   int rc;
-  if ((rc = alloc((void**)&w.D, sizeof(double2) * nL, "spectrum")) ||
-      (rc = alloc((void**)&w.T, sizeof(double2) * nL, "transpose")) ||
-      (rc = alloc((void**)&w.wx, sizeof(double2) * Lx, "twiddles")) ||
-      (rc = alloc((void**)&w.wy, sizeof(double2) * Ly, "twiddles")))
+  if ((rc = alloc(w, (void**)&w.D, sizeof(double2) * nL, "spectrum")) ||
+      (rc = alloc(w, (void**)&w.T, sizeof(double2) * nL, "transpose")) ||
+      (rc = alloc(w, (void**)&w.wx, sizeof(double2) * Lx, "twiddles")) ||
+      (rc = alloc(w, (void**)&w.wy, sizeof(double2) * Ly, "twiddles")))
     return rc;
   k_twiddle<<<(Lx + 255) / 256, 256, 0, st>>>(w.wx, Lx);
   k_twiddle<<<(Ly + 255) / 256, 256, 0, st>>>(w.wy, Ly);
   KL_CUDA_TRY(cudaGetLastError());
   if (gx > 0) {
     const size_t ng = (size_t)gx * gy, nb = std::max(nk, 3);  // >= 3: FI uses three slots
-    if ((rc = alloc((void**)&w.X, sizeof(double2) * ng * nb, "fields")) ||
-        (rc = alloc((void**)&w.E, sizeof(double2) * ng * nb, "fields")) ||
-        (rc = alloc((void**)&w.wg, sizeof(double2) * gx, "grid twiddles")) ||
-        (rc = alloc((void**)&w.wgy, sizeof(double2) * gy, "grid twiddles")) ||
-        (rc = alloc((void**)&w.acc, sizeof(double) * ng, "accumulator")))
+    if ((rc = alloc(w, (void**)&w.X, sizeof(double2) * ng * nb, "fields")) ||
+        (rc = alloc(w, (void**)&w.E, sizeof(double2) * ng * nb, "fields")) ||
+        (rc = alloc(w, (void**)&w.wg, sizeof(double2) * gx, "grid twiddles")) ||
+        (rc = alloc(w, (void**)&w.wgy, sizeof(double2) * gy, "grid twiddles")) ||
+        (rc = alloc(w, (void**)&w.acc, sizeof(double) * ng, "accumulator")))
       return rc;
     k_twiddle<<<(gx + 255) / 256, 256, 0, st>>>(w.wg, gx);
     k_twiddle<<<(gy + 255) / 256, 256, 0, st>>>(w.wgy, gy);
@@ -538,9 +528,9 @@ int socs_vjp(const float* masks, const float* targets, int nclips, int Lx, int L
   Fp64Work w;
   if ((rc = prepare(w, Lx, Ly, gx, gy, nk, st))) return rc;
   const size_t ng = (size_t)gx * gy, nL = (size_t)Lx * Ly;
-  if ((rc = alloc((void**)&w.Y, sizeof(double2) * 2 * ng, "adjoint grid")) ||
-      (rc = alloc((void**)&w.G, sizeof(double) * nL, "dL/dI")) ||
-      (!images && (rc = alloc((void**)&w.I, sizeof(double) * nL, "image"))))
+  if ((rc = alloc(w, (void**)&w.Y, sizeof(double2) * 2 * ng, "adjoint grid")) ||
+      (rc = alloc(w, (void**)&w.G, sizeof(double) * nL, "dL/dI")) ||
+      (!images && (rc = alloc(w, (void**)&w.I, sizeof(double) * nL, "image"))))
     return rc;
   KL_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(double) * nclips, st));
   const int nb = (2 * Nx + 1) * (2 * Ny + 1);
@@ -580,7 +570,7 @@ int hopkins_image(const float* masks, int nclips, int Lx, int Ly, int Nx, int Ny
   if (rc) return rc;
   const int N = (2 * Nx + 1) * (2 * Ny + 1), nh = (2 * Nx + 1) * (4 * Ny + 1);
   double2* half = nullptr;
-  if ((rc = alloc((void**)&half, sizeof(double2) * nh, "Hopkins spectrum"))) return rc;
+  if ((rc = alloc(w, (void**)&half, sizeof(double2) * nh, "Hopkins spectrum"))) return rc;
   const size_t nL = (size_t)Lx * Ly;
   for (int c = 0; c < nclips && !rc; ++c) {
     if ((rc = mask_dft(w, masks + (size_t)c * nL, st))) break;
@@ -602,8 +592,6 @@ int hopkins_image(const float* masks, int nclips, int Lx, int Ly, int Nx, int Ny
     rc = image_from_spectrum(w, images + (size_t)c * nL, st);
   }
   if (rc == KL_ERR_CUDA) set_error("kl_fp64_hopkins_image: kernel launch failed");
-  cudaStreamSynchronize(st);
-  cudaFree(half);
   return rc;
 }
 

@@ -9,6 +9,8 @@
 #include <fstream>
 #include <iostream>
 #include <sstream>
+#include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -18,6 +20,37 @@ namespace kl {
 
 static thread_local std::string t_err;
 void set_error(const std::string& msg) { t_err = msg; }
+
+int scratch_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
+  static std::mutex mu;
+  static std::vector<int> pooled;  // devices whose default pool keeps freed memory
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (std::find(pooled.begin(), pooled.end(), dev) == pooled.end()) {
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      cudaGetLastError();
+      pooled.push_back(dev);
+    }
+  }
+  *p = nullptr;
+  if (cudaMallocAsync(p, bytes ? bytes : 16, st) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    set_error(std::string("device allocation failed (") + what + ", " + std::to_string(bytes) + " bytes)");
+    return KL_ERR_NOMEM;
+  }
+  return KL_OK;
+}
+
+void scratch_free(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
 const char* last_error() { return t_err.c_str(); }
 
 namespace {

@@ -13,6 +13,13 @@ namespace kl {
 
 // thread-local last error text, returned by kl_last_error()
 void set_error(const std::string& msg);
+
+// Per-call scratch: stream-ordered allocations from the current device's
+// default memory pool, which keeps freed blocks cached, so temporaries cost
+// neither a device synchronisation nor a fresh cudaMalloc on repeat calls.
+// scratch_alloc returns KL_OK or KL_ERR_NOMEM (with the message set).
+int scratch_alloc(void** p, size_t bytes, cudaStream_t st, const char* what);
+void scratch_free(void* p, cudaStream_t st);
 const char* last_error();
 
 #define KL_CUDA_TRY(expr)                                                      \

@@ -14,25 +14,30 @@
 #include "kl_tcc.h"
 
 namespace {
+// Plan buffers and host-synchronous temporaries come from the device's pooled
+// scratch allocator on the legacy stream; dalloc waits for the block to be
+// usable from any stream, dfree is called only after the work using the
+// block has been synchronised.
+void dfree(void* p) { kl::scratch_free(p, nullptr); }
+
 void free_plan(kl_tcc_plan p) {
   if (!p) return;
-  cudaFree(p->pts_dev);
-  cudaFree(p->A);
-  cudaFree(p->P);
-  cudaFree(p->J);
-  cudaFree(p->src_id);
-  cudaFree(p->tcc64);
-  cudaFree(p->err);
+  cudaDeviceSynchronize();
+  dfree(p->pts_dev);
+  dfree(p->A);
+  dfree(p->P);
+  dfree(p->J);
+  dfree(p->src_id);
+  dfree(p->tcc64);
+  dfree(p->err);
   if (p->hopkins) kl_socs_plan_destroy(p->hopkins);
   delete p;
 }
 
 int dalloc(void** ptr, size_t bytes, const char* what) {
-  if (cudaMalloc(ptr, bytes ? bytes : 16) != cudaSuccess) {
-    cudaGetLastError();
-    kl::set_error(std::string("cudaMalloc(") + what + ") failed");
-    return KL_ERR_NOMEM;
-  }
+  const int rc = kl::scratch_alloc(ptr, bytes, nullptr, what);
+  if (rc) return rc;
+  KL_CUDA_TRY(cudaStreamSynchronize(nullptr));
   return KL_OK;
 }
 
@@ -166,10 +171,10 @@ int kl_tcc_build(kl_tcc_plan p, void* tcc_dev, void* stream) {
   void *X1 = nullptr, *X2 = nullptr, *Y = nullptr;
   const size_t ob = sizeof(uint16_t) * (size_t)N * Kp;
   int rc;
-  if ((rc = dalloc(&X1, ob, "split operand")) || (rc = dalloc(&X2, ob, "split operand")) ||
-      (rc = dalloc(&Y, ob, "split operand"))) {
-    cudaFree(X1);
-    cudaFree(X2);
+  if ((rc = kl::scratch_alloc(&X1, ob, st, "split operand")) || (rc = kl::scratch_alloc(&X2, ob, st, "split operand")) ||
+      (rc = kl::scratch_alloc(&Y, ob, st, "split operand"))) {
+    kl::scratch_free(X1, st);
+    kl::scratch_free(X2, st);
     return rc;
   }
   KL_CUDA_TRY(cudaMemsetAsync(p->err, 0, sizeof(int), st));
@@ -186,9 +191,9 @@ int kl_tcc_build(kl_tcc_plan p, void* tcc_dev, void* stream) {
       rc = KL_ERR_CUDA;
     }
   }
-  cudaFree(X1);
-  cudaFree(X2);
-  cudaFree(Y);
+  kl::scratch_free(X1, st);
+  kl::scratch_free(X2, st);
+  kl::scratch_free(Y, st);
   return rc;
 }
 
@@ -204,11 +209,12 @@ int kl_tcc_build_minmax(kl_tcc_plan p, double* out4) {
   KL_CHECK_ARG(p && out4, "kl_tcc_build_minmax: NULL argument");
   const size_t n = (size_t)p->pp.N * p->pp.N;
   void* tcc = nullptr;
-  int rc = dalloc(&tcc, (p->precision == KL_PREC_FP64 ? sizeof(double2) : sizeof(float2)) * n, "TCC");
+  int rc = kl::scratch_alloc(&tcc, (p->precision == KL_PREC_FP64 ? sizeof(double2) : sizeof(float2)) * n,
+                             nullptr, "TCC");
   if (rc) return rc;
   rc = kl_tcc_build(p, tcc, nullptr);
   if (!rc) rc = kl_tcc_minmax(p, tcc, out4, nullptr);
-  cudaFree(tcc);
+  kl::scratch_free(tcc, nullptr);
   return rc;
 }
 
@@ -222,18 +228,18 @@ struct TopkBuffers {
   kl::EigenResult res{};
   int alloc(int N, int K) {
     int rc;
-    if ((rc = dalloc((void**)&U, sizeof(double2) * (size_t)N * K, "eigenvectors")) ||
-        (rc = dalloc((void**)&ev, sizeof(double) * K, "eigenvalues")) ||
-        (rc = dalloc((void**)&re, sizeof(float) * (size_t)N * K, "kernels")) ||
-        (rc = dalloc((void**)&im, sizeof(float) * (size_t)N * K, "kernels")))
+    if ((rc = kl::scratch_alloc((void**)&U, sizeof(double2) * (size_t)N * K, nullptr, "eigenvectors")) ||
+        (rc = kl::scratch_alloc((void**)&ev, sizeof(double) * K, nullptr, "eigenvalues")) ||
+        (rc = kl::scratch_alloc((void**)&re, sizeof(float) * (size_t)N * K, nullptr, "kernels")) ||
+        (rc = kl::scratch_alloc((void**)&im, sizeof(float) * (size_t)N * K, nullptr, "kernels")))
       return rc;
     return KL_OK;
   }
   ~TopkBuffers() {
-    cudaFree(U);
-    cudaFree(ev);
-    cudaFree(re);
-    cudaFree(im);
+    kl::scratch_free(U, nullptr);
+    kl::scratch_free(ev, nullptr);
+    kl::scratch_free(re, nullptr);
+    kl::scratch_free(im, nullptr);
   }
 };
 
@@ -369,14 +375,14 @@ int kl_hopkins_image(kl_tcc_plan p, const float* masks_dev, int nclips, float* i
     float* lam = nullptr;
     if ((rc = dalloc((void**)&H, sizeof(float2) * (size_t)N * S, "Abbe kernels")) ||
         (rc = dalloc((void**)&lam, sizeof(float) * S, "Abbe weights"))) {
-      cudaFree(H);
+      dfree(H);
       return rc;
     }
     rc = kl::tcc_factor_kernels(p->A, N, S, H, lam, st);
     if (!rc) rc = kl_socs_set_kernels_device(p->hopkins, 0, H, lam, st);
     cudaStreamSynchronize(st);
-    cudaFree(H);
-    cudaFree(lam);
+    dfree(H);
+    dfree(lam);
     if (rc) return rc;
   }
   return kl_socs_forward(p->hopkins, masks_dev, nclips, images_dev, stream);
@@ -396,7 +402,7 @@ int kl_socs_vjp_source(kl_socs_plan sp, kl_tcc_plan tp, float* grad_src, void* s
   int rc;
   if ((rc = dalloc((void**)&H, sizeof(float2) * (size_t)N * S, "source kernels")) ||
       (rc = dalloc((void**)&lam, sizeof(float) * S, "source weights"))) {
-    cudaFree(H);
+    dfree(H);
     return rc;
   }
   KL_CUDA_TRY(cudaMemsetAsync(grad_src, 0, sizeof(float) * (size_t)tp->srcSize * tp->srcSize, st));
@@ -408,8 +414,8 @@ int kl_socs_vjp_source(kl_socs_plan sp, kl_tcc_plan tp, float* grad_src, void* s
     rc = kl::vjp_launch_source(sp->g, sp->partial, sp->gpart, nimg, sp->nsets, H, tp->J, tp->src_id,
                                S, nsplit, grad_src, st);
   cudaStreamSynchronize(st);
-  cudaFree(H);
-  cudaFree(lam);
+  dfree(H);
+  dfree(lam);
   return rc;
 }
 
@@ -419,7 +425,7 @@ int kl_hopkins_image_host(kl_tcc_plan p, const float* mask_host, float* image_ho
   float *md = nullptr, *id = nullptr;
   int rc;
   if ((rc = dalloc((void**)&md, bytes, "mask")) || (rc = dalloc((void**)&id, bytes, "image"))) {
-    cudaFree(md);
+    dfree(md);
     return rc;
   }
   cudaMemcpy(md, mask_host, bytes, cudaMemcpyHostToDevice);
@@ -428,8 +434,8 @@ int kl_hopkins_image_host(kl_tcc_plan p, const float* mask_host, float* image_ho
     kl::set_error(std::string("kl_hopkins_image_host: ") + cudaGetErrorString(cudaGetLastError()));
     rc = KL_ERR_CUDA;
   }
-  cudaFree(md);
-  cudaFree(id);
+  dfree(md);
+  dfree(id);
   return rc;
 }
 
