@@ -329,7 +329,7 @@ def bench_fwd_adj(args, stream, peak_gbs):
     import torch
     import klitho as K
     import synth
-    L, n, nk = 1024, 32, 24
+    L, n, nk = 1024, (args.clips if args.part == "fwd_adj" and args.clips else 32), 24
     src = K.createSource(41, "Annular", 0.6, 0.9)
     tp = K.TccPlan(src, 1.35, 0.0, L, L, n_medium=synth.N_WATER)
     krn, sc, _, _ = tp.topk(nk)
@@ -359,7 +359,7 @@ def bench_fwd_adj(args, stream, peak_gbs):
     plan.vjp_source(tp, gs)
     src_ms = (time.perf_counter() - t0) * 1e3
     # plain FP64 GPU path on 8 of the clips (same loss, one kernel set)
-    nf = 8
+    nf = min(8, n)
     kd = torch.from_numpy(np.stack([krn.real, krn.imag], -1).astype(np.float32).copy()).cuda()
     sd = torch.from_numpy(np.asarray(sc, dtype=np.float32)).cuda()
     g64 = torch.empty((nf, L, L), dtype=torch.float64, device="cuda")
@@ -579,6 +579,17 @@ def run_reference(args):
     print(json.dumps(out))
 
 
+def run_part(args):
+    """One secondary measurement alone, printed as its own JSON object."""
+    import torch
+    torch.cuda.set_device(0)
+    if args.part == "fwd_adj":
+        r = bench_fwd_adj(args, torch.cuda.current_stream(), peaks()[0])
+    else:
+        r = bench_tcc_eigen(args)
+    print(json.dumps(r))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -594,6 +605,8 @@ def main():
     ap.add_argument("--only", type=int, default=0,
                     help="restrict to one clip size (profiling cases)")
     ap.add_argument("--clips", type=int, default=0, help="clip count for --only")
+    ap.add_argument("--part", choices=["all", "fwd_adj", "tcc_eigen"], default="all",
+                    help="run one secondary measurement alone (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -602,6 +615,8 @@ def main():
         CLASSES[:] = [(args.only, n)]
     if args.impl == "reference":
         run_reference(args)
+    elif args.part != "all":
+        run_part(args)
     else:
         run_ours(args)
 
