@@ -225,7 +225,11 @@ def run_ours(args):
         achieved = bytes_per_step[dom] / launches_per_step / (avg_launch_ms / 1e3) / 1e9
         roof = {"kernel": names[dom], "bound": "hbm", "achieved": round(achieved, 1),
                 "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None,
+                "frac": round(achieved / peak, 4),
+                "traffic": (int(TRAFFIC_PER_ALGORITHMIC_BYTE[names[dom]] * bytes_per_step[dom] / launches_per_step)
+                            if names[dom] in TRAFFIC_PER_ALGORITHMIC_BYTE else None),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 48 x 1024^2 "
+                                  "capture (profiles/socs_kernels_1024x48_full.md), scaled by pixels",
                 "algorithmic_bytes_per_launch": int(bytes_per_step[dom] / launches_per_step)}
     else:
         roof = {"kernel": names[dom], "bound": "compute", "achieved": None, "peak": None,
@@ -285,6 +289,13 @@ def run_ours(args):
         p.close()
     if dist:
         dist.destroy_process_group()
+
+
+# DRAM bytes per algorithmic byte measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) on 48 clips of 1024^2 x 3 kernel sets; both kernels
+# stream their clip data once, so traffic scales with the pixels of a launch.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"socs_inverse": (6.695 + 546.386) / 603.98,
+                                "socs_forward": (201.372 + 4.389) / 201.33}
 
 
 def fp64_baseline(masks_d, kset0, value_per_gpu, img_equiv):
