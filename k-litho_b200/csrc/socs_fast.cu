@@ -406,7 +406,7 @@ __global__ void __launch_bounds__(kThreads) k_socs_inverse(const float2* __restr
                                                            const SocsGeom g,
                                                            const float2* __restrict__ tx,
                                                            const float2* __restrict__ ty,
-                                                           int nsplit,
+                                                           int nsplit, int spc,
                                                            float* __restrict__ images) {
   constexpr int J = 32 * RJ;
   constexpr int QP = NBM + 1;
@@ -416,65 +416,85 @@ __global__ void __launch_bounds__(kThreads) k_socs_inverse(const float2* __restr
   float2* Ts = Qs + J * QP;                         // [nty][ntx]
   float2* ph = Ts + g.nty * g.ntx;                  // [nty]     e^{2 pi i a s / Ly}
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int s = blockIdx.x, img = blockIdx.y;
+  const int img = blockIdx.y;
+  const int s0 = blockIdx.x * spc, s1 = min(g.nS, s0 + spc);  // this CTA's strips
   const size_t tsz = (size_t)g.nty * g.ntx;
   const float2* Ti = T + (size_t)img * nsplit * tsz;
 
+  // once per CTA: the image's band spectrum (slices summed), the x twiddles,
+  // and the zero columns b >= ntx of the row coefficients
+#pragma unroll 4
   for (int i = threadIdx.x; i < (int)tsz; i += kThreads) {
     float2 v = __ldg(Ti + i);
     for (int p = 1; p < nsplit; ++p) v = cadd(v, __ldg(Ti + p * tsz + i));
     Ts[i] = v;
   }
+#pragma unroll 4
   for (int i = threadIdx.x; i < NBM * V; i += kThreads) twi[i] = __ldg(tx + i);
-  for (int i = threadIdx.x; i < g.nty; i += kThreads) ph[i] = __ldg(ty + (size_t)s * g.nty + i);
   for (int i = threadIdx.x; i < J * QP; i += kThreads) Qs[i] = make_float2(0.f, 0.f);
+  float2 ph_next = make_float2(0.f, 0.f);
+  if (threadIdx.x < g.nty) ph_next = __ldg(ty + (size_t)s0 * g.nty + threadIdx.x);
   __syncthreads();
 
-  // rows of the strip: Q[y = s + nS j][b] = sum_a T[a][b] e^{2 pi i a y / Ly}
   WarpFFT<RJ, +1> wf;
   wf.init(lane);
   const int br = (int)(__brev((unsigned)lane) >> 27);
   const int A = 2 * g.Ny;
-  for (int b = warp; b < g.ntx; b += kWarps) {
-    float2 vv[RJ];
-#pragma unroll
-    for (int j = 0; j < RJ; ++j) {
-      const int n = lane + 32 * j;
-      float2 f = make_float2(0.f, 0.f);
-      for (int a = n - J * ((n + A) / J); a <= A; a += J)
-        f = cfma(Ts[(a + A) * g.ntx + b], ph[a + A], f);
-      vv[j] = f;
-    }
-    wf.run(vv, lane);
-    const float w = b == 0 ? 1.f : 2.f;
-#pragma unroll
-    for (int q1 = 0; q1 < RJ; ++q1) Qs[(q1 + RJ * br) * QP + b] = cscale(vv[q1], w);
-  }
-  __syncthreads();
-
   float* out = images + (size_t)img * g.Lx * g.Ly;
-  for (int jj = warp; jj < J; jj += kWarps) {
-    float* row = out + (size_t)(s + g.nS * jj) * (V * P);
-    const float2* q = Qs + jj * QP;
 #pragma unroll 1
-    for (int c = 0; c < V / 32; ++c) {
-      const int lp = lane + 32 * c;
-      float2 Z[P];
-#pragma unroll
-      for (int i = 0; i < P; ++i) Z[i] = make_float2(0.f, 0.f);
-#pragma unroll
-      for (int b = 0; b < NBM; ++b) {
-        // Z += q[b] * conj(tw)
-        const float2 qb = q[b], w = twi[b * V + lp];
-        const int k = b % P;
-        Z[k] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Z[k].x)),
-                           fmaf(qb.y, w.x, fmaf(-qb.x, w.y, Z[k].y)));
-      }
-      float o[P];
-      re_idft_reg<P>(Z, o);
-#pragma unroll
-      for (int i = 0; i < P; ++i) row[lp + V * i] = o[i];
+  for (int s = s0; s < s1; ++s) {
+    if (threadIdx.x < g.nty) {
+      ph[threadIdx.x] = ph_next;
+      if (s + 1 < s1) ph_next = __ldg(ty + (size_t)(s + 1) * g.nty + threadIdx.x);
     }
+    __syncthreads();
+    // rows of the strip: Q[y = s + nS j][b] = sum_a T[a][b] e^{2 pi i a y / Ly}
+    for (int b = warp; b < g.ntx; b += kWarps) {
+      float2 vv[RJ];
+#pragma unroll
+      for (int j = 0; j < RJ; ++j) {
+        const int n = lane + 32 * j;
+        float2 f = make_float2(0.f, 0.f);
+        for (int a = n - J * ((n + A) / J); a <= A; a += J)
+          f = cfma(Ts[(a + A) * g.ntx + b], ph[a + A], f);
+        vv[j] = f;
+      }
+      wf.run(vv, lane);
+      const float w = b == 0 ? 1.f : 2.f;
+#pragma unroll
+      for (int q1 = 0; q1 < RJ; ++q1) Qs[(q1 + RJ * br) * QP + b] = cscale(vv[q1], w);
+    }
+    __syncthreads();
+
+    for (int jj = warp; jj < J; jj += kWarps) {
+      float* row = out + (size_t)(s + g.nS * jj) * (V * P);
+      const float2* q = Qs + jj * QP;
+#pragma unroll 1
+      for (int c = 0; c < V / 32; ++c) {
+        const int lp = lane + 32 * c;
+        float2 Z[P];
+#pragma unroll
+        for (int i = 0; i < P; ++i) Z[i] = make_float2(0.f, 0.f);
+        // Z[k] += q[b] * conj(tw[b]) for b = k (mod P), in chunks of P bins so that
+        // only one chunk of coefficients is live in registers
+        constexpr int KB = NBM < P ? NBM : P;
+#pragma unroll 1
+        for (int b0 = 0; b0 < NBM; b0 += KB) {
+#pragma unroll
+          for (int k = 0; k < KB; ++k) {
+            const float2 qb = q[b0 + k], w = twi[(b0 + k) * V + lp];
+            const int kk = k;  // b0 is a multiple of P when NBM > P
+            Z[kk] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Z[kk].x)),
+                                fmaf(qb.y, w.x, fmaf(-qb.x, w.y, Z[kk].y)));
+          }
+        }
+        float o[P];
+        re_idft_reg<P>(Z, o);
+#pragma unroll
+        for (int i = 0; i < P; ++i) row[lp + V * i] = o[i];
+      }
+    }
+    __syncthreads();  // Qs and ph are rewritten for the next strip
   }
 }
 
@@ -540,7 +560,11 @@ int launch_inv(const SocsGeom& g, const float2* tx, const float2* ty, const floa
   auto kern = k_socs_inverse<P, V, NBM, RJ>;
   int rc = set_smem(kern, sm);
   if (rc) return rc;
-  kern<<<dim3(g.nS, nimg), kThreads, sm, st>>>(T, g, tx, ty, nsplit, images);
+  // strips per CTA: the image's spectrum and the twiddle table are loaded once
+  // per CTA, so give each CTA several strips while keeping >= 4 CTAs per SM
+  int spc = 1;
+  while (spc < 8 && spc * 2 <= g.nS && (long long)nimg * ((g.nS + 2 * spc - 1) / (2 * spc)) >= 4 * 148) spc *= 2;
+  kern<<<dim3((g.nS + spc - 1) / spc, nimg), kThreads, sm, st>>>(T, g, tx, ty, nsplit, spc, images);
   return check_launch("k_socs_inverse");
 }
 
