@@ -124,6 +124,43 @@ int kl_socs_forward_host(kl_socs_plan plan, const float* masks_host, int nclips,
                          float* images_host, void* stream);
 
 /* ------------------------------------------------------------------------- */
+/* Batched imaging: launch-shape autotuning and graph-captured batches.       */
+/* No counterpart in the reference, which images one clip per process.       */
+/* ------------------------------------------------------------------------- */
+
+/* Times the plan's launch shapes for batches of nclips clips (kernel slices of
+ * the spectral stage: 1, 2, 4, 8; image strips per CTA of the synthesis stage:
+ * 1 .. 16) with CUDA events on `stream` and keeps the fastest; later calls of
+ * kl_socs_forward with nclips clips use it.  Writes images_dev (the images of
+ * the chosen shape).  Synchronous.  The chosen shape is returned in
+ * *nsplit / *spc when those are not NULL. */
+int kl_socs_autotune(kl_socs_plan plan, const float* masks_dev, int nclips, float* images_dev,
+                     void* stream, int* nsplit, int* spc);
+
+typedef struct kl_socs_batch_s* kl_socs_batch;
+/* A batch of plans (e.g. one per clip size, each holding one kernel set per
+ * focus value) imaged together: kl_socs_batch_forward runs the plans as
+ * concurrent branches of one CUDA graph, so the on-chip stage of one plan
+ * overlaps the memory-bound stages of the others.  The plans must outlive the
+ * batch. */
+int kl_socs_batch_create(kl_socs_batch* batch, const kl_socs_plan* plans, int nplans);
+int kl_socs_batch_destroy(kl_socs_batch batch);
+/* masks_dev[i] / images_dev[i] / nclips[i] for plan i (layouts as in
+ * kl_socs_forward).  The first call for a given set of buffers and counts
+ * runs the work directly and captures it as a graph; later calls with the
+ * same buffers and counts replay the graph (buffer contents may change).
+ * Ordered after earlier work on `stream`; later work on `stream` waits for it. */
+int kl_socs_batch_forward(kl_socs_batch batch, const float* const* masks_dev, const int* nclips,
+                          float* const* images_dev, void* stream);
+/* Per-stage timing inside the graph (recaptures on change); stage times of
+ * plan `plan` in the last completed call: ms[0] forward, ms[1] spectral,
+ * ms[2] synthesis. */
+int kl_socs_batch_enable_timing(kl_socs_batch batch, int enable);
+int kl_socs_batch_stage_times(kl_socs_batch batch, int plan, double* ms);
+/* Number of graphs captured so far (for checking that replays reuse one). */
+int kl_socs_batch_graph_builds(kl_socs_batch batch);
+
+/* ------------------------------------------------------------------------- */
 /* Adjoint (VJP) of SOCS imaging under a sigmoid resist and an L2 loss.       */
 /* No counterpart in the reference.                                            */
 /* ------------------------------------------------------------------------- */

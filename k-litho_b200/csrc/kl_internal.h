@@ -81,8 +81,9 @@ int socs_launch_forward(const SocsGeom& g, const float2* tx, const float2* ty, c
 int socs_launch_spectral(const SocsGeom& g, const float2* partial, int nclips, const float2* H,
                          const float* lam, int K, int nsets, int nsplit, float2* T,
                          cudaStream_t st);
+// spc: strips per CTA of the inverse kernel (0 = chosen from the batch size)
 int socs_launch_inverse(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T,
-                        int nclips, int nsets, int nsplit, float* images, cudaStream_t st);
+                        int nclips, int nsets, int nsplit, float* images, cudaStream_t st, int spc = 0);
 // centred band of FT_r2c (DC at the band centre), complex64 nby x nbx per clip
 int socs_launch_band(const SocsGeom& g, const float2* partial, int nclips, float2* band,
                      cudaStream_t st);

@@ -30,7 +30,17 @@ struct kl_socs_plan_s {
   // optional stage timing: 4 events per kl_socs_forward
   bool timing = false;
   std::vector<cudaEvent_t> events;
+  // launch shape chosen by kl_socs_autotune for batches of tune_clips clips
+  int tcap = 0;  // clip x kernel-slice products the spectra buffer holds
+  int tune_clips = 0, tune_nsplit = 0, tune_spc = 0;
 };
+
+namespace kl {
+// one forward pass of a plan on `st`; ev4 (optional) receives the stage
+// boundaries, otherwise the plan's own timing marks are used
+int socs_run_forward(kl_socs_plan_s* p, const float* masks, int nclips, float* images, cudaStream_t st,
+                     const cudaEvent_t* ev4);
+}  // namespace kl
 
 struct kl_tcc_plan_s {
   int precision = KL_PREC_FAST;

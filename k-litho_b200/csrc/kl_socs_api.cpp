@@ -51,19 +51,44 @@ int mark(kl_socs_plan p, cudaStream_t st) {
   return KL_OK;
 }
 
-int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st) {
+int stage_mark(kl_socs_plan p, cudaStream_t st, const cudaEvent_t* ev4, int i) {
+  if (!ev4) return mark(p, st);
+  // inside a stream capture the record must become an event node of the graph
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  KL_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+  KL_CUDA_TRY(cudaEventRecordWithFlags(ev4[i], st,
+                                       cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal
+                                                                           : cudaEventRecordDefault));
+  return KL_OK;
+}
+
+// the launch shape for a batch of nclips: the autotuned one when it was tuned
+// for this batch size, else the heuristic
+void launch_shape(kl_socs_plan p, int nclips, int* nsplit, int* spc) {
+  if (p->tune_clips == nclips && p->tune_nsplit > 0) {
+    *nsplit = p->tune_nsplit;
+    *spc = p->tune_spc;
+  } else {
+    *nsplit = kl::socs_choose_split(p->g, nclips, p->nsets, p->K);
+    *spc = 0;
+  }
+}
+
+int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st,
+                const cudaEvent_t* ev4 = nullptr) {
   int rc;
-  if ((rc = mark(p, st))) return rc;
-  const int nsplit = kl::socs_choose_split(p->g, nclips, p->nsets, p->K);
+  if ((rc = stage_mark(p, st, ev4, 0))) return rc;
+  int nsplit, spc;
+  launch_shape(p, nclips, &nsplit, &spc);
   if ((rc = kl::socs_launch_forward(p->g, p->tx, p->ty, masks, nclips, p->partial, st))) return rc;
-  if ((rc = mark(p, st))) return rc;
+  if ((rc = stage_mark(p, st, ev4, 1))) return rc;
   rc = kl::socs_launch_spectral(p->g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, nsplit,
                                 p->T, st);
   if (rc) return rc;
-  if ((rc = mark(p, st))) return rc;
-  rc = kl::socs_launch_inverse(p->g, p->tx, p->ty, p->T, nclips, p->nsets, nsplit, images, st);
+  if ((rc = stage_mark(p, st, ev4, 2))) return rc;
+  rc = kl::socs_launch_inverse(p->g, p->tx, p->ty, p->T, nclips, p->nsets, nsplit, images, st, spc);
   if (rc) return rc;
-  return mark(p, st);
+  return stage_mark(p, st, ev4, 3);
 }
 int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
                 int max_clips, bool adjoint) {
@@ -100,6 +125,7 @@ int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int 
     const int c = n * kl::socs_choose_split(g, n, nsets, nk);
     tcap = c > tcap ? c : tcap;
   }
+  p->tcap = tcap;
   if ((rc = alloc((void**)&p->T, kl::socs_spectrum_bytes(g, tcap, nsets, 1), "spectra")) ||
       (rc = kl::socs_build_tables(g, p->tx, p->ty, nullptr))) {
     free_plan(p);
@@ -125,6 +151,11 @@ int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int 
   return KL_OK;
 }
 }  // namespace
+
+int kl::socs_run_forward(kl_socs_plan_s* p, const float* masks, int nclips, float* images, cudaStream_t st,
+                         const cudaEvent_t* ev4) {
+  return run_forward(p, masks, nclips, images, st, ev4);
+}
 
 extern "C" {
 

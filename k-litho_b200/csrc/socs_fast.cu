@@ -554,7 +554,7 @@ int launch_fwd(const SocsGeom& g, const float2* tx, const float2* ty, const floa
 
 template <int P, int V, int NBM, int RJ>
 int launch_inv(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T, int nimg,
-               int nsplit, float* images, cudaStream_t st) {
+               int nsplit, float* images, cudaStream_t st, int spc) {
   size_t sm = sizeof(float2) * ((size_t)NBM * V + (size_t)32 * RJ * (NBM + 1) +
                                 (size_t)g.nty * g.ntx + g.nty);
   auto kern = k_socs_inverse<P, V, NBM, RJ>;
@@ -562,8 +562,11 @@ int launch_inv(const SocsGeom& g, const float2* tx, const float2* ty, const floa
   if (rc) return rc;
   // strips per CTA: the image's spectrum and the twiddle table are loaded once
   // per CTA, so give each CTA several strips while keeping >= 4 CTAs per SM
-  int spc = 1;
-  while (spc < 8 && spc * 2 <= g.nS && (long long)nimg * ((g.nS + 2 * spc - 1) / (2 * spc)) >= 4 * 148) spc *= 2;
+  if (spc <= 0) {
+    spc = 1;
+    while (spc < 8 && spc * 2 <= g.nS && (long long)nimg * ((g.nS + 2 * spc - 1) / (2 * spc)) >= 4 * 148) spc *= 2;
+  }
+  spc = spc < g.nS ? spc : g.nS;
   kern<<<dim3((g.nS + spc - 1) / spc, nimg), kThreads, sm, st>>>(T, g, tx, ty, nsplit, spc, images);
   return check_launch("k_socs_inverse");
 }
@@ -616,12 +619,12 @@ int socs_launch_spectral(const SocsGeom& g, const float2* partial, int nclips, c
 }
 
 int socs_launch_inverse(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T,
-                        int nclips, int nsets, int nsplit, float* images, cudaStream_t st) {
+                        int nclips, int nsets, int nsplit, float* images, cudaStream_t st, int spc) {
   if (nclips <= 0) return KL_OK;
   const int RJ = g.J / 32, nimg = nclips * nsets;
 #define KL_INV(P_, V_, N_, R_)                               \
   if (g.P == P_ && g.V == V_ && g.NBM == N_ && RJ == R_) \
-    return launch_inv<P_, V_, N_, R_>(g, tx, ty, T, nimg, nsplit, images, st);
+    return launch_inv<P_, V_, N_, R_>(g, tx, ty, T, nimg, nsplit, images, st, spc);
   KL_PV_LIST(KL_INV, 32, 1)
   KL_PV_LIST(KL_INV, 32, 2)
   KL_PV_LIST(KL_INV, 64, 1)

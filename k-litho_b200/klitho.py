@@ -100,6 +100,13 @@ def lib() -> ctypes.CDLL:
         L.kl_socs_vjp.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                   _vp, _vp, _vp, _vp]
         L.kl_socs_vjp_source.argtypes = [_vp, _vp, _vp, _vp]
+        L.kl_socs_autotune.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, _c_int_p, _c_int_p]
+        L.kl_socs_batch_create.argtypes = [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int]
+        L.kl_socs_batch_destroy.argtypes = [_vp]
+        L.kl_socs_batch_forward.argtypes = [_vp, ctypes.POINTER(_vp), _c_int_p, ctypes.POINTER(_vp), _vp]
+        L.kl_socs_batch_enable_timing.argtypes = [_vp, ctypes.c_int]
+        L.kl_socs_batch_stage_times.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+        L.kl_socs_batch_graph_builds.argtypes = [_vp]
         L.kl_socs_enable_timing.argtypes = [_vp, ctypes.c_int]
         L.kl_socs_stage_times.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), _c_int_p]
         _LIB = L
@@ -266,6 +273,16 @@ class SocsPlan:
         check(lib().kl_socs_vjp_source(self._h, tcc_plan._h, _dev_ptr(grad_src_dev),
                                        _stream_ptr(stream)), "kl_socs_vjp_source")
 
+    def autotune(self, masks_dev, images_dev, nclips: int | None = None, stream=None):
+        """Pick the fastest launch shape for batches of nclips clips
+        (kl_socs_autotune); returns (kernel slices, strips per CTA)."""
+        n = masks_dev.shape[0] if nclips is None else nclips
+        ns, spc = ctypes.c_int(), ctypes.c_int()
+        check(lib().kl_socs_autotune(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(images_dev),
+                                     _stream_ptr(stream), ctypes.byref(ns), ctypes.byref(spc)),
+              "kl_socs_autotune")
+        return ns.value, spc.value
+
     def enable_timing(self, on: bool = True) -> None:
         check(lib().kl_socs_enable_timing(self._h, int(bool(on))), "kl_socs_enable_timing")
 
@@ -280,6 +297,48 @@ class SocsPlan:
         n = masks_dev.shape[0] if nclips is None else nclips
         check(lib().kl_mask_spectrum(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(band_dev),
                                      _stream_ptr(stream)), "kl_mask_spectrum")
+
+
+class SocsBatch:
+    """Several SOCS plans imaged as concurrent branches of one CUDA graph
+    (kl_socs_batch_*); the plans must stay open while the batch is used."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        h = _vp()
+        arr = (_vp * len(self.plans))(*[p._h for p in self.plans])
+        check(lib().kl_socs_batch_create(ctypes.byref(h), arr, len(self.plans)), "kl_socs_batch_create")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().kl_socs_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, masks_list, images_list, nclips=None, stream=None) -> None:
+        n = len(self.plans)
+        counts = [m.shape[0] for m in masks_list] if nclips is None else list(nclips)
+        m = (_vp * n)(*[_dev_ptr(t) for t in masks_list])
+        o = (_vp * n)(*[_dev_ptr(t) for t in images_list])
+        c = (ctypes.c_int * n)(*counts)
+        check(lib().kl_socs_batch_forward(self._h, m, c, o, _stream_ptr(stream)), "kl_socs_batch_forward")
+
+    def enable_timing(self, on: bool = True) -> None:
+        check(lib().kl_socs_batch_enable_timing(self._h, int(bool(on))), "kl_socs_batch_enable_timing")
+
+    def stage_times(self, i: int):
+        ms = (ctypes.c_double * 3)()
+        check(lib().kl_socs_batch_stage_times(self._h, int(i), ms), "kl_socs_batch_stage_times")
+        return list(ms)
+
+    def graph_builds(self) -> int:
+        return int(lib().kl_socs_batch_graph_builds(self._h))
 
 
 # ---------------------------------------------------------------------------
