@@ -38,7 +38,7 @@ constexpr int kWarps = kThreads / 32;
 // image rows + loss + forward row DFT of G (bins gx in [0, 2Nx])
 // ---------------------------------------------------------------------------
 template <int P, int V, int NBM, int RJ>
-__global__ void __launch_bounds__(kThreads) k_vjp_inverse(const float2* __restrict__ T,
+__global__ void __launch_bounds__(kThreads, 2) k_vjp_inverse(const float2* __restrict__ T,
                                                           const SocsGeom g,
                                                           const float2* __restrict__ tx,
                                                           const float2* __restrict__ ty,
@@ -101,9 +101,14 @@ __global__ void __launch_bounds__(kThreads) k_vjp_inverse(const float2* __restri
   for (int jj = warp; jj < J; jj += kWarps) {
     const size_t roff = (size_t)(s + g.nS * jj) * (V * P);
     const float2* q = Qs + jj * QP;
-    float acc[2 * NBM];
+    // row DFT of G, bins gx in [0, NBM): reduce-scattered over the warp in two
+    // halves of NBM floats, each lane keeping NBM/32 sums per half
+    constexpr int PER = NBM / 32;
+    float red[2][PER];
 #pragma unroll
-    for (int i = 0; i < 2 * NBM; ++i) acc[i] = 0.f;
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int i = 0; i < PER; ++i) red[h][i] = 0.f;
 #pragma unroll 1
     for (int c = 0; c < V / 32; ++c) {
       const int lp = lane + 32 * c;
@@ -134,19 +139,27 @@ __global__ void __launch_bounds__(kThreads) k_vjp_inverse(const float2* __restri
       float2 S[P / 2 + 1];
       rdft_reg<P>(o, S);
 #pragma unroll
-      for (int gx = 0; gx < NBM; ++gx) {
-        const int k = gx % P;
-        const float2 sv = (k <= P / 2) ? S[k] : cconj(S[P - k]);
-        const float2 w = tw[gx * V + lp];
-        acc[2 * gx] = fmaf(sv.x, w.x, fmaf(-sv.y, w.y, acc[2 * gx]));
-        acc[2 * gx + 1] = fmaf(sv.x, w.y, fmaf(sv.y, w.x, acc[2 * gx + 1]));
+      for (int h = 0; h < 2; ++h) {
+        float acc[NBM];
+#pragma unroll
+        for (int j = 0; j < NBM / 2; ++j) {
+          const int gx = h * (NBM / 2) + j;
+          const int k = gx % P;
+          const float2 sv = (k <= P / 2) ? S[k] : cconj(S[P - k]);
+          const float2 w = tw[gx * V + lp];
+          acc[2 * j] = fmaf(sv.x, w.x, -sv.y * w.y);
+          acc[2 * j + 1] = fmaf(sv.x, w.y, sv.y * w.x);
+        }
+        warp_reduce_scatter<NBM>(acc, lane);
+#pragma unroll
+        for (int i = 0; i < PER; ++i) red[h][i] += acc[i];
       }
     }
-    warp_reduce_scatter<2 * NBM>(acc, lane);
-    constexpr int PER = 2 * NBM / 32;
     float* rb = reinterpret_cast<float*>(Gr + jj * NBM);
 #pragma unroll
-    for (int i = 0; i < PER; ++i) rb[lane * PER + i] = acc[i];
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+      for (int i = 0; i < PER; ++i) rb[h * NBM + lane * PER + i] = red[h][i];
   }
   for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
   if (lane == 0) s_loss[warp] = lsum;
