@@ -175,7 +175,8 @@ int kl_socs_plan_create_adjoint(kl_socs_plan* plan, int Lx, int Ly, int Nx, int 
  * SOCS image I of clip c under kernel set s, and grad_dev[c] = dL/dmask
  * summed over the sets (nclips x Ly x Lx float32).  images_dev may be NULL
  * (the image is then not written).  The K coherent fields are recomputed on
- * chip, never stored.  Stream-ordered; loss_dev is device memory. */
+ * chip, never stored.  Stream-ordered; loss_dev is device memory.
+ * targets_dev must be 16-byte aligned (any cudaMalloc or torch allocation is). */
 int kl_socs_vjp(kl_socs_plan plan, const float* masks_dev, const float* targets_dev, int nclips,
                 float alpha, float threshold, float* images_dev, float* grad_dev,
                 double* loss_dev, void* stream);

@@ -1,6 +1,7 @@
 // kl_socs_api.cpp -- C ABI for SOCS imaging plans (see include/klitho_gpu.h).
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstring>
 #include <new>
 #include <string>
@@ -172,6 +173,7 @@ int kl_socs_plan_create_adjoint(kl_socs_plan* plan, int Lx, int Ly, int Nx, int 
 int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nclips, float alpha,
                 float threshold, float* images, float* grad, double* loss, void* stream) {
   KL_CHECK_ARG(p && masks && targets && grad && loss, "kl_socs_vjp: NULL argument");
+  KL_CHECK_ARG((reinterpret_cast<uintptr_t>(targets) & 15) == 0, "kl_socs_vjp: targets_dev must be 16-byte aligned");
   KL_CHECK_ARG(p->adjoint, "kl_socs_vjp: the plan was not created by kl_socs_plan_create_adjoint");
   KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_socs_vjp: nclips exceeds the plan");
   cudaStream_t st = (cudaStream_t)stream;

@@ -22,6 +22,8 @@
 // k_vjp_spectral (per clip and kernel slice: Gam), k_vjp_gradT (Gam -> the
 // half-plane spectrum of the gradient, synthesised by k_socs_inverse), and
 // k_vjp_source (per clip and source slice: dL/dJ).
+#include <cuda_pipeline.h>
+
 #include <climits>
 
 #include "kl_device.cuh"
@@ -56,6 +58,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_vjp_inverse(const float2* __res
   float2* Gr = Qs + J * QP;                        // [J][NBM]  row bins of G
   float2* Ts = Gr + J * NBM;                       // [nty][ntx]
   float2* ph = Ts + g.nty * g.ntx;                 // [nty]
+  // [kWarps][V P] target rows, on a 16-byte boundary (an even float2 offset)
+  const int toff = NBM * V + J * QP + J * NBM + g.nty * g.ntx + g.nty;
+  float* trows = reinterpret_cast<float*>(reinterpret_cast<float2*>(smem4) + toff + (toff & 1));
   __shared__ double s_loss[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int s = blockIdx.x, img = blockIdx.y, clip = img / nsets;
@@ -98,9 +103,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_vjp_inverse(const float2* __res
   float* out = images ? images + (size_t)img * px : nullptr;
   const float* tgt = targets + (size_t)clip * px;
   double lsum = 0.0;
+  float* trow = trows + warp * (V * P);
   for (int jj = warp; jj < J; jj += kWarps) {
     const size_t roff = (size_t)(s + g.nS * jj) * (V * P);
     const float2* q = Qs + jj * QP;
+    // the row's targets go to shared memory asynchronously while the row is
+    // synthesised (16-byte pieces; rows start on 16-byte boundaries)
+    for (int m = lane; m < V * P / 4; m += 32) __pipeline_memcpy_async(trow + 4 * m, tgt + roff + 4 * m, 16);
+    __pipeline_commit();
     // row DFT of G, bins gx in [0, NBM): reduce-scattered over the warp in two
     // halves of NBM floats, each lane keeping NBM/32 sums per half
     constexpr int PER = NBM / 32;
@@ -127,12 +137,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_vjp_inverse(const float2* __res
         re_idft_reg<P>(Z, o);
       }
       // resist model, loss and dL/dI on the lane's pixels
+      __pipeline_wait_prior(0);
+      __syncwarp();
 #pragma unroll
       for (int i = 0; i < P; ++i) {
         const size_t x = roff + lp + V * i;
         if (out) out[x] = o[i];
         const float sg = 1.0f / (1.0f + __expf(-alpha * (o[i] - thr)));
-        const float d = sg - __ldg(tgt + x);
+        const float d = sg - trow[lp + V * i];
         lsum += (double)(d * d);
         o[i] = 2.0f * d * sg * (1.0f - sg) * alpha;
       }
@@ -160,6 +172,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_vjp_inverse(const float2* __res
     for (int h = 0; h < 2; ++h)
 #pragma unroll
       for (int i = 0; i < PER; ++i) rb[h * NBM + lane * PER + i] = red[h][i];
+    __syncwarp();  // every lane has read trow before the next row's copy
   }
   for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
   if (lane == 0) s_loss[warp] = lsum;
@@ -505,8 +518,8 @@ int launch_vinv(const SocsGeom& g, const float2* tx, const float2* ty, const flo
                 int nsplit, int nsets, const float* targets, float alpha, float thr, float* images,
                 double* loss, float2* gpart, cudaStream_t st) {
   constexpr int J = 32 * RJ;
-  size_t sm = sizeof(float2) * ((size_t)NBM * V + (size_t)J * (NBM + 1) + (size_t)J * NBM +
-                                (size_t)g.nty * g.ntx + g.nty);
+  const size_t toff = (size_t)NBM * V + (size_t)J * (NBM + 1) + (size_t)J * NBM + (size_t)g.nty * g.ntx + g.nty;
+  size_t sm = sizeof(float2) * (toff + (toff & 1)) + sizeof(float) * (size_t)kWarps * V * P;
   auto kern = k_vjp_inverse<P, V, NBM, RJ>;
   int rc = set_smem(kern, sm);
   if (rc) return rc;
