@@ -24,6 +24,7 @@
 // k_vjp_source (per clip and source slice: dL/dJ).
 #include <cuda_pipeline.h>
 
+#include <algorithm>
 #include <climits>
 
 #include "kl_device.cuh"
@@ -317,13 +318,14 @@ __global__ void __launch_bounds__(kThreads) k_vjp_spectral(const float2* __restr
   constexpr int G = 32 * RG, GP = G + 1;
   extern __shared__ float4 smem4[];
   const int nb2 = g.nby * g.nbx;
-  const int W = 4 * g.Nx + 1;
   float2* Cm = reinterpret_cast<float2*>(smem4);    // [nby][nbx]
   float2* Gacc = Cm + nb2;                           // [nby][nbx]
-  float2* Gb = Gacc + nb2;                           // [nty][W]   (later reused)
-  float2* E1 = Gb + g.nty * W;                       // [max(nby, nty, G)][GP]
-  float2* Wg = E1 + G * GP;                          // [G][GP]
-  float* gam = reinterpret_cast<float*>(Wg + G * GP);  // [G][GP]
+  float2* E1 = Gacc + nb2;                           // [G][GP]  (G >= nby, nty)
+  float* gam = reinterpret_cast<float*>(E1 + G * GP);  // [G][GP]
+  // the band of dL/dI is read only while gam is made; the per-kernel stages
+  // then reuse its space (two CTAs per SM at 1024^2)
+  float2* Gb = reinterpret_cast<float2*>(gam + G * GP);  // [nty][W]
+  float2* Wg = Gb;                                        // [G][GP]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int clip = blockIdx.x, set = blockIdx.y, split = blockIdx.z;
   const int nsets = gridDim.y, nsplit = gridDim.z;
@@ -530,8 +532,8 @@ int launch_vinv(const SocsGeom& g, const float2* tx, const float2* ty, const flo
 
 size_t vjp_spectral_smem(const SocsGeom& g) {
   const int G = g.G, GP = G + 1, nb2 = g.nby * g.nbx, W = 4 * g.Nx + 1;
-  return sizeof(float2) * ((size_t)2 * nb2 + (size_t)g.nty * W + (size_t)2 * G * GP) +
-         sizeof(float) * (size_t)G * GP;
+  const size_t shared = std::max((size_t)g.nty * W, (size_t)G * GP);  // dL/dI band, then Wg
+  return sizeof(float2) * ((size_t)2 * nb2 + (size_t)G * GP + shared) + sizeof(float) * (size_t)G * GP;
 }
 size_t vjp_source_smem(const SocsGeom& g) {
   const int G = g.G, GP = G + 1, nb2 = g.nby * g.nbx, W = 4 * g.Nx + 1;
