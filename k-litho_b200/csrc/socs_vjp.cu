@@ -140,15 +140,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_vjp_inverse(const float2* __res
       // resist model, loss and dL/dI on the lane's pixels
       __pipeline_wait_prior(0);
       __syncwarp();
+      float rsum = 0.f;  // the lane's P pixels; added to the double total once per row
 #pragma unroll
       for (int i = 0; i < P; ++i) {
         const size_t x = roff + lp + V * i;
         if (out) out[x] = o[i];
-        const float sg = 1.0f / (1.0f + __expf(-alpha * (o[i] - thr)));
+        const float sg = __frcp_rn(1.0f + __expf(-alpha * (o[i] - thr)));
         const float d = sg - trow[lp + V * i];
-        lsum += (double)(d * d);
+        rsum = fmaf(d, d, rsum);
         o[i] = 2.0f * d * sg * (1.0f - sg) * alpha;
       }
+      lsum += (double)rsum;
       float2 S[P / 2 + 1];
       rdft_reg<P>(o, S);
 #pragma unroll
