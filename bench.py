@@ -293,6 +293,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
         secondary["fwd_adj"] = bench_fwd_adj(args, stream, peaks()[0])
         secondary["tcc_eigen"] = bench_tcc_eigen(args)
+        secondary["tcc_eigen_large"] = bench_tcc_eigen_large(args)
 
     if rank == 0:
         out = {
@@ -513,6 +514,63 @@ def bench_tcc_eigen(args):
                       "the fast eigensolve and is timed separately"}
 
 
+def bench_tcc_eigen_large(args):
+    """TCC + top-K eigen at the stress field: 4096^2, cross-quadrupole
+    (0.75, 0.12) on an 81^2 grid (196 source points), NA 1.35 water, K = 64,
+    block 96.  Fast path: FP32 factor + subspace iteration on A(A^H X) with
+    FP64 CholeskyQR2 and Rayleigh-Ritz (S > 128, so no one-step Gram solve);
+    five focus values.  Plain FP64 GPU path: FP64 TCC by direct accumulation
+    (N = 11449, 2.1 GB) and FP64 subspace iteration on the dense TCC, at one
+    focus value (seconds per focus)."""
+    import torch
+    import klitho as K
+    import synth
+    L, nk, blk = 4096, 64, 96
+    src = K.createSource(81, "CrossQuadrupole", radius=0.12, offset=0.75)
+    focus = [-50.0, -25.0, 0.0, 25.0, 50.0]
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    # warm-up of both paths at this size (memory pool growth, first launches)
+    for prec in (K.PREC_FAST, K.PREC_FP64):
+        w = K.TccPlan(src, 1.35, 0.0, L, L, n_medium=synth.N_WATER, precision=prec)
+        w.topk(nk, block=blk)
+        w.close()
+    fast_t, its, evs = [], [], []
+    for f_nm in focus:
+        def fast():
+            tp = K.TccPlan(src, 1.35, synth.defocus_arg(f_nm), L, L, n_medium=synth.N_WATER)
+            r = tp.topk(nk, block=blk)
+            N, S = tp.N, tp.S
+            tp.close()
+            return r, N, S
+        ((krn, sc, ev, it), N, S), t = timed(fast)
+        fast_t.append(t)
+        its.append(it)
+        evs.append(ev)
+
+    def fp64():
+        tq = K.TccPlan(src, 1.35, synth.defocus_arg(focus[2]), L, L, n_medium=synth.N_WATER,
+                       precision=K.PREC_FP64)
+        r = tq.topk(nk, block=blk)
+        tq.close()
+        return r
+    (k64, s64, ev64, it64), t64 = timed(fp64)
+    f = float(np.median(fast_t))
+    return {"metric": "TCC + top-K eigen seconds per focus (4096^2 cross-quadrupole, K=64)",
+            "fast_s": round(f, 4), "fast_s_each": [round(x, 4) for x in fast_t],
+            "fp64_gpu_s": round(t64, 4), "speedup_vs_fp64_gpu": round(t64 / f, 2),
+            "N": N, "S": S, "subspace_iterations": its, "fp64_iterations": it64,
+            "eigenvalue_rel_err_vs_fp64": float(np.max(np.abs(evs[2] - ev64)) / np.max(np.abs(ev64))),
+            "timing": "wall clock per focus incl. plan, eigen-solve and kernel download, after a warm-up "
+                      "solve of each path; FP64 at focus 0 only"}
+
+
 def run_e2e(plans, masks_h, args, ws, img_equiv):
     import torch
     steps = max(1, min(args.steps, args.e2e_steps))
@@ -626,6 +684,8 @@ def run_part(args):
     torch.cuda.set_device(0)
     if args.part == "fwd_adj":
         r = bench_fwd_adj(args, torch.cuda.current_stream(), peaks()[0])
+    elif args.part == "tcc_eigen_large":
+        r = bench_tcc_eigen_large(args)
     else:
         r = bench_tcc_eigen(args)
     print(json.dumps(r))
@@ -646,7 +706,7 @@ def main():
     ap.add_argument("--only", type=int, default=0,
                     help="restrict to one clip size (profiling cases)")
     ap.add_argument("--clips", type=int, default=0, help="clip count for --only")
-    ap.add_argument("--part", choices=["all", "fwd_adj", "tcc_eigen"], default="all",
+    ap.add_argument("--part", choices=["all", "fwd_adj", "tcc_eigen", "tcc_eigen_large"], default="all",
                     help="run one secondary measurement alone (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -645,6 +645,10 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
         converged = true;
         break;
       }
+      // continue from the Ritz basis: the next projected matrix is then nearly
+      // diagonal and its Jacobi solve takes a few sweeps
+      if ((rc = zgemm<G_NN>(ws.X, B, ws.Q, B, ws.W, B, N, B, B, st))) return rc;
+      KL_CUDA_TRY(cudaMemcpyAsync(ws.X, ws.W, sizeof(double2) * (size_t)N * B, cudaMemcpyDeviceToDevice, st));
     }
     if ((rc = apply(ws.X, ws.W))) return rc;
     KL_CUDA_TRY(cudaMemcpyAsync(ws.X, ws.W, sizeof(double2) * (size_t)N * B, cudaMemcpyDeviceToDevice, st));
