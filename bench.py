@@ -148,15 +148,17 @@ def run_ours(args):
     # kernel sets: config-0 optics (annular 0.6/0.9 on 41^2, NA 1.35, water) at
     # each clip size and focus, K=24, from the GPU TCC + subspace iteration
     src = K.createSource(41, "Annular", 0.6, 0.9)
-    plans, masks_d, imgs_d, masks_h, kset0 = [], [], [], [], []
+    plans, masks_d, imgs_d, masks_h, kset0, ksets = [], [], [], [], [], []
     for ci, (L, n) in enumerate(CLASSES):
         Nx, Ny = class_band(L)
         p = K.SocsPlan(L, L, Nx, Ny, NK, nsets=len(FOCUS_NM), max_clips=n)
+        ksets_cur = []
         for s, f_nm in enumerate(FOCUS_NM):
             tp = K.TccPlan(src, 1.35, synth.defocus_arg(f_nm), L, L, n_medium=synth.N_WATER)
             krn, sc, _, _ = tp.topk(NK)
             tp.close()
             p.set_kernels(s, krn, sc)
+            ksets_cur.append((krn, sc))
             if s == 0:
                 kset0.append((krn, sc))
         m = make_masks(L, n, SEED + 1000 * ci + rank)
@@ -165,16 +167,33 @@ def run_ours(args):
         imgs_d.append(torch.empty((n, len(FOCUS_NM), L, L), dtype=torch.float32,
                                   device=f"cuda:{local}"))
         plans.append(p)
+        ksets.append(list(ksets_cur))
     px_per_step = sum(L * L * n * len(FOCUS_NM) for L, n in CLASSES)
     img_equiv = px_per_step / float(1024 * 1024)
 
     # launch shapes tuned per size class, then all classes in one graph whose
-    # branches run concurrently (kl_socs_autotune + kl_socs_batch_forward)
+    # branches run concurrently (kl_socs_autotune + kl_socs_batch_forward);
+    # the larger classes are split into CHUNKS plans over contiguous clip
+    # ranges so that one chunk's on-chip stage overlaps another's memory-bound
+    # stages
     tuned = [p.autotune(md, im, stream=stream) for p, md, im in zip(plans, masks_d, imgs_d)]
-    batch = K.SocsBatch(plans)
+    bplans, bmasks, bimgs = [], [], []
+    for (L, n), md, im, ks in zip(CLASSES, masks_d, imgs_d, ksets):
+        nch = max(1, min(args.chunks if L >= 1024 else 1, n))
+        Nx, Ny = class_band(L)
+        for c in range(nch):
+            a, b = n * c // nch, n * (c + 1) // nch
+            bp = K.SocsPlan(L, L, Nx, Ny, NK, nsets=len(FOCUS_NM), max_clips=b - a)
+            for si, (krn, sc) in enumerate(ks):
+                bp.set_kernels(si, krn, sc)
+            bp.autotune(md[a:b], im[a:b], stream=stream)
+            bplans.append(bp)
+            bmasks.append(md[a:b])
+            bimgs.append(im[a:b])
+    batch = K.SocsBatch(bplans)
 
     def step():
-        batch.forward(masks_d, imgs_d, stream=stream)
+        batch.forward(bmasks, bimgs, stream=stream)
 
     clocks = ClockSampler(local)
     clocks.start()
@@ -218,13 +237,13 @@ def run_ours(args):
     # ... and their spans inside the graph, where the size classes overlap
     # (stage events captured into a separate graph)
     batch.enable_timing(True)
-    spans = [np.zeros(3) for _ in plans]
+    spans = [np.zeros(3) for _ in bplans]
     for _ in range(tsteps):
         step()
-        for i in range(len(plans)):
+        for i in range(len(bplans)):
             spans[i] += np.array(batch.stage_times(i))
-    for pc, sp in zip(per_class, spans):
-        pc["in_graph_span_ms"] = [round(x / tsteps, 4) for x in sp]
+    branches = [{"L": bp.Lx, "clips": int(bm.shape[0]), "span_ms": [round(x / tsteps, 4) for x in sp]}
+                for bp, bm, sp in zip(bplans, bmasks, spans)]
     batch.enable_timing(False)
     if dist:
         t = torch.tensor([ms], device=f"cuda:{local}")
@@ -284,6 +303,8 @@ def run_ours(args):
         fp64 = fp64_baseline(masks_d, kset0, value / ws, img_equiv)
 
     batch.close()
+    for bp in bplans:
+        bp.close()
     secondary = {}
     if not args.no_secondary:
         for p in plans:
@@ -308,9 +329,9 @@ def run_ours(args):
                        "image_equiv_1024_per_step_per_gpu": img_equiv,
                        "l2": "inputs larger than L2 (1.9 GB masks, 5.8 GB images per GPU)",
                        "parallelism": f"clip sharding, {ws} GPU(s), no collective on the data path"},
-            "roofline": roof, "stages": other, "per_class": per_class,
+            "roofline": roof, "stages": other, "per_class": per_class, "graph_branches": branches,
             "clocks": clk, "e2e": e2e,
-            "gpu_launches": int(3 * len(CLASSES) * args.steps),
+            "gpu_launches": int(3 * len(bplans) * args.steps),
             "cpu_baseline": cpu,
             "fp64_gpu_baseline": fp64,
             "secondary": secondary,
@@ -706,6 +727,8 @@ def main():
     ap.add_argument("--only", type=int, default=0,
                     help="restrict to one clip size (profiling cases)")
     ap.add_argument("--clips", type=int, default=0, help="clip count for --only")
+    ap.add_argument("--chunks", type=int, default=1,
+                    help="plans per size class (>= 1024^2) in the timed graph")
     ap.add_argument("--part", choices=["all", "fwd_adj", "tcc_eigen", "tcc_eigen_large"], default="all",
                     help="run one secondary measurement alone (profiling cases)")
     args = ap.parse_args()
