@@ -271,8 +271,8 @@ def run_ours(args):
                 "frac": round(achieved / peak, 4),
                 "traffic": (int(TRAFFIC_PER_ALGORITHMIC_BYTE[names[dom]] * bytes_per_step[dom] / launches_per_step)
                             if names[dom] in TRAFFIC_PER_ALGORITHMIC_BYTE else None),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 48 x 1024^2 "
-                                  "capture (profiles/socs_kernels_1024x48_full.md), scaled by pixels",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2048^2 and "
+                                  "1024^2 captures (profiles/socs_inverse_full.md), scaled by pixels",
                 "algorithmic_bytes_per_launch": int(bytes_per_step[dom] / launches_per_step)}
     else:
         roof = {"kernel": names[dom], "bound": "compute", "achieved": None, "peak": None,
@@ -346,9 +346,10 @@ def run_ours(args):
 
 
 # DRAM bytes per algorithmic byte measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) on 48 clips of 1024^2 x 3 kernel sets; both kernels
-# stream their clip data once, so traffic scales with the pixels of a launch.
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"socs_inverse": (6.695 + 546.386) / 603.98,
+# dram__bytes_write.sum): synthesis on 48 x 2048^2 + 144 x 1024^2 images, forward
+# on 48 clips of 1024^2; both kernels stream their clip data once, so traffic
+# scales with the pixels of a launch.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"socs_inverse": (3.376 + 544.117 + 4.802 + 749.687) / (603.98 + 805.31),
                                 "socs_forward": (201.372 + 4.389) / 201.33}
 
 
