@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double2* __restrict__ G,
 constexpr int kJacobiThreads = 1024;
 constexpr int kJacobiMaxSweeps = 40;
 constexpr int kJacobiMaxJobs = 16;
-constexpr int kGramMaxS = 128;  // factor widths solved by one Gram eigensolve
+constexpr int kGramMaxS = 256;  // factor widths solved by one Gram eigensolve (pair tables hold bytes)
 
 struct JacobiJob {
   double2* H;    // B x B Hermitian input (overwritten when worked in place)
@@ -447,15 +447,31 @@ __global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiJobs jobs, int 
 // independently (entries p, q of the row mix under pair (p, q)), so each warp
 // replays the log on one row held in shared memory, two pairs per lane.
 constexpr int kVecWarps = 8;
-constexpr int kVecChunk = 32;  // logged steps staged per pass
+constexpr int kVecChunkMax = 32;  // logged steps staged per pass (fewer for large B)
+
+int jacobi_vectors_chunk(int B) {
+  const int Bp = B + (B & 1), npairs = Bp / 2;
+  const size_t fixed = sizeof(double2) * kVecWarps * B + sizeof(uchar2) * (Bp - 1) * npairs + 16;
+  const size_t budget = 200 * 1024;
+  const int c = (int)((budget - std::min(budget, fixed)) / (sizeof(double4) * npairs));
+  return std::max(1, std::min(kVecChunkMax, c));
+}
 
 size_t jacobi_vectors_smem(int B) {
   const int Bp = B + (B & 1), npairs = Bp / 2;
-  return sizeof(double4) * kVecChunk * npairs + sizeof(double2) * kVecWarps * B +
+  return sizeof(double4) * jacobi_vectors_chunk(B) * npairs + sizeof(double2) * kVecWarps * B +
          ((sizeof(uchar2) * (Bp - 1) * npairs + 15) & ~size_t(15));
 }
 
-__global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jobs) {
+__device__ __forceinline__ void replay_pair(double2* row, int B, uchar2 pq, double4 u) {
+  const int p = pq.x, q = pq.y;
+  if (q >= B) return;
+  const double2 vp = row[p], e = zmul(row[q], make_double2(u.z, -u.w));
+  row[p] = make_double2(u.x * vp.x - u.y * e.x, u.x * vp.y - u.y * e.y);
+  row[q] = make_double2(u.y * vp.x + u.x * e.x, u.y * vp.y + u.x * e.y);
+}
+
+__global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jobs, int chunk) {
   extern __shared__ __align__(16) unsigned char vsm[];
   const JacobiJob job = jobs.j[blockIdx.y];
   const int B = job.B;
@@ -464,19 +480,18 @@ __global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jo
   const int* __restrict__ jst = job.jst;
   double2* __restrict__ Q = job.Q;
   const int Bp = B + (B & 1), npairs = Bp / 2;
-  double4* lg = reinterpret_cast<double4*>(vsm);                       // kVecChunk x npairs
-  double2* rows = reinterpret_cast<double2*>(lg + kVecChunk * npairs);  // kVecWarps x B
-  uchar2* ptab = reinterpret_cast<uchar2*>(rows + kVecWarps * B);       // (Bp - 1) x npairs
+  double4* lg = reinterpret_cast<double4*>(vsm);                   // chunk x npairs
+  double2* rows = reinterpret_cast<double2*>(lg + chunk * npairs);  // kVecWarps x B
+  uchar2* ptab = reinterpret_cast<uchar2*>(rows + kVecWarps * B);   // (Bp - 1) x npairs
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int k = blockIdx.x * kVecWarps + warp;
   double2* row = rows + warp * B;
   for (int p = lane; p < B; p += 32) row[p] = make_double2(p == k ? 1.0 : 0.0, 0.0);
   jacobi_pair_table(ptab, Bp);
   const int nsteps = jst[0];
-  const bool two = lane + 32 < npairs;
   int step = 0;
-  for (int s0 = 0; s0 < nsteps; s0 += kVecChunk) {
-    const int ns = min(kVecChunk, nsteps - s0);
+  for (int s0 = 0; s0 < nsteps; s0 += chunk) {
+    const int ns = min(chunk, nsteps - s0);
     __syncthreads();
     for (int i = threadIdx.x; i < ns * npairs; i += blockDim.x) lg[i] = rot[(size_t)s0 * npairs + i];
     __syncthreads();
@@ -484,24 +499,13 @@ __global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jo
     for (int j = 0; j < ns; ++j) {
       const uchar2* pr = ptab + step * npairs;
       const double4* uj = lg + j * npairs;
-      if (lane < npairs) {
-        const int p0 = pr[lane].x, q0 = pr[lane].y;
-        const int p1 = two ? pr[lane + 32].x : p0, q1 = two ? pr[lane + 32].y : q0;
-        const bool ok0 = q0 < B, ok1 = two && q1 < B;
-        const double4 u0 = uj[lane];
-        const double4 u1 = two ? uj[lane + 32] : u0;
-        const double2 vp0 = row[p0], vq0 = ok0 ? row[q0] : vp0;
-        const double2 vp1 = row[p1], vq1 = ok1 ? row[q1] : vp1;
-        const double2 e0 = zmul(vq0, make_double2(u0.z, -u0.w));
-        const double2 e1 = zmul(vq1, make_double2(u1.z, -u1.w));
-        if (ok0) {
-          row[p0] = make_double2(u0.x * vp0.x - u0.y * e0.x, u0.x * vp0.y - u0.y * e0.y);
-          row[q0] = make_double2(u0.y * vp0.x + u0.x * e0.x, u0.y * vp0.y + u0.x * e0.y);
-        }
-        if (ok1) {
-          row[p1] = make_double2(u1.x * vp1.x - u1.y * e1.x, u1.x * vp1.y - u1.y * e1.y);
-          row[q1] = make_double2(u1.y * vp1.x + u1.x * e1.x, u1.y * vp1.y + u1.x * e1.y);
-        }
+      // disjoint pairs: each lane takes pairs lane, lane + 32, ... (two at a time)
+      for (int t = lane; t < npairs; t += 64) {
+        const bool two = t + 32 < npairs;
+        const uchar2 a = pr[t], b = two ? pr[t + 32] : make_uchar2(0, 255);
+        const double4 ua = uj[t], ub = two ? uj[t + 32] : ua;
+        replay_pair(row, B, a, ua);
+        if (two) replay_pair(row, B, b, ub);
       }
       __syncwarp();
       if (++step == Bp - 1) step = 0;
@@ -587,7 +591,8 @@ int jacobi_batch(const std::vector<JacobiJob>& all, cudaStream_t st) {
     const size_t vsm = jacobi_vectors_smem(bmax);
     if (vsm > 48 * 1024)
       KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
-    k_jacobi_vectors<<<dim3((bmax + kVecWarps - 1) / kVecWarps, nj), 32 * kVecWarps, vsm, st>>>(jobs);
+    k_jacobi_vectors<<<dim3((bmax + kVecWarps - 1) / kVecWarps, nj), 32 * kVecWarps, vsm, st>>>(
+        jobs, jacobi_vectors_chunk(bmax));
     KL_CUDA_TRY(cudaGetLastError());
   }
   return KL_OK;

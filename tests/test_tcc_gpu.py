@@ -31,6 +31,9 @@ CASES = {
                    synth.defocus_arg(-50.0), 32),
     "dry_na08": (512, "Annular", 41, dict(innerRadius=0.5, outerRadius=0.8), 0.8, 1.0, 0.2, 12),
     "quad512": (512, "CrossQuadrupole", 41, dict(radius=0.12, offset=0.75), 1.35, 1.44, 0.0, 16),
+    # 196 source points: the one-step Gram solve with the Jacobi matrix in global memory
+    "quad81_512": (512, "CrossQuadrupole", 81, dict(radius=0.12, offset=0.75), 1.35, 1.44,
+                   synth.defocus_arg(30.0), 32),
 }
 
 _oracle_cache = {}
