@@ -89,6 +89,18 @@ int kl_write_kernel_info(const char* path, int krnSizeX, int krnSizeY, int nk,
 int kl_read_kernel_info(const char* path, int* krnSizeX, int* krnSizeY, int* nk, float* scales,
                         int cap);
 
+/* writeFloatArrayToPNGWithGrayscale / ...With7Colors / ...WithContinuousColor:
+ * common/file_io.cpp:7-135.  colormap 0 = grey, 1 = seven colours, 2 =
+ * continuous colour, each over [min, max] with the reference's pixel
+ * arithmetic; data is sizeY rows of sizeX floats.  The file is encoded by
+ * the library (zlib deflate), so only the decoded pixels equal the
+ * reference's. */
+#define KL_PNG_GRAY 0
+#define KL_PNG_7COLORS 1
+#define KL_PNG_CONTINUOUS 2
+int kl_write_png(const char* path, const float* data, int sizeX, int sizeY, float min, float max,
+                 int colormap);
+
 /* ------------------------------------------------------------------------- */
 /* SOCS imaging: K-Litho-SOCS/klitho_socs.cpp:196-241 (calcSOCS) + :158-194   */
 /* (FI), fed by FT_r2c :70-121.  Fused single-precision path.                 */
@@ -281,6 +293,10 @@ int kl_tcc_minmax(kl_tcc_plan plan, const void* tcc_dev, double* out4, void* str
  * and release it (what klitho_tcc prints; the TCC itself is not an output of
  * the reference program). */
 int kl_tcc_build_minmax(kl_tcc_plan plan, double* out4);
+/* The TCC as two host float planes (N x N each, row f1, column f2): the
+ * tccReal / tccImag arrays klitho_tcc.cpp:517-529 turns into tcc_r.png /
+ * tcc_i.png.  Synchronous. */
+int kl_tcc_build_host(kl_tcc_plan plan, float* re_host, float* im_host);
 
 /* calcKernels (klitho_tcc.cpp:300-377): top-nk eigenpairs of the TCC by
  * blocked subspace iteration (block `block`, 0 = automatic) with FP64

@@ -5,7 +5,9 @@
 #include <chrono>
 #include <iostream>
 #include <sstream>
+#include <cstdlib>
 #include <string>
+#include <vector>
 
 #include "klitho_gpu.h"
 
@@ -40,6 +42,34 @@ inline std::string mask_params(int Lx, int Ly, int msx, int msy, const std::stri
      << "\nMask Type: " << type << "\n";
   if (type == "LineSpace") ss << "Line Width: " << lw << "\nSpace Width: " << sw << "\n";
   return ss.str();
+}
+
+// the reference's optional PNG outputs (common/file_io.cpp:7-135); KLITHO_PNG=0
+// skips them
+inline bool png_enabled() {
+  const char* e = std::getenv("KLITHO_PNG");
+  return !(e && std::string(e) == "0");
+}
+
+inline float min_of(const std::vector<float>& v) {
+  float m = v.empty() ? 0.f : v[0];
+  for (float x : v) m = x < m ? x : m;
+  return m;
+}
+inline float max_of(const std::vector<float>& v) {
+  float m = v.empty() ? 0.f : v[0];
+  for (float x : v) m = x > m ? x : m;
+  return m;
+}
+
+// writes a PNG like the reference: on failure, the message and exit(1)
+inline void png(const std::string& path, const std::vector<float>& data, int sx, int sy, float mn, float mx,
+                int colormap) {
+  if (!png_enabled()) return;
+  if (kl_write_png(path.c_str(), data.data(), sx, sy, mn, mx, colormap) != KL_OK) {
+    std::cerr << kl_last_error() << std::endl;
+    std::exit(1);
+  }
 }
 
 inline int fail(const char* what) {

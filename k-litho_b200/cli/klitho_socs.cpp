@@ -11,6 +11,9 @@
 
 #include "cli_common.h"
 
+// TARGET_INTENSITY of klitho_socs.cpp:275, the top of image_s.png's colour scale
+constexpr float kTargetIntensity = 0.225f;
+
 int main(int argc, char* argv[]) {
   klcli::banner_start();
   auto start = std::chrono::system_clock::now();
@@ -64,6 +67,7 @@ int main(int argc, char* argv[]) {
   if (kl_create_mask(Lx, Ly, msx, msy, maskType.c_str(), lineWidth, spaceWidth, isHorizontal,
                      maskFile.c_str(), 1.0f, msk.data()) != KL_OK)
     return 1;
+  klcli::png("./out/mask.png", msk, Lx, Ly, klcli::min_of(msk), klcli::max_of(msk), KL_PNG_GRAY);
 
   std::cout << std::endl << "Simulation Parameters:" << std::endl;
   std::cout << "-------------------" << std::endl;
@@ -83,10 +87,11 @@ int main(int argc, char* argv[]) {
     return klcli::fail("kl_socs_forward_host");
   kl_socs_plan_destroy(plan);
 
-  float mx = -1e+30f;
-  for (float v : img) mx = v > mx ? v : mx;
+  const float mx = klcli::max_of(img), mn = klcli::min_of(img);
   std::cout << "Max. Intensity: " << mx << std::endl;
   if (kl_write_float_file("./out/image.bin", img.data(), Lx * Ly) != KL_OK) std::exit(1);
+  klcli::png("./out/image.png", img, Lx, Ly, mn, mx, KL_PNG_CONTINUOUS);
+  klcli::png("./out/image_s.png", img, Lx, Ly, 0.0f, kTargetIntensity, KL_PNG_7COLORS);
   klcli::banner_end(start);
   return 0;
 }

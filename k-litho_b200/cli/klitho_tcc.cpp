@@ -17,6 +17,9 @@
 
 #include "cli_common.h"
 
+// TARGET_INTENSITY of klitho_tcc.cpp:442, the top of image_s.png's colour scale
+constexpr float kTargetIntensity = 0.225f;
+
 int main(int argc, char* argv[]) {
   klcli::banner_start();
   auto start = std::chrono::system_clock::now();
@@ -72,6 +75,7 @@ int main(int argc, char* argv[]) {
   if (kl_create_source(srcSize, srcType.c_str(), innerR, outerR, radius, offset, onXAxis ? 1 : 0,
                        ptX, ptY, sourceFile.c_str(), src.data()) != KL_OK)
     std::exit(1);
+  klcli::png("./out/source.png", src, srcSize, srcSize, klcli::min_of(src), klcli::max_of(src), KL_PNG_GRAY);
   std::stringstream ssrc;
   ssrc << "Source Size: " << srcSize << " x " << srcSize << "\nSource Type: " << srcType << "\n";
   if (srcType == "Annular")
@@ -87,6 +91,7 @@ int main(int argc, char* argv[]) {
   if (kl_create_mask(Lx, Ly, msx, msy, maskType.c_str(), lineWidth, spaceWidth, isHorizontal,
                      maskFile.c_str(), dose, msk.data()) != KL_OK)
     std::exit(1);
+  klcli::png("./out/mask.png", msk, Lx, Ly, klcli::min_of(msk), klcli::max_of(msk), KL_PNG_GRAY);
 
   float outerSigma = kl_outer_sigma(src.data(), srcSize);
   if (outerSigma > 1) {
@@ -120,7 +125,17 @@ int main(int argc, char* argv[]) {
     return klcli::fail("kl_tcc_plan_create");
 
   klcli::banner_section("Starting calcTCC...");
-  {
+  if (klcli::png_enabled()) {
+    std::vector<float> tr((size_t)tccSize * tccSize), ti((size_t)tccSize * tccSize);
+    if (kl_tcc_build_host(plan, tr.data(), ti.data()) != KL_OK) return klcli::fail("kl_tcc_build_host");
+    float mx = klcli::max_of(tr), mn = klcli::min_of(tr);
+    std::cout << "Max. TCC Real Value: " << mx << std::endl;
+    klcli::png("./out/tcc_r.png", tr, tccSize, tccSize, mn, mx, KL_PNG_CONTINUOUS);
+    mx = klcli::max_of(ti);
+    mn = klcli::min_of(ti);
+    std::cout << "Max. TCC Imag Value: " << mx << std::endl;
+    klcli::png("./out/tcc_i.png", ti, tccSize, tccSize, mn, mx, KL_PNG_CONTINUOUS);
+  } else {
     double mm[4];
     if (kl_tcc_build_minmax(plan, mm) != KL_OK) return klcli::fail("kl_tcc_build_minmax");
     std::cout << "Max. TCC Real Value: " << (float)mm[0] << std::endl;
@@ -131,10 +146,11 @@ int main(int argc, char* argv[]) {
   {
     std::vector<float> img((size_t)Lx * Ly);
     if (kl_hopkins_image_host(plan, msk.data(), img.data()) != KL_OK) return klcli::fail("kl_hopkins_image_host");
-    float mx = -1e+30f;
-    for (float v : img) mx = v > mx ? v : mx;
+    const float mx = klcli::max_of(img), mn = klcli::min_of(img);
     std::cout << "Max. Intensity: " << mx << std::endl;
     if (kl_write_float_file("./out/image.bin", img.data(), Lx * Ly) != KL_OK) std::exit(1);
+    klcli::png("./out/image.png", img, Lx, Ly, mn, mx, KL_PNG_CONTINUOUS);
+    klcli::png("./out/image_s.png", img, Lx, Ly, 0.0f, kTargetIntensity, KL_PNG_7COLORS);
   }
 
   if (nk > 0) {
@@ -163,6 +179,11 @@ int main(int argc, char* argv[]) {
       if (kl_write_float_file((b + "_r.bin").c_str(), kre.data() + (size_t)i * tccSize, tccSize) != KL_OK ||
           kl_write_float_file((b + "_i.bin").c_str(), kim.data() + (size_t)i * tccSize, tccSize) != KL_OK)
         std::exit(1);
+      const std::vector<float> kr(kre.begin() + (size_t)i * tccSize, kre.begin() + (size_t)(i + 1) * tccSize);
+      const std::vector<float> ki(kim.begin() + (size_t)i * tccSize, kim.begin() + (size_t)(i + 1) * tccSize);
+      const std::string pb = "./out/kernels/png/krn_" + std::to_string(i);
+      klcli::png(pb + "_r.png", kr, 2 * Nx + 1, 2 * Ny + 1, klcli::min_of(kr), klcli::max_of(kr), KL_PNG_CONTINUOUS);
+      klcli::png(pb + "_i.png", ki, 2 * Nx + 1, 2 * Ny + 1, klcli::min_of(ki), klcli::max_of(ki), KL_PNG_CONTINUOUS);
     }
     if (kl_write_kernel_info("./out/kernels/kernel_info.txt", 2 * Nx + 1, 2 * Ny + 1, nk, scales.data()) != KL_OK)
       std::exit(1);

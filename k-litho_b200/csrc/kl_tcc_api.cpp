@@ -205,6 +205,36 @@ int kl_tcc_minmax(kl_tcc_plan p, const void* tcc_dev, double* out4, void* stream
   return kl::tcc_minmax_c64((const float2*)tcc_dev, n, out4, (cudaStream_t)stream);
 }
 
+int kl_tcc_build_host(kl_tcc_plan p, float* re_host, float* im_host) {
+  KL_CHECK_ARG(p && re_host && im_host, "kl_tcc_build_host: NULL argument");
+  const size_t n = (size_t)p->pp.N * p->pp.N;
+  const bool f64 = p->precision == KL_PREC_FP64;
+  void* tcc = nullptr;
+  int rc = kl::scratch_alloc(&tcc, (f64 ? sizeof(double2) : sizeof(float2)) * n, nullptr, "TCC");
+  if (rc) return rc;
+  rc = kl_tcc_build(p, tcc, nullptr);
+  if (!rc) {
+    if (f64) {
+      std::vector<double2> h(n);
+      if (cudaMemcpy(h.data(), tcc, sizeof(double2) * n, cudaMemcpyDeviceToHost) != cudaSuccess) rc = KL_ERR_CUDA;
+      for (size_t i = 0; i < n && !rc; ++i) {
+        re_host[i] = (float)h[i].x;
+        im_host[i] = (float)h[i].y;
+      }
+    } else {
+      std::vector<float2> h(n);
+      if (cudaMemcpy(h.data(), tcc, sizeof(float2) * n, cudaMemcpyDeviceToHost) != cudaSuccess) rc = KL_ERR_CUDA;
+      for (size_t i = 0; i < n && !rc; ++i) {
+        re_host[i] = h[i].x;
+        im_host[i] = h[i].y;
+      }
+    }
+    if (rc) kl::set_error(std::string("kl_tcc_build_host: ") + cudaGetErrorString(cudaGetLastError()));
+  }
+  kl::scratch_free(tcc, nullptr);
+  return rc;
+}
+
 int kl_tcc_build_minmax(kl_tcc_plan p, double* out4) {
   KL_CHECK_ARG(p && out4, "kl_tcc_build_minmax: NULL argument");
   const size_t n = (size_t)p->pp.N * p->pp.N;

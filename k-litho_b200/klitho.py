@@ -100,6 +100,8 @@ def lib() -> ctypes.CDLL:
         L.kl_socs_vjp.argtypes = [_vp, _vp, _vp, ctypes.c_int, ctypes.c_float, ctypes.c_float,
                                   _vp, _vp, _vp, _vp]
         L.kl_socs_vjp_source.argtypes = [_vp, _vp, _vp, _vp]
+        L.kl_write_png.argtypes = [ctypes.c_char_p, _c_float_p, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                   ctypes.c_float, ctypes.c_int]
         L.kl_socs_autotune.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, _c_int_p, _c_int_p]
         L.kl_socs_batch_create.argtypes = [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int]
         L.kl_socs_batch_destroy.argtypes = [_vp]

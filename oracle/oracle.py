@@ -265,8 +265,18 @@ def ref_tcc():
         L.kref_read_kernel_info.argtypes = [ctypes.c_char_p, _c_int_p, _c_int_p, _c_int_p,
                                             _c_float_p, ctypes.c_int]
         L.kref_read_float_file.argtypes = [ctypes.c_char_p, ctypes.c_int, _c_float_p]
+        L.kref_write_png.argtypes = [ctypes.c_char_p, _c_float_p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_float, ctypes.c_float, ctypes.c_int]
         _REF_TCC = L
     return _REF_TCC
+
+
+def ref_write_png(path, data, mn, mx, mode) -> None:
+    """The reference's PNG writers (common/file_io.cpp:7-135; mode 0 grey,
+    1 seven colours, 2 continuous) on a float32 array (rows x columns)."""
+    d = np.ascontiguousarray(data, dtype=np.float32)
+    ref_tcc().kref_write_png(str(path).encode(), _fp(d), d.shape[1], d.shape[0], float(mn), float(mx),
+                             int(mode))
 
 
 def ref_socs():

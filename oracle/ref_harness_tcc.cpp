@@ -193,4 +193,17 @@ int kref_read_float_file(const char* path, int size, float* out) {
   return (int)d.size();
 }
 
+// the reference's PNG writers (common/file_io.cpp:7-135, stb_image_write):
+// mode 0 grayscale, 1 seven colours, 2 continuous colour
+int kref_write_png(const char* path, const float* data, int sx, int sy, float mn, float mx, int mode) {
+  vector<float> d(data, data + (size_t)sx * sy);
+  if (mode == 0)
+    writeFloatArrayToPNGWithGrayscale(sx, sy, d, mn, mx, string(path));
+  else if (mode == 1)
+    writeFloatArrayToPNGWith7Colors(sx, sy, d, string(path), mn, mx);
+  else
+    writeFloatArrayToPNGWithContinuousColor(sx, sy, d, string(path), mn, mx);
+  return 0;
+}
+
 }  // extern "C"
