@@ -22,6 +22,9 @@ struct kl_socs_plan_s {
   float* stage_in = nullptr; // host-entry staging (lazily allocated)
   float* stage_out = nullptr;
   size_t stage_clips = 0;
+  // host-entry pipeline: copy-in, compute, copy-out streams and their hand-offs
+  cudaStream_t hs[3] = {nullptr, nullptr, nullptr};
+  cudaEvent_t hev[3] = {nullptr, nullptr, nullptr};
   // adjoint state (kl_socs_plan_create_adjoint)
   float2* gpart = nullptr;   // strip partials of the spectrum of dL/dI
   float2* gam = nullptr;     // per-slice Gam partials

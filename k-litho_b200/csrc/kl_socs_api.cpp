@@ -19,6 +19,13 @@ void drop_events(kl_socs_plan p) {
 void free_plan(kl_socs_plan p) {
   if (!p) return;
   drop_events(p);
+  for (int i = 0; i < 3; ++i) {
+    if (p->hs[i]) {
+      cudaStreamSynchronize(p->hs[i]);
+      cudaStreamDestroy(p->hs[i]);
+    }
+    if (p->hev[i]) cudaEventDestroy(p->hev[i]);
+  }
   cudaFree(p->H);
   cudaFree(p->lam);
   cudaFree(p->partial);
@@ -252,12 +259,37 @@ int kl_socs_forward_host(kl_socs_plan p, const float* masks_host, int nclips, fl
       return rc;
     p->stage_clips = (size_t)nclips;
   }
-  KL_CUDA_TRY(cudaMemcpyAsync(p->stage_in, masks_host, sizeof(float) * px * nclips,
-                              cudaMemcpyHostToDevice, st));
-  int rc = run_forward(p, p->stage_in, nclips, p->stage_out, st);
-  if (rc) return rc;
-  KL_CUDA_TRY(cudaMemcpyAsync(images_host, p->stage_out, sizeof(float) * px * nclips * p->nsets,
-                              cudaMemcpyDeviceToHost, st));
+  if (nclips == 0) return KL_OK;
+  // chunks flow through three streams: copy-in, compute (in order, so the
+  // plan's scratch is reused safely), copy-out; the two copy directions and
+  // the kernels of neighbouring chunks overlap
+  if (!p->hs[0]) {
+    for (int i = 0; i < 3; ++i) {
+      KL_CUDA_TRY(cudaStreamCreateWithFlags(&p->hs[i], cudaStreamNonBlocking));
+      KL_CUDA_TRY(cudaEventCreateWithFlags(&p->hev[i], cudaEventDisableTiming));
+    }
+  }
+  cudaStream_t sin = p->hs[0], scomp = p->hs[1], sout = p->hs[2];
+  KL_CUDA_TRY(cudaEventRecord(p->hev[0], st));  // after earlier work on the caller's stream
+  for (int i = 0; i < 3; ++i) KL_CUDA_TRY(cudaStreamWaitEvent(p->hs[i], p->hev[0], 0));
+  const int nchunks = nclips >= 16 ? 4 : (nclips >= 4 ? 2 : 1);
+  const size_t outpx = px * p->nsets;
+  for (int c = 0; c < nchunks; ++c) {
+    const int a = (int)((long long)nclips * c / nchunks), b = (int)((long long)nclips * (c + 1) / nchunks);
+    if (b == a) continue;
+    KL_CUDA_TRY(cudaMemcpyAsync(p->stage_in + px * a, masks_host + px * a, sizeof(float) * px * (b - a),
+                                cudaMemcpyHostToDevice, sin));
+    KL_CUDA_TRY(cudaEventRecord(p->hev[1], sin));
+    KL_CUDA_TRY(cudaStreamWaitEvent(scomp, p->hev[1], 0));
+    int rc = run_forward(p, p->stage_in + px * a, b - a, p->stage_out + outpx * a, scomp);
+    if (rc) return rc;
+    KL_CUDA_TRY(cudaEventRecord(p->hev[2], scomp));
+    KL_CUDA_TRY(cudaStreamWaitEvent(sout, p->hev[2], 0));
+    KL_CUDA_TRY(cudaMemcpyAsync(images_host + outpx * a, p->stage_out + outpx * a, sizeof(float) * outpx * (b - a),
+                                cudaMemcpyDeviceToHost, sout));
+  }
+  KL_CUDA_TRY(cudaEventRecord(p->hev[0], sout));
+  KL_CUDA_TRY(cudaStreamWaitEvent(st, p->hev[0], 0));
   KL_CUDA_TRY(cudaStreamSynchronize(st));
   return KL_OK;
 }

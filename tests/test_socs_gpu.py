@@ -126,6 +126,24 @@ def test_socs_host_entry_matches_device(cuda):
     assert np.array_equal(host, dev)
 
 
+def test_socs_host_entry_pipelined_chunks(cuda):
+    # 18 clips go through the host entry in 4 chunks (copy-in, compute and
+    # copy-out streams overlapping); images equal the device-entry ones up to
+    # the summation order of kernel slices
+    L, Nx = 512, 6
+    sets = [synth.random_kernels(5, Nx, Nx, seed=s) for s in (7, 8)]
+    masks = np.stack([synth.rect_mask(L, 9, seed=100 + s) for s in range(18)])
+    plan = K.SocsPlan(L, L, Nx, Nx, 5, nsets=2, max_clips=18)
+    for i, (k, sc) in enumerate(sets):
+        plan.set_kernels(i, k, sc)
+    host = plan.forward_host(masks)
+    again = plan.forward_host(masks)
+    dev = gpu_images(masks, sets, Nx, Nx)
+    scale = np.abs(dev).max()
+    assert np.abs(host - dev).max() <= 1e-6 * scale
+    assert np.array_equal(host, again)
+
+
 def test_socs_unsupported_geometry_is_an_error(cuda):
     with pytest.raises(K.KLError) as e:
         K.SocsPlan(300, 300, 3, 3, 2)
