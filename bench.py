@@ -49,6 +49,15 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def peaks_tensor():
+    """Dense bf16 TFLOP/s (burst figure: a kernel timed on its own)."""
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["bf16_tflops"])
+    return 1590.0
+
+
 def class_band(L):
     # config-0 optics: annular 0.6/0.9 on 41^2, NA 1.35 (sigma_o = 0.9)
     import klitho as K
@@ -317,6 +326,7 @@ def run_ours(args):
         secondary["fwd_adj"] = bench_fwd_adj(args, stream, peaks()[0])
         secondary["tcc_eigen"] = bench_tcc_eigen(args)
         secondary["tcc_eigen_large"] = bench_tcc_eigen_large(args)
+        secondary["tcc_gemm"] = bench_tcc_gemm(args)
 
     if rank == 0:
         out = {
@@ -595,6 +605,48 @@ def bench_tcc_eigen_large(args):
                       "solve of each path; FP64 at focus 0 only"}
 
 
+def bench_tcc_gemm(args):
+    """The TCC as a materialised matrix (kl_tcc_build: BF16x3 split + tcgen05
+    GEMM, FP32 accumulate in TMEM, Hermitian mirror in the epilogue), CUDA
+    events around the call on its stream, at config 1 (2048^2 dipole, N = 2809,
+    S = 98) and config 4 (4096^2 cross-quadrupole, N = 11449, S = 196).
+    Rooflines: tensor (8 N^2 S flop, the dense complex product counted once)
+    against the measured bf16 peak, and store (N^2 x 8 B of complex64)
+    against the measured HBM copy bandwidth."""
+    import torch
+    import klitho as K
+    import synth
+    out = []
+    for name, L, src in (("2048^2 dipole", 2048, K.createSource(61, "Dipole", radius=0.15, offset=0.7, onXAxis=1)),
+                         ("4096^2 cross-quadrupole", 4096,
+                          K.createSource(81, "CrossQuadrupole", radius=0.12, offset=0.75))):
+        tp = K.TccPlan(src, 1.35, synth.defocus_arg(25.0), L, L, n_medium=synth.N_WATER)
+        N, S = tp.N, tp.S
+        T = torch.empty((N, N, 2), dtype=torch.float32, device="cuda")
+        st = torch.cuda.current_stream()
+        for _ in range(2):
+            K.check(K.lib().kl_tcc_build(tp._h, K._dev_ptr(T), st.cuda_stream), "kl_tcc_build")
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record(st)
+        for _ in range(reps):
+            K.check(K.lib().kl_tcc_build(tp._h, K._dev_ptr(T), st.cuda_stream), "kl_tcc_build")
+        e1.record(st)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / reps / 1e3
+        flop, byts = 8.0 * N * N * S, 8.0 * N * N
+        bf16 = peaks_tensor()
+        out.append({"case": name, "N": N, "S": S, "ms": round(t * 1e3, 4),
+                    "tensor_TFLOPs": round(flop / t / 1e12, 1), "tensor_frac": round(flop / t / 1e12 / bf16, 4),
+                    "store_GBps": round(byts / t / 1e9, 1), "store_frac": round(byts / t / 1e9 / peaks()[0], 4)})
+        del T
+        tp.close()
+    return {"metric": "TCC materialisation (kl_tcc_build) device time", "cases": out,
+            "peaks": {"bf16_TFLOPs": peaks_tensor(), "hbm_GBps": peaks()[0]},
+            "timing": "CUDA events around kl_tcc_build (operand split + tcgen05 GEMM) on its stream, "
+                      "5 calls after 2 warm-up calls; the call synchronises to check the pipeline status"}
+
+
 def run_e2e(plans, masks_h, args, ws, img_equiv):
     import torch
     steps = max(1, min(args.steps, args.e2e_steps))
@@ -710,6 +762,8 @@ def run_part(args):
         r = bench_fwd_adj(args, torch.cuda.current_stream(), peaks()[0])
     elif args.part == "tcc_eigen_large":
         r = bench_tcc_eigen_large(args)
+    elif args.part == "tcc_gemm":
+        r = bench_tcc_gemm(args)
     else:
         r = bench_tcc_eigen(args)
     print(json.dumps(r))
@@ -732,7 +786,7 @@ def main():
     ap.add_argument("--clips", type=int, default=0, help="clip count for --only")
     ap.add_argument("--chunks", type=int, default=1,
                     help="plans per size class (>= 1024^2) in the timed graph")
-    ap.add_argument("--part", choices=["all", "fwd_adj", "tcc_eigen", "tcc_eigen_large"], default="all",
+    ap.add_argument("--part", choices=["all", "fwd_adj", "tcc_eigen", "tcc_eigen_large", "tcc_gemm"], default="all",
                     help="run one secondary measurement alone (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:

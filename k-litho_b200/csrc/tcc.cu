@@ -176,7 +176,7 @@ int tcc_split_operands(const float2* A, int N, int S, int Kp, void* X1, void* X2
 // tcgen05 Hermitian GEMM
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int TM = 128, TN = 128, TK = 64, STAGES = 4;
+constexpr int TM = 128, TN = 128, TK = 64, STAGES = 2;  // 2 CTAs per SM: one's epilogue overlaps the other's MMAs
 constexpr int TILE_BYTES = TM * TK * 2;         // 16 KB, one 128 x 64 bf16 tile
 constexpr int STAGE_BYTES = 3 * TILE_BYTES;     // X1, X2, Y
 constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
@@ -263,7 +263,7 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 }
 }  // namespace
 
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
     k_tcc_gemm(const __grid_constant__ CUtensorMap tmX1, const __grid_constant__ CUtensorMap tmX2,
                const __grid_constant__ CUtensorMap tmY, int N, int nkb, int nt,
                float2* __restrict__ tcc, int* __restrict__ err) {
@@ -363,19 +363,26 @@ __global__ void __launch_bounds__(128, 1)
       tmem_ld32(base + (uint32_t)c0, re);
       tmem_ld32(base + 128u + (uint32_t)c0, im);
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      // direct tile: row i, columns j0 + c0 + c
-      if (i < N) {
-        float2* row = tcc + (size_t)i * N;
+      // direct tile: the warp's 32 x 32 block goes through shared memory (the
+      // pipeline stages are free once `done` has fired) so that each store
+      // writes 32 consecutive columns of one row
+      float2* stage = reinterpret_cast<float2*>(smem) + warp * 32 * 33;
 #pragma unroll
-        for (int c = 0; c < 32; ++c) {
-          const int j = jb * TN + c0 + c;
-          if (j < N && (!diag || c0 + c >= r)) {
-            float2 v = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
-            if (diag && c0 + c == r) v.y = 0.f;
-            row[j] = v;
+      for (int c = 0; c < 32; ++c) stage[lane * 33 + c] = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
+      __syncwarp();
+      {
+        const int j = jb * TN + c0 + lane;
+#pragma unroll 4
+        for (int rr = 0; rr < 32; ++rr) {
+          const int row = warp * 32 + rr, ii = ib * TM + row;
+          if (ii < N && j < N && (!diag || c0 + lane >= row)) {
+            float2 v = stage[rr * 33 + lane];
+            if (diag && c0 + lane == row) v.y = 0.f;
+            tcc[(size_t)ii * N + j] = v;
           }
         }
       }
+      __syncwarp();
       // conjugate transpose: tcc[j][i], consecutive lanes write consecutive i
 #pragma unroll
       for (int c = 0; c < 32; ++c) {
