@@ -7,6 +7,8 @@
 // arithmetic is complex FP64 on the CUDA cores; products of the FP32 factor
 // are formed exactly in FP64.  The B x B problems (Cholesky, triangular
 // inverse, Hermitian eigensolve by cyclic Jacobi) run in one CTA each.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -234,6 +236,7 @@ struct JacobiJob {
   double* w;     // B eigenvalues, descending
   int* jst;      // [0] steps applied, [1 + i] rank of diagonal entry i
   int B;
+  uchar2* ptab = nullptr;  // pair table of one sweep, jacobi_ptab_elems(B) (cluster solver only)
 };
 struct JacobiJobs {
   JacobiJob j[kJacobiMaxJobs];
@@ -443,23 +446,309 @@ __global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiJobs jobs, int 
   if (threadIdx.x == 0) job.jst[0] = nsteps;
 }
 
+// ---------------------------------------------------------------------------
+// Cluster Jacobi for matrices too large for one CTA's shared memory
+// (116 < B <= 256).  The padded order Bp (a multiple of 2 kCl) is cut into
+// 2 kCl groups of g = Bp / (2 kCl) consecutive indices; a round gives each of
+// the kCl CTAs of a thread-block cluster one pair of groups (a perfect
+// matching of the groups by the circle method), and the CTA keeps those 2g
+// rows of H (all B columns) in its shared memory.  Within a round every
+// rotation pairs two rows of one CTA: round 0 runs a circle-method sweep over
+// the CTA's 2g indices (its pairs inside and across its two groups), the
+// other rounds pair index j of the lower group with index (j + k) mod g of the
+// upper one at step k.  The 2 kCl - 1 rounds visit every pair once in Bp - 1
+// steps, the minimum.  A step: each CTA computes its g rotations from its own
+// rows and stores them into every CTA's shared memory, one cluster barrier,
+// then each CTA applies all rotations to its own rows (two-sided 2 x 2
+// updates; row p and q of a pair are local, the columns are all there).
+// Between rounds each CTA keeps one of its groups and pulls the other new one
+// from the CTA that held it (walking the alternating cycles of the two
+// matchings makes such an assignment exist for any two matchings).  The log
+// stores the rotation of canonical pair (edge e, index j) at slot e g + j, so
+// one pair table describes every sweep.
+// ---------------------------------------------------------------------------
+constexpr int kCl = 8;            // CTAs per matrix (portable cluster size)
+constexpr int kClThreads = 512;
+
+__host__ __device__ inline int jacobi_cluster_bp(int B) { return (B + 2 * kCl - 1) / (2 * kCl) * (2 * kCl); }
+
+struct ClusterSmem {
+  int g, npairs;
+  size_t rows, rot, pq, part, diag, total;
+  __host__ __device__ explicit ClusterSmem(int B) {
+    const int Bp = jacobi_cluster_bp(B);
+    g = Bp / (2 * kCl);
+    npairs = Bp / 2;
+    rows = 0;                                                   // 3 slots x g rows x B
+    rot = sizeof(double2) * 3 * (size_t)g * B;                  // 2 x npairs double4
+    pq = rot + sizeof(double4) * 2 * npairs;                    // 2 x npairs uchar2
+    part = (pq + sizeof(uchar2) * 2 * npairs + 15) & ~size_t(15);  // kCl x 2 double
+    diag = part + sizeof(double) * 2 * kCl;                     // Bp double (rank 0)
+    total = diag + sizeof(double) * Bp;
+  }
+};
+
+// logical (p < q) of pair j at step k of round r for the CTA holding groups ga < gb
+__device__ __forceinline__ void cluster_pair(int r, int k, int j, int ga, int gb, int g, int& p, int& q) {
+  if (r == 0) {
+    int lp, lq;
+    jacobi_pair(k, j, 2 * g, lp, lq);
+    p = lp < g ? ga * g + lp : gb * g + lp - g;
+    q = lq < g ? ga * g + lq : gb * g + lq - g;
+  } else {
+    p = ga * g + j;
+    q = gb * g + (j + k) % g;
+  }
+}
+
+__global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
+    k_jacobi_cluster(JacobiJobs jobs, int max_sweeps) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char csm[];
+  const int me = (int)cl.block_rank();
+  const JacobiJob job = jobs.j[blockIdx.x / kCl];
+  const int B = job.B, Bp = jacobi_cluster_bp(B);
+  const ClusterSmem L(B);
+  const int g = L.g, npairs = L.npairs, ngroups = 2 * kCl;
+  const size_t slot_elems = (size_t)g * B;
+  double2* slots = reinterpret_cast<double2*>(csm + L.rows);
+  double4* rotx = reinterpret_cast<double4*>(csm + L.rot);
+  uchar2* pqx = reinterpret_cast<uchar2*>(csm + L.pq);
+  double* part = reinterpret_cast<double*>(csm + L.part);
+  double* diag = reinterpret_cast<double*>(csm + L.diag);
+  // cluster state, the same in every CTA: groups and edge of each CTA, slot of each group
+  __shared__ int s_grp[kCl][2], s_edge[kCl], s_gcta[2 * kCl], s_gslot[2 * kCl], s_free[kCl];
+  __shared__ int s_src, s_srcslot, s_dst;
+  __shared__ double s_red[2][kClThreads / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
+
+  if (tid == 0) {
+    for (int c = 0; c < kCl; ++c) {
+      int a, b;
+      jacobi_pair(0, c, ngroups, a, b);
+      s_grp[c][0] = a;
+      s_grp[c][1] = b;
+      s_edge[c] = c;
+      s_gcta[a] = s_gcta[b] = c;
+      s_gslot[a] = 0;
+      s_gslot[b] = 1;
+      s_free[c] = 2;
+    }
+  }
+  if (me == 0)  // the sweep's pair table, read by the eigenvector replay
+    for (int i = tid; i < (Bp - 1) * npairs; i += nthr) {
+      const int s = i / npairs, t = i - s * npairs, e = t / g, j = t - e * g;
+      const int r = s < 2 * g - 1 ? 0 : 1 + (s - (2 * g - 1)) / g;
+      const int k = r == 0 ? s : (s - (2 * g - 1)) % g;
+      int ga, gb, p, q;
+      jacobi_pair(r, e, ngroups, ga, gb);
+      cluster_pair(r, k, j, ga, gb, g, p, q);
+      job.ptab[i] = make_uchar2((unsigned char)p, (unsigned char)q);
+    }
+  __syncthreads();
+  for (int i = tid; i < 2 * (int)slot_elems; i += nthr) {
+    const int sl = i / (int)slot_elems, rem = i - sl * (int)slot_elems, rr = rem / B, col = rem - rr * B;
+    const int l = s_grp[me][sl] * g + rr;
+    slots[i] = l < B ? job.H[(size_t)l * B + col] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  auto row_of = [&](int l) -> double2* {
+    const int G = l / g;
+    return slots + ((size_t)s_gslot[G] * g + (l - G * g)) * B;
+  };
+
+  int nsteps = 0, sweep = 0, round = 0;
+  while (true) {
+    if (round == 0) {
+      // convergence: off-diagonal vs diagonal mass over the rows of all CTAs
+      double off = 0.0, dg = 0.0;
+      for (int i = tid; i < 2 * (int)slot_elems; i += nthr) {
+        const int sl = i / (int)slot_elems, rem = i - sl * (int)slot_elems, rr = rem / B, col = rem - rr * B;
+        const int G = s_grp[me][sl], l = G * g + rr;
+        if (l >= B) continue;
+        const double2 h = slots[(size_t)s_gslot[G] * slot_elems + (size_t)rr * B + col];
+        if (col == l) dg += h.x * h.x; else off += h.x * h.x + h.y * h.y;
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        off += __shfl_xor_sync(0xffffffffu, off, o);
+        dg += __shfl_xor_sync(0xffffffffu, dg, o);
+      }
+      if (lane == 0) {
+        s_red[0][warp] = off;
+        s_red[1][warp] = dg;
+      }
+      __syncthreads();
+      if (tid < kCl) {
+        double a = 0.0, b = 0.0;
+        for (int w = 0; w < nthr / 32; ++w) {
+          a += s_red[0][w];
+          b += s_red[1][w];
+        }
+        double* dst = cl.map_shared_rank(part, tid);
+        dst[2 * me] = a;
+        dst[2 * me + 1] = b;
+      }
+      cl.sync();
+      double a = 0.0, b = 0.0;
+      for (int c = 0; c < kCl; ++c) {
+        a += part[2 * c];
+        b += part[2 * c + 1];
+      }
+      if (!(a > 1e-28 * b) || b == 0.0 || sweep == max_sweeps) break;  // uniform over the cluster
+    }
+    const int e = s_edge[me], ga = s_grp[me][0], gb = s_grp[me][1];
+    const int nk = round == 0 ? 2 * g - 1 : g;
+    for (int k = 0; k < nk; ++k, ++nsteps) {
+      const int par = nsteps & 1;
+      double4* rb = rotx + par * npairs;
+      uchar2* pb = pqx + par * npairs;
+      // this CTA's g rotations, stored into every CTA (thread i: pair i % g, CTA i / g)
+      for (int i = tid; i < g * kCl; i += nthr) {
+        const int j = i % g, dst = i / g;
+        int p, q;
+        cluster_pair(round, k, j, ga, gb, g, p, q);
+        double4 u = make_double4(1.0, 0.0, 1.0, 0.0);
+        if (q < B) {
+          const double2* rp = row_of(p);
+          double tb;
+          u = jacobi_rotation(rp[p].x, row_of(q)[q].x, rp[q], &tb);
+        }
+        const int t = e * g + j;
+        cl.map_shared_rank(rb, dst)[t] = u;
+        cl.map_shared_rank(pb, dst)[t] = make_uchar2((unsigned char)p, (unsigned char)q);
+        if (dst == me) job.rot[(size_t)nsteps * npairs + t] = u;
+      }
+      cl.sync();
+      // U_j^H H[rows of pair j, columns of pair t2] U_t2 for own pairs j, all t2
+      for (int bi = tid; bi < g * npairs; bi += nthr) {
+        const int j = bi / npairs, t2 = bi - j * npairs, t1 = e * g + j;
+        const uchar2 pr = pb[t1], pc = pb[t2];
+        const int p = pr.x, q = pr.y, p2 = pc.x, q2 = pc.y;
+        if (p >= B || p2 >= B) continue;
+        const bool rq = q < B, cq = q2 < B;
+        double2* rp = row_of(p);
+        double2* rw = rq ? row_of(q) : nullptr;
+        const double2 z = make_double2(0.0, 0.0);
+        double2 x00 = rp[p2], x01 = cq ? rp[q2] : z, x10 = rq ? rw[p2] : z, x11 = (rq && cq) ? rw[q2] : z;
+        rot_block(x00, x01, x10, x11, rb[t1], rb[t2]);
+        if (t2 == t1) {
+          rp[p] = make_double2(x00.x, 0.0);
+          if (rq) {
+            rp[q] = z;
+            rw[p] = z;
+            rw[q] = make_double2(x11.x, 0.0);
+          }
+        } else {
+          rp[p2] = x00;
+          if (cq) rp[q2] = x01;
+          if (rq) {
+            rw[p2] = x10;
+            if (cq) rw[q2] = x11;
+          }
+        }
+      }
+      __syncthreads();
+    }
+    // next round: every CTA keeps one group and pulls the other from its holder
+    const int nr = round + 1 == ngroups - 1 ? 0 : round + 1;
+    if (tid == 0) {
+      int np[2 * kCl], ne[2 * kCl], keep[kCl], recv[kCl], src[kCl], srcslot[kCl], dstslot[kCl], nfree[kCl];
+      bool seen[kCl];
+      for (int x = 0; x < kCl; ++x) {
+        int a, b;
+        jacobi_pair(nr, x, ngroups, a, b);
+        np[a] = b;
+        np[b] = a;
+        ne[a] = ne[b] = x;
+        seen[x] = false;
+      }
+      for (int c0 = 0; c0 < kCl; ++c0) {
+        if (seen[c0]) continue;
+        int c = c0, kp = s_grp[c0][0];
+        for (int guard = 0; guard < kCl; ++guard) {  // an alternating cycle has at most kCl CTAs
+          const int rv = np[kp];
+          keep[c] = kp;
+          recv[c] = rv;
+          seen[c] = true;
+          const int c2 = s_gcta[rv];
+          if (seen[c2]) break;
+          kp = s_grp[c2][0] == rv ? s_grp[c2][1] : s_grp[c2][0];
+          c = c2;
+        }
+      }
+      for (int c = 0; c < kCl; ++c) {
+        src[c] = s_gcta[recv[c]];
+        srcslot[c] = s_gslot[recv[c]];
+        if (src[c] == c) {
+          dstslot[c] = srcslot[c];
+          nfree[c] = s_free[c];
+        } else {
+          const int sent = s_grp[c][0] == keep[c] ? s_grp[c][1] : s_grp[c][0];
+          dstslot[c] = s_free[c];
+          nfree[c] = s_gslot[sent];
+        }
+      }
+      for (int c = 0; c < kCl; ++c) {
+        s_gcta[recv[c]] = c;
+        s_gslot[recv[c]] = dstslot[c];
+        s_free[c] = nfree[c];
+        s_grp[c][0] = min(keep[c], recv[c]);
+        s_grp[c][1] = max(keep[c], recv[c]);
+        s_edge[c] = ne[keep[c]];
+      }
+      s_src = src[me];
+      s_srcslot = srcslot[me];
+      s_dst = dstslot[me];
+    }
+    cl.sync();  // every CTA's updates of the finished round are visible
+    if (s_src != me) {
+      const double2* from = cl.map_shared_rank(slots, s_src) + (size_t)s_srcslot * slot_elems;
+      double2* to = slots + (size_t)s_dst * slot_elems;
+      for (size_t i = tid; i < slot_elems; i += nthr) to[i] = from[i];
+    }
+    __syncthreads();
+    round = nr;
+    if (round == 0) ++sweep;
+  }
+  // eigenvalues: every CTA sends its diagonal to rank 0, which ranks them
+  for (int i = tid; i < 2 * g; i += nthr) {
+    const int l = s_grp[me][i / g] * g + (i % g);
+    if (l < B) cl.map_shared_rank(diag, 0)[l] = row_of(l)[l].x;
+  }
+  cl.sync();
+  if (me == 0) {
+    for (int i = tid; i < B; i += nthr) {
+      const double vi = diag[i];
+      int r = 0;
+      for (int j = 0; j < B; ++j) {
+        const double vj = diag[j];
+        r += (vj > vi) || (vj == vi && j < i);
+      }
+      job.w[r] = vi;
+      job.jst[1 + i] = r;
+    }
+    if (tid == 0) job.jst[0] = nsteps;
+  }
+}
+
 // Q[k][rank[p]] = (prod of the logged rotations)[k][p]: row k of Q evolves
 // independently (entries p, q of the row mix under pair (p, q)), so each warp
 // replays the log on one row held in shared memory, two pairs per lane.
 constexpr int kVecWarps = 8;
 constexpr int kVecChunkMax = 32;  // logged steps staged per pass (fewer for large B)
 
-int jacobi_vectors_chunk(int B) {
-  const int Bp = B + (B & 1), npairs = Bp / 2;
+int jacobi_vectors_chunk(int B, int Bp) {
+  const int npairs = Bp / 2;
   const size_t fixed = sizeof(double2) * kVecWarps * B + sizeof(uchar2) * (Bp - 1) * npairs + 16;
   const size_t budget = 200 * 1024;
   const int c = (int)((budget - std::min(budget, fixed)) / (sizeof(double4) * npairs));
   return std::max(1, std::min(kVecChunkMax, c));
 }
 
-size_t jacobi_vectors_smem(int B) {
-  const int Bp = B + (B & 1), npairs = Bp / 2;
-  return sizeof(double4) * jacobi_vectors_chunk(B) * npairs + sizeof(double2) * kVecWarps * B +
+size_t jacobi_vectors_smem(int B, int Bp) {
+  const int npairs = Bp / 2;
+  return sizeof(double4) * jacobi_vectors_chunk(B, Bp) * npairs + sizeof(double2) * kVecWarps * B +
          ((sizeof(uchar2) * (Bp - 1) * npairs + 15) & ~size_t(15));
 }
 
@@ -479,7 +768,7 @@ __global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jo
   const double4* __restrict__ rot = job.rot;
   const int* __restrict__ jst = job.jst;
   double2* __restrict__ Q = job.Q;
-  const int Bp = B + (B & 1), npairs = Bp / 2;
+  const int Bp = job.ptab ? jacobi_cluster_bp(B) : B + (B & 1), npairs = Bp / 2;
   double4* lg = reinterpret_cast<double4*>(vsm);                   // chunk x npairs
   double2* rows = reinterpret_cast<double2*>(lg + chunk * npairs);  // kVecWarps x B
   uchar2* ptab = reinterpret_cast<uchar2*>(rows + kVecWarps * B);   // (Bp - 1) x npairs
@@ -487,7 +776,10 @@ __global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jo
   const int k = blockIdx.x * kVecWarps + warp;
   double2* row = rows + warp * B;
   for (int p = lane; p < B; p += 32) row[p] = make_double2(p == k ? 1.0 : 0.0, 0.0);
-  jacobi_pair_table(ptab, Bp);
+  if (job.ptab)
+    for (int i = threadIdx.x; i < (Bp - 1) * npairs; i += blockDim.x) ptab[i] = job.ptab[i];
+  else
+    jacobi_pair_table(ptab, Bp);
   const int nsteps = jst[0];
   int step = 0;
   for (int s0 = 0; s0 < nsteps; s0 += chunk) {
@@ -530,6 +822,7 @@ __global__ void k_to_kernels(const double2* __restrict__ U, int N, int ldu, int 
 struct Workspace {
   double2 *X = nullptr, *W = nullptr, *Z = nullptr, *G = nullptr, *Rinv = nullptr, *Q = nullptr;
   double4* rot = nullptr;
+  uchar2* ptab = nullptr;
   double* w = nullptr;
   int *status = nullptr, *jst = nullptr;
   cudaStream_t st = nullptr;
@@ -551,9 +844,38 @@ struct Workspace {
 // k_jacobi keeps H in shared memory up to this size, else works in place
 constexpr size_t kJacobiSmemCap = 220 * 1024;
 bool jacobi_h_in_smem(int B) { return JacobiSmem(B).total_no_h + sizeof(double2) * (size_t)B * B <= kJacobiSmemCap; }
+
+// larger matrices (up to kGramMaxS) go to the cluster solver when the device
+// can co-schedule a cluster of kCl CTAs of its size; otherwise k_jacobi works
+// on H in place in global memory
+bool jacobi_use_cluster(int B) {
+  if (jacobi_h_in_smem(B) || B > kGramMaxS) return false;
+  static int ok = -1;
+  if (ok < 0) {
+    ok = 0;
+    const size_t sm = ClusterSmem(kGramMaxS).total;
+    if (cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) ==
+        cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(kCl);
+      cfg.blockDim = dim3(kClThreads);
+      cfg.dynamicSmemBytes = sm;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, k_jacobi_cluster, &cfg) == cudaSuccess && n > 0) ok = 1;
+    }
+    (void)cudaGetLastError();
+  }
+  return ok == 1;
+}
+// padded order of the sweep (pairs per step = order / 2, steps per sweep = order - 1)
+int jacobi_order(int B) { return jacobi_use_cluster(B) ? jacobi_cluster_bp(B) : B + (B & 1); }
 size_t jacobi_log_elems(int B) {
-  const int Bp = B + (B & 1);
+  const int Bp = jacobi_order(B);
   return (size_t)kJacobiMaxSweeps * (Bp - 1) * (Bp / 2) + 1;
+}
+size_t jacobi_ptab_elems(int B) {
+  const int Bp = jacobi_order(B);
+  return jacobi_use_cluster(B) ? (size_t)(Bp - 1) * (Bp / 2) : 1;
 }
 
 // X (N x B) <- orth(X) by CholeskyQR2; the first pass shifted for safety
@@ -571,36 +893,53 @@ int cholqr2(double2* X, int N, int B, Workspace& ws, cudaStream_t st) {
   return KL_OK;
 }
 
-// Eigen-decompositions of a batch of Hermitian matrices, one CTA each (see
-// JacobiJob); H is overwritten when it does not fit in shared memory.
+// Eigen-decompositions of a batch of Hermitian matrices (see JacobiJob): one
+// CTA each, or one cluster each for the sizes jacobi_use_cluster picks; H is
+// overwritten when one CTA works on it in global memory.
 int jacobi_batch(const std::vector<JacobiJob>& all, cudaStream_t st) {
-  for (size_t j0 = 0; j0 < all.size(); j0 += kJacobiMaxJobs) {
-    const int nj = (int)std::min(all.size() - j0, (size_t)kJacobiMaxJobs);
-    JacobiJobs jobs{};
-    int bmax = 1;
-    for (int j = 0; j < nj; ++j) {
-      jobs.j[j] = all[j0 + j];
-      bmax = std::max(bmax, jobs.j[j].B);
+  std::vector<JacobiJob> by_path[2];
+  for (const JacobiJob& j : all) by_path[jacobi_use_cluster(j.B) ? 1 : 0].push_back(j);
+  for (int cluster = 0; cluster < 2; ++cluster) {
+    const std::vector<JacobiJob>& v = by_path[cluster];
+    for (size_t j0 = 0; j0 < v.size(); j0 += kJacobiMaxJobs) {
+      const int nj = (int)std::min(v.size() - j0, (size_t)kJacobiMaxJobs);
+      JacobiJobs jobs{};
+      int bmax = 1, bpmax = 2;
+      for (int j = 0; j < nj; ++j) {
+        jobs.j[j] = v[j0 + j];
+        if (!cluster) jobs.j[j].ptab = nullptr;
+        KL_CHECK_ARG(!cluster || jobs.j[j].ptab, "jacobi: the cluster solver needs a pair table");
+        bmax = std::max(bmax, jobs.j[j].B);
+        bpmax = std::max(bpmax, jacobi_order(jobs.j[j].B));
+      }
+      if (cluster) {
+        const size_t sm = ClusterSmem(bmax).total;
+        KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_jacobi_cluster<<<nj * kCl, kClThreads, sm, st>>>(jobs, kJacobiMaxSweeps);
+      } else {
+        const bool in_smem = jacobi_h_in_smem(bmax);
+        const size_t sm = JacobiSmem(bmax).total_no_h + (in_smem ? sizeof(double2) * (size_t)bmax * bmax : 0);
+        if (sm > 48 * 1024)
+          KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_jacobi<<<nj, kJacobiThreads, sm, st>>>(jobs, in_smem ? 1 : 0, kJacobiMaxSweeps);
+      }
+      KL_CUDA_TRY(cudaGetLastError());
+      const size_t vsm = jacobi_vectors_smem(bmax, bpmax);
+      if (vsm > 48 * 1024)
+        KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
+      k_jacobi_vectors<<<dim3((bmax + kVecWarps - 1) / kVecWarps, nj), 32 * kVecWarps, vsm, st>>>(
+          jobs, jacobi_vectors_chunk(bmax, bpmax));
+      KL_CUDA_TRY(cudaGetLastError());
     }
-    const bool in_smem = jacobi_h_in_smem(bmax);
-    const size_t sm = JacobiSmem(bmax).total_no_h + (in_smem ? sizeof(double2) * (size_t)bmax * bmax : 0);
-    if (sm > 48 * 1024)
-      KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_jacobi<<<nj, kJacobiThreads, sm, st>>>(jobs, in_smem ? 1 : 0, kJacobiMaxSweeps);
-    KL_CUDA_TRY(cudaGetLastError());
-    const size_t vsm = jacobi_vectors_smem(bmax);
-    if (vsm > 48 * 1024)
-      KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_vectors, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
-    k_jacobi_vectors<<<dim3((bmax + kVecWarps - 1) / kVecWarps, nj), 32 * kVecWarps, vsm, st>>>(
-        jobs, jacobi_vectors_chunk(bmax));
-    KL_CUDA_TRY(cudaGetLastError());
   }
   return KL_OK;
 }
 
 // Q (B x B, column j = eigenvector j) and w (descending) of the Hermitian H
-int jacobi(double2* H, int B, double4* rot, int* jst, double2* Q, double* w, cudaStream_t st) {
-  return jacobi_batch({JacobiJob{H, rot, Q, w, jst, B}}, st);
+int jacobi(double2* H, int B, double4* rot, uchar2* ptab, int* jst, double2* Q, double* w, cudaStream_t st) {
+  JacobiJob j{H, rot, Q, w, jst, B};
+  j.ptab = ptab;
+  return jacobi_batch({j}, st);
 }
 
 // Generic driver.  apply(X, W): W = TCC X (N x B); project(X, H): H = X^H TCC X (B x B).
@@ -614,6 +953,7 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   if ((arc = ws.get(&ws.X, (size_t)N * B)) || (arc = ws.get(&ws.W, (size_t)N * B)) ||
       (arc = ws.get(&ws.G, (size_t)B * B)) || (arc = ws.get(&ws.Rinv, (size_t)B * B)) ||
       (arc = ws.get(&ws.Q, (size_t)B * B)) || (arc = ws.get(&ws.rot, jacobi_log_elems(B))) ||
+      (arc = ws.get(&ws.ptab, jacobi_ptab_elems(B))) ||
       (arc = ws.get(&ws.jst, (size_t)B + 1)) || (arc = ws.get(&ws.w, (size_t)B)) ||
       (arc = ws.get(&ws.status, 1)))
     return arc;
@@ -637,7 +977,7 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   for (it = 1; it <= opt.max_iter; ++it) {
     if (it % check_every == 0) {
       if ((rc = project(ws.X, ws.G))) return rc;
-      if ((rc = jacobi(ws.G, B, ws.rot, ws.jst, ws.Q, ws.w, st))) return rc;
+      if ((rc = jacobi(ws.G, B, ws.rot, ws.ptab, ws.jst, ws.Q, ws.w, st))) return rc;
       KL_CUDA_TRY(cudaMemcpyAsync(cur.data(), ws.w, sizeof(double) * B, cudaMemcpyDeviceToHost, st));
       KL_CUDA_TRY(cudaStreamSynchronize(st));
       change = 0.0;
@@ -662,7 +1002,7 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   // final Rayleigh-Ritz on the current block (G holds the eigvecs in Q)
   if (!converged) {
     if ((rc = project(ws.X, ws.G))) return rc;
-    if ((rc = jacobi(ws.G, B, ws.rot, ws.jst, ws.Q, ws.w, st))) return rc;
+    if ((rc = jacobi(ws.G, B, ws.rot, ws.ptab, ws.jst, ws.Q, ws.w, st))) return rc;
   }
   // U = X Q[:, :K] (N x K, row-major), eigenvalues
   if ((rc = zgemm<G_NN>(ws.X, B, ws.Q, B, ws.W, B, N, B, B, st))) return rc;
@@ -723,12 +1063,14 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
     w.st = st;
     int arc;
     if ((arc = w.get(&w.G, (size_t)S * S)) || (arc = w.get(&w.Q, (size_t)S * S)) ||
-        (arc = w.get(&w.rot, jacobi_log_elems(S))) || (arc = w.get(&w.jst, (size_t)S + 1)) ||
+        (arc = w.get(&w.rot, jacobi_log_elems(S))) || (arc = w.get(&w.ptab, jacobi_ptab_elems(S))) ||
+        (arc = w.get(&w.jst, (size_t)S + 1)) ||
         (arc = w.get(&w.W, (size_t)S * K)) || (arc = w.get(&w.w, (size_t)S)))
       return arc;
     int rc = zgemm<G_AHA>(pr[i].A, S, pr[i].A, S, w.G, S, S, S, pr[i].N, st);
     if (rc) return rc;
     jobs[i] = JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S};
+    jobs[i].ptab = w.ptab;
   }
   int rc = jacobi_batch(jobs, st);
   if (rc) return rc;
@@ -744,7 +1086,7 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
   KL_CUDA_TRY(cudaStreamSynchronize(st));
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S;
-    const int sweeps = nsteps[i] / (S + (S & 1) - 1);
+    const int sweeps = nsteps[i] / (jacobi_order(S) - 1);
     if (sweeps >= kJacobiMaxSweeps) {
       set_error("eig_topk_factor: Jacobi eigensolve of the Gram matrix did not converge in " +
                 std::to_string(kJacobiMaxSweeps) + " sweeps");

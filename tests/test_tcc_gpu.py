@@ -31,7 +31,7 @@ CASES = {
                    synth.defocus_arg(-50.0), 32),
     "dry_na08": (512, "Annular", 41, dict(innerRadius=0.5, outerRadius=0.8), 0.8, 1.0, 0.2, 12),
     "quad512": (512, "CrossQuadrupole", 41, dict(radius=0.12, offset=0.75), 1.35, 1.44, 0.0, 16),
-    # 196 source points: the one-step Gram solve with the Jacobi matrix in global memory
+    # 196 source points: the one-step Gram solve on a thread-block cluster
     "quad81_512": (512, "CrossQuadrupole", 81, dict(radius=0.12, offset=0.75), 1.35, 1.44,
                    synth.defocus_arg(30.0), 32),
 }
@@ -160,6 +160,60 @@ def test_topk_batch_focus_sweep(cuda):
         Pr = weighted_projector(kr, er)
         assert np.linalg.norm(weighted_projector(kb[i], eb[i]) - Pr) / np.linalg.norm(Pr) <= 1e-5
         assert 0 < itb[i] < 40  # Jacobi sweeps of the one Gram solve
+
+
+def eig_residual(krn, ev, tcc):
+    """max_k ||T v_k - lam_k v_k|| / lam_0 over the returned kernels."""
+    V = np.asarray(krn, dtype=np.complex128)[:, ::-1].T  # N x K
+    R = tcc @ V - V * np.asarray(ev, dtype=np.float64)[None, :]
+    return np.linalg.norm(R, axis=0).max() / abs(ev[0])
+
+
+def gap_cut(w, hi, rel=1e-3):
+    """largest n <= hi with lam_{n-1} - lam_n > rel lam_0 (a unique top-n projector)."""
+    return max(n for n in range(1, hi + 1) if w[n - 1] - w[n] > rel * w[0])
+
+
+def test_topk_batch_cluster_jacobi(cuda):
+    # 196 source points: each focus value's 196 x 196 Gram eigensolve runs on
+    # one thread-block cluster, three clusters in one launch
+    L, nk = 512, 48
+    src = K.createSource(71, "CrossQuadrupole", radius=0.12, offset=0.75)
+    assert int((np.asarray(src) > 0).sum()) == 196
+    focus = [-40.0, 10.0, 60.0]
+    sig = O.outer_sigma(src)
+    Nx, Ny = O.band(1.35, L, L, sig)
+    plans = [K.TccPlan(src, 1.35, synth.defocus_arg(f), L, L, n_medium=1.44) for f in focus]
+    kb, sb, eb, itb = K.TccPlan.topk_batch(plans, nk)
+    for i, f in enumerate(focus):
+        tcc = O.calc_tcc(src, sig, 1.35, synth.defocus_arg(f), L, L, Nx, Ny, n_medium=1.44)
+        kr, _, er = O.calc_kernels(tcc, nk)
+        assert np.abs(eb[i] - er).max() <= 1e-6 * np.abs(er).max()
+        # eigenpairs of the TCC whatever the degenerate pairs (BF16x3 TCC: ~3e-5)
+        assert eig_residual(kb[i], eb[i], tcc) <= 1e-4
+        n = gap_cut(np.linalg.eigvalsh(tcc)[::-1], nk)
+        Pr = weighted_projector(kr[:n], er[:n])
+        assert np.linalg.norm(weighted_projector(kb[i][:n], eb[i][:n]) - Pr) / np.linalg.norm(Pr) <= 1e-5
+        assert np.allclose(np.linalg.norm(kb[i].astype(np.complex128), axis=1), 1.0, atol=1e-6)
+        assert 0 < itb[i] < 40
+
+
+def test_topk_subspace_cluster_block(cuda):
+    # 572 source points (subspace iteration) with an 80-kernel request: the
+    # 120-wide Rayleigh-Ritz blocks are solved by the cluster Jacobi
+    L, nk = 1024, 80
+    src = K.createSource(41, "Annular", 0.6, 0.9)
+    plan = K.TccPlan(src, 1.35, synth.defocus_arg(20.0), L, L, n_medium=1.44)
+    krn, sc, ev, it = plan.topk(nk)
+    sig = O.outer_sigma(src)
+    Nx, Ny = O.band(1.35, L, L, sig)
+    tcc = O.calc_tcc(src, sig, 1.35, synth.defocus_arg(20.0), L, L, Nx, Ny, n_medium=1.44)
+    kr, _, er = O.calc_kernels(tcc, nk)
+    assert np.abs(ev - er).max() <= 1e-6 * np.abs(er).max(), it
+    assert eig_residual(krn, ev, tcc) <= 1e-4
+    n = gap_cut(np.linalg.eigvalsh(tcc)[::-1], nk)
+    Pr = weighted_projector(kr[:n], er[:n])
+    assert np.linalg.norm(weighted_projector(krn[:n], ev[:n]) - Pr) / np.linalg.norm(Pr) <= 1e-5
 
 
 @pytest.mark.parametrize("precision", [K.PREC_FAST, K.PREC_FP64])
