@@ -8,6 +8,7 @@
 // are formed exactly in FP64.  The B x B problems (Cholesky, triangular
 // inverse, Hermitian eigensolve by cyclic Jacobi) run in one CTA each.
 #include <cooperative_groups.h>
+#include <cuda_pipeline.h>
 
 #include <algorithm>
 #include <cmath>
@@ -231,18 +232,17 @@ constexpr int kGramMaxS = 256;  // factor widths solved by one Gram eigensolve (
 
 struct JacobiJob {
   double2* H;    // B x B Hermitian input (overwritten when worked in place)
-  double4* rot;  // rotation log, jacobi_log_elems(B)
+  double4* rot;  // rotation log (cluster solver: block log), jacobi_log_elems(B)
   double2* Q;    // B x B output, column j = eigenvector j
   double* w;     // B eigenvalues, descending
   int* jst;      // [0] steps applied, [1 + i] rank of diagonal entry i
   int B;
-  uchar2* ptab = nullptr;  // pair table of one sweep, jacobi_ptab_elems(B) (cluster solver only)
 };
 struct JacobiJobs {
   JacobiJob j[kJacobiMaxJobs];
 };
 
-__device__ __forceinline__ void jacobi_pair(int t, int i, int Bp, int& p, int& q) {
+__host__ __device__ inline void jacobi_pair(int t, int i, int Bp, int& p, int& q) {
   const int m = Bp - 1;
   if (i == 0) {
     p = 0;
@@ -463,42 +463,59 @@ __global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiJobs jobs, int 
 // updates; row p and q of a pair are local, the columns are all there).
 // Between rounds each CTA keeps one of its groups and pulls the other new one
 // from the CTA that held it (walking the alternating cycles of the two
-// matchings makes such an assignment exist for any two matchings).  The log
-// stores the rotation of canonical pair (edge e, index j) at slot e g + j, so
-// one pair table describes every sweep.
+// matchings makes such an assignment exist for any two matchings).
+// The rotations of a round only mix the 2g indices of each CTA, so their
+// product is block diagonal: each CTA accumulates its 2g x 2g block W (the
+// rotations applied to W's columns) and logs it at the end of the round;
+// k_jacobi_vectors_blocks forms the eigenvectors from these blocks.
 // ---------------------------------------------------------------------------
 constexpr int kCl = 8;            // CTAs per matrix (portable cluster size)
 constexpr int kClThreads = 512;
+constexpr int kClMaxG = kGramMaxS / (2 * kCl);  // largest group
 
 __host__ __device__ inline int jacobi_cluster_bp(int B) { return (B + 2 * kCl - 1) / (2 * kCl) * (2 * kCl); }
 
 struct ClusterSmem {
   int g, npairs;
-  size_t rows, rot, pq, part, diag, total;
+  size_t rows, rot, pq, w, r0, part, diag, total;
   __host__ __device__ explicit ClusterSmem(int B) {
     const int Bp = jacobi_cluster_bp(B);
     g = Bp / (2 * kCl);
     npairs = Bp / 2;
-    rows = 0;                                                   // 3 slots x g rows x B
-    rot = sizeof(double2) * 3 * (size_t)g * B;                  // 2 x npairs double4
-    pq = rot + sizeof(double4) * 2 * npairs;                    // 2 x npairs uchar2
-    part = (pq + sizeof(uchar2) * 2 * npairs + 15) & ~size_t(15);  // kCl x 2 double
-    diag = part + sizeof(double) * 2 * kCl;                     // Bp double (rank 0)
+    rows = 0;                                                      // 3 slots x g rows x B
+    rot = sizeof(double2) * 3 * (size_t)g * B;                     // 2 x npairs double4
+    pq = rot + sizeof(double4) * 2 * npairs;                       // 2 x npairs uchar2
+    w = (pq + sizeof(uchar2) * 2 * npairs + 15) & ~size_t(15);     // 2g x 2g double2
+    r0 = w + sizeof(double2) * 4 * (size_t)g * g;                  // (2g - 1) x g uchar2
+    part = (r0 + sizeof(uchar2) * (2 * g - 1) * g + 15) & ~size_t(15);  // kCl x 2 double
+    diag = part + sizeof(double) * 2 * kCl;                        // Bp double (rank 0)
     total = diag + sizeof(double) * Bp;
   }
 };
 
-// logical (p < q) of pair j at step k of round r for the CTA holding groups ga < gb
-__device__ __forceinline__ void cluster_pair(int r, int k, int j, int ga, int gb, int g, int& p, int& q) {
-  if (r == 0) {
-    int lp, lq;
-    jacobi_pair(k, j, 2 * g, lp, lq);
-    p = lp < g ? ga * g + lp : gb * g + lp - g;
-    q = lq < g ? ga * g + lq : gb * g + lq - g;
-  } else {
-    p = ga * g + j;
-    q = gb * g + (j + k) % g;
-  }
+// Round transitions of the cluster, the same for every matrix size: entry
+// [t * kCl + c] describes CTA c after the t-th round of the run (bits: lower
+// group 0-3, upper group 4-7, matching edge 8-10, slot of the lower group
+// 11-12, of the upper 13-14, CTA to pull the new group from 15-17, its slot
+// there 18-19, slot it lands in 20-21, pull needed 22); filled by the host.
+__constant__ uint32_t c_cluster_sched[kJacobiMaxSweeps * (2 * kCl - 1) * kCl];
+
+// double2 elements of the block log: one 2g x 2g block per CTA and round
+__host__ __device__ inline size_t cluster_log_elems(int B, int max_sweeps) {
+  const int g2 = jacobi_cluster_bp(B) / kCl;
+  return (size_t)max_sweeps * (2 * kCl - 1) * kCl * g2 * g2;
+}
+
+// local position l < 2g of the CTA holding groups ga < gb -> logical index
+__device__ __forceinline__ int cluster_index(int l, int ga, int gb, int g) {
+  return l < g ? ga * g + l : gb * g + l - g;
+}
+
+// row[p], row[q] <- the pair's columns of row . U (U as in rot_block's right factor)
+__device__ __forceinline__ void rot_cols(double2& vp, double2& vq, double4 u) {
+  const double2 e = zmul(vq, make_double2(u.z, -u.w)), a = vp;
+  vp = make_double2(u.x * a.x - u.y * e.x, u.x * a.y - u.y * e.y);
+  vq = make_double2(u.y * a.x + u.x * e.x, u.y * a.y + u.x * e.y);
 }
 
 __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
@@ -508,67 +525,56 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
   extern __shared__ __align__(16) unsigned char csm[];
   const int me = (int)cl.block_rank();
   const JacobiJob job = jobs.j[blockIdx.x / kCl];
-  const int B = job.B, Bp = jacobi_cluster_bp(B);
+  const int B = job.B;
   const ClusterSmem L(B);
-  const int g = L.g, npairs = L.npairs, ngroups = 2 * kCl;
-  const size_t slot_elems = (size_t)g * B;
+  const int g = L.g, g2 = 2 * g, npairs = L.npairs, ngroups = 2 * kCl;
+  const int slot_elems = g * B;
   double2* slots = reinterpret_cast<double2*>(csm + L.rows);
   double4* rotx = reinterpret_cast<double4*>(csm + L.rot);
   uchar2* pqx = reinterpret_cast<uchar2*>(csm + L.pq);
+  double2* W = reinterpret_cast<double2*>(csm + L.w);
+  uchar2* r0 = reinterpret_cast<uchar2*>(csm + L.r0);
   double* part = reinterpret_cast<double*>(csm + L.part);
   double* diag = reinterpret_cast<double*>(csm + L.diag);
-  // cluster state, the same in every CTA: groups and edge of each CTA, slot of each group
-  __shared__ int s_grp[kCl][2], s_edge[kCl], s_gcta[2 * kCl], s_gslot[2 * kCl], s_free[kCl];
-  __shared__ int s_src, s_srcslot, s_dst;
+  double2* wlog = reinterpret_cast<double2*>(job.rot);
+  __shared__ int s_rowoff[2 * kClMaxG];  // element offset of local position l's row, -1: padding
+  __shared__ int4 s_own[kClMaxG];        // own pair j of the step: row offsets of p, q (-1: padding), lp, lq
   __shared__ double s_red[2][kClThreads / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
+  const double2 zero = make_double2(0.0, 0.0), one = make_double2(1.0, 0.0);
+  // this CTA's groups (ga < gb), their slots and its matching edge; round 0 starts with edge me
+  int ga, gb, sa = 0, sb = 1, e = me;
+  jacobi_pair(0, me, ngroups, ga, gb);
 
-  if (tid == 0) {
-    for (int c = 0; c < kCl; ++c) {
-      int a, b;
-      jacobi_pair(0, c, ngroups, a, b);
-      s_grp[c][0] = a;
-      s_grp[c][1] = b;
-      s_edge[c] = c;
-      s_gcta[a] = s_gcta[b] = c;
-      s_gslot[a] = 0;
-      s_gslot[b] = 1;
-      s_free[c] = 2;
-    }
+  for (int i = tid; i < (g2 - 1) * g; i += nthr) {
+    int lp, lq;
+    jacobi_pair(i / g, i % g, g2, lp, lq);
+    r0[i] = make_uchar2((unsigned char)lp, (unsigned char)lq);
   }
-  if (me == 0)  // the sweep's pair table, read by the eigenvector replay
-    for (int i = tid; i < (Bp - 1) * npairs; i += nthr) {
-      const int s = i / npairs, t = i - s * npairs, e = t / g, j = t - e * g;
-      const int r = s < 2 * g - 1 ? 0 : 1 + (s - (2 * g - 1)) / g;
-      const int k = r == 0 ? s : (s - (2 * g - 1)) % g;
-      int ga, gb, p, q;
-      jacobi_pair(r, e, ngroups, ga, gb);
-      cluster_pair(r, k, j, ga, gb, g, p, q);
-      job.ptab[i] = make_uchar2((unsigned char)p, (unsigned char)q);
-    }
-  __syncthreads();
-  for (int i = tid; i < 2 * (int)slot_elems; i += nthr) {
-    const int sl = i / (int)slot_elems, rem = i - sl * (int)slot_elems, rr = rem / B, col = rem - rr * B;
-    const int l = s_grp[me][sl] * g + rr;
-    slots[i] = l < B ? job.H[(size_t)l * B + col] : make_double2(0.0, 0.0);
+  for (int i = tid; i < g2 * g2; i += nthr) W[i] = (i / g2 == i % g2) ? one : zero;
+  for (int i = tid; i < 2 * slot_elems; i += nthr) {
+    const int sl = i / slot_elems, rem = i - sl * slot_elems, rr = rem / B, col = rem - rr * B;
+    const int l = (sl ? gb : ga) * g + rr;
+    slots[i] = l < B ? job.H[(size_t)l * B + col] : zero;
+  }
+  if (tid < g2) {
+    const int l = tid % g, gl = (tid < g ? ga : gb) * g + l;
+    s_rowoff[tid] = gl < B ? ((tid < g ? sa : sb) * g + l) * B : -1;
   }
   __syncthreads();
-  auto row_of = [&](int l) -> double2* {
-    const int G = l / g;
-    return slots + ((size_t)s_gslot[G] * g + (l - G * g)) * B;
-  };
+  // the H update: thread (jg, t2) applies column pair t2 to own row pairs jg, jg + ngrp, ...
+  const int ngrp = nthr / npairs, t2 = tid % npairs, jg = tid / npairs;
 
-  int nsteps = 0, sweep = 0, round = 0;
+  int nsteps = 0, sweep = 0, round = 0, nrounds = 0;
   while (true) {
     if (round == 0) {
       // convergence: off-diagonal vs diagonal mass over the rows of all CTAs
       double off = 0.0, dg = 0.0;
-      for (int i = tid; i < 2 * (int)slot_elems; i += nthr) {
-        const int sl = i / (int)slot_elems, rem = i - sl * (int)slot_elems, rr = rem / B, col = rem - rr * B;
-        const int G = s_grp[me][sl], l = G * g + rr;
-        if (l >= B) continue;
-        const double2 h = slots[(size_t)s_gslot[G] * slot_elems + (size_t)rr * B + col];
-        if (col == l) dg += h.x * h.x; else off += h.x * h.x + h.y * h.y;
+      for (int i = tid; i < g2 * B; i += nthr) {
+        const int l = i / B, col = i - l * B, o = s_rowoff[l];
+        if (o < 0) continue;
+        const double2 h = slots[o + col];
+        if (col == cluster_index(l, ga, gb, g)) dg += h.x * h.x; else off += h.x * h.x + h.y * h.y;
       }
       for (int o = 16; o > 0; o >>= 1) {
         off += __shfl_xor_sync(0xffffffffu, off, o);
@@ -597,124 +603,128 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
       }
       if (!(a > 1e-28 * b) || b == 0.0 || sweep == max_sweeps) break;  // uniform over the cluster
     }
-    const int e = s_edge[me], ga = s_grp[me][0], gb = s_grp[me][1];
-    const int nk = round == 0 ? 2 * g - 1 : g;
+    const int nk = round == 0 ? g2 - 1 : g;
     for (int k = 0; k < nk; ++k, ++nsteps) {
       const int par = nsteps & 1;
       double4* rb = rotx + par * npairs;
       uchar2* pb = pqx + par * npairs;
       // this CTA's g rotations, stored into every CTA (thread i: pair i % g, CTA i / g)
       for (int i = tid; i < g * kCl; i += nthr) {
-        const int j = i % g, dst = i / g;
-        int p, q;
-        cluster_pair(round, k, j, ga, gb, g, p, q);
+        const int dst = i / g, j = i - dst * g;
+        int lp, lq;
+        if (round == 0) {
+          const uchar2 v = r0[k * g + j];
+          lp = v.x;
+          lq = v.y;
+        } else {
+          lp = j;
+          lq = j + k < g ? g + j + k : j + k;  // g + (j + k) mod g
+        }
+        const int p = cluster_index(lp, ga, gb, g), q = cluster_index(lq, ga, gb, g);
+        const int op = s_rowoff[lp], oq = s_rowoff[lq];
         double4 u = make_double4(1.0, 0.0, 1.0, 0.0);
         if (q < B) {
-          const double2* rp = row_of(p);
           double tb;
-          u = jacobi_rotation(rp[p].x, row_of(q)[q].x, rp[q], &tb);
+          u = jacobi_rotation(slots[op + p].x, slots[oq + q].x, slots[op + q], &tb);
         }
         const int t = e * g + j;
         cl.map_shared_rank(rb, dst)[t] = u;
         cl.map_shared_rank(pb, dst)[t] = make_uchar2((unsigned char)p, (unsigned char)q);
-        if (dst == me) job.rot[(size_t)nsteps * npairs + t] = u;
+        if (dst == me) s_own[j] = make_int4(op, q < B ? oq : -1, lp, lq);
       }
       cl.sync();
-      // U_j^H H[rows of pair j, columns of pair t2] U_t2 for own pairs j, all t2
-      for (int bi = tid; bi < g * npairs; bi += nthr) {
-        const int j = bi / npairs, t2 = bi - j * npairs, t1 = e * g + j;
-        const uchar2 pr = pb[t1], pc = pb[t2];
-        const int p = pr.x, q = pr.y, p2 = pc.x, q2 = pc.y;
-        if (p >= B || p2 >= B) continue;
-        const bool rq = q < B, cq = q2 < B;
-        double2* rp = row_of(p);
-        double2* rw = rq ? row_of(q) : nullptr;
-        const double2 z = make_double2(0.0, 0.0);
-        double2 x00 = rp[p2], x01 = cq ? rp[q2] : z, x10 = rq ? rw[p2] : z, x11 = (rq && cq) ? rw[q2] : z;
-        rot_block(x00, x01, x10, x11, rb[t1], rb[t2]);
-        if (t2 == t1) {
-          rp[p] = make_double2(x00.x, 0.0);
-          if (rq) {
-            rp[q] = z;
-            rw[p] = z;
-            rw[q] = make_double2(x11.x, 0.0);
+      // W <- W U over the own pairs (row r of W, columns lp and lq)
+      for (int i = tid; i < g * g2; i += nthr) {
+        const int j = i / g2, r = i - j * g2;
+        const int4 o = s_own[j];
+        double2* wr = W + r * g2;
+        double2 vp = wr[o.z], vq = wr[o.w];
+        rot_cols(vp, vq, rb[e * g + j]);
+        wr[o.z] = vp;
+        wr[o.w] = vq;
+      }
+      // U_j^H H[rows of own pair j, columns of pair t2] U_t2
+      if (jg < ngrp) {
+        const uchar2 pc = pb[t2];
+        const int p2 = pc.x, q2 = pc.y;
+        const bool cq = q2 < B;
+        const double4 u2 = rb[t2];
+        if (p2 < B)
+          for (int j = jg; j < g; j += ngrp) {
+            const int t1 = e * g + j;
+            const int4 o = s_own[j];
+            if (o.x < 0) continue;
+            const bool rq = o.y >= 0;
+            double2* rp = slots + o.x;
+            double2* rw = slots + (rq ? o.y : o.x);
+            double2 x00 = rp[p2], x01 = cq ? rp[q2] : zero, x10 = rq ? rw[p2] : zero,
+                    x11 = (rq && cq) ? rw[q2] : zero;
+            rot_block(x00, x01, x10, x11, rb[t1], u2);
+            if (t2 == t1) {  // (p2, q2) = (p, q)
+              rp[p2] = make_double2(x00.x, 0.0);
+              if (rq) {
+                rp[q2] = zero;
+                rw[p2] = zero;
+                rw[q2] = make_double2(x11.x, 0.0);
+              }
+            } else {
+              rp[p2] = x00;
+              if (cq) rp[q2] = x01;
+              if (rq) {
+                rw[p2] = x10;
+                if (cq) rw[q2] = x11;
+              }
+            }
           }
-        } else {
-          rp[p2] = x00;
-          if (cq) rp[q2] = x01;
-          if (rq) {
-            rw[p2] = x10;
-            if (cq) rw[q2] = x11;
-          }
-        }
       }
       __syncthreads();
     }
+    // log this round's block and restart it from the identity
+    {
+      double2* out = wlog + ((size_t)nrounds * kCl + e) * g2 * g2;
+      for (int i = tid; i < g2 * g2; i += nthr) {
+        out[i] = W[i];
+        W[i] = (i / g2 == i % g2) ? one : zero;
+      }
+    }
+    ++nrounds;
     // next round: every CTA keeps one group and pulls the other from its holder
     const int nr = round + 1 == ngroups - 1 ? 0 : round + 1;
-    if (tid == 0) {
-      int np[2 * kCl], ne[2 * kCl], keep[kCl], recv[kCl], src[kCl], srcslot[kCl], dstslot[kCl], nfree[kCl];
-      bool seen[kCl];
-      for (int x = 0; x < kCl; ++x) {
-        int a, b;
-        jacobi_pair(nr, x, ngroups, a, b);
-        np[a] = b;
-        np[b] = a;
-        ne[a] = ne[b] = x;
-        seen[x] = false;
-      }
-      for (int c0 = 0; c0 < kCl; ++c0) {
-        if (seen[c0]) continue;
-        int c = c0, kp = s_grp[c0][0];
-        for (int guard = 0; guard < kCl; ++guard) {  // an alternating cycle has at most kCl CTAs
-          const int rv = np[kp];
-          keep[c] = kp;
-          recv[c] = rv;
-          seen[c] = true;
-          const int c2 = s_gcta[rv];
-          if (seen[c2]) break;
-          kp = s_grp[c2][0] == rv ? s_grp[c2][1] : s_grp[c2][0];
-          c = c2;
-        }
-      }
-      for (int c = 0; c < kCl; ++c) {
-        src[c] = s_gcta[recv[c]];
-        srcslot[c] = s_gslot[recv[c]];
-        if (src[c] == c) {
-          dstslot[c] = srcslot[c];
-          nfree[c] = s_free[c];
-        } else {
-          const int sent = s_grp[c][0] == keep[c] ? s_grp[c][1] : s_grp[c][0];
-          dstslot[c] = s_free[c];
-          nfree[c] = s_gslot[sent];
-        }
-      }
-      for (int c = 0; c < kCl; ++c) {
-        s_gcta[recv[c]] = c;
-        s_gslot[recv[c]] = dstslot[c];
-        s_free[c] = nfree[c];
-        s_grp[c][0] = min(keep[c], recv[c]);
-        s_grp[c][1] = max(keep[c], recv[c]);
-        s_edge[c] = ne[keep[c]];
-      }
-      s_src = src[me];
-      s_srcslot = srcslot[me];
-      s_dst = dstslot[me];
-    }
+    const uint32_t tr = c_cluster_sched[(nrounds - 1) * kCl + me];
+    ga = tr & 15;
+    gb = (tr >> 4) & 15;
+    e = (tr >> 8) & 7;
+    sa = (tr >> 11) & 3;
+    sb = (tr >> 13) & 3;
     cl.sync();  // every CTA's updates of the finished round are visible
-    if (s_src != me) {
-      const double2* from = cl.map_shared_rank(slots, s_src) + (size_t)s_srcslot * slot_elems;
-      double2* to = slots + (size_t)s_dst * slot_elems;
-      for (size_t i = tid; i < slot_elems; i += nthr) to[i] = from[i];
+    if ((tr >> 22) & 1) {
+      const double2* from = cl.map_shared_rank(slots, (int)((tr >> 15) & 7)) + (size_t)((tr >> 18) & 3) * slot_elems;
+      double2* to = slots + (size_t)((tr >> 20) & 3) * slot_elems;
+      constexpr int U = 4;  // independent remote loads in flight per thread
+      for (int i0 = tid; i0 < slot_elems; i0 += U * nthr) {
+        double2 v[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (i0 + u * nthr < slot_elems) v[u] = from[i0 + u * nthr];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+          if (i0 + u * nthr < slot_elems) to[i0 + u * nthr] = v[u];
+      }
+    }
+    if (tid < g2) {
+      const int l = tid % g, gl = (tid < g ? ga : gb) * g + l;
+      s_rowoff[tid] = gl < B ? ((tid < g ? sa : sb) * g + l) * B : -1;
     }
     __syncthreads();
     round = nr;
     if (round == 0) ++sweep;
   }
   // eigenvalues: every CTA sends its diagonal to rank 0, which ranks them
-  for (int i = tid; i < 2 * g; i += nthr) {
-    const int l = s_grp[me][i / g] * g + (i % g);
-    if (l < B) cl.map_shared_rank(diag, 0)[l] = row_of(l)[l].x;
+  {
+    for (int l = tid; l < g2; l += nthr) {
+      const int gl = cluster_index(l, ga, gb, g), o = s_rowoff[l];
+      if (o >= 0) cl.map_shared_rank(diag, 0)[gl] = slots[o + gl].x;
+    }
   }
   cl.sync();
   if (me == 0) {
@@ -729,6 +739,85 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
       job.jst[1 + i] = r;
     }
     if (tid == 0) job.jst[0] = nsteps;
+  }
+}
+
+// Q[k][rank[c]] = (e_k^T W_1 W_2 ... )[c] for the logged block-diagonal
+// round products of k_jacobi_cluster: each CTA keeps kVbRows rows of Q in
+// shared memory and, per round, stages the round's kCl blocks and replaces
+// each row's 2g entries of every block by their product with the block.
+constexpr int kVbRows = 2;
+constexpr int kVbThreads = 256;
+constexpr int kVbItems = (kVbRows * kCl * 2 * kClMaxG + kVbThreads - 1) / kVbThreads;
+
+size_t jacobi_vectors_blocks_smem(int B) {
+  const int Bp = jacobi_cluster_bp(B), g2 = Bp / kCl;
+  return sizeof(double2) * ((size_t)kCl * g2 * g2 + (size_t)kVbRows * Bp) + sizeof(int) * kCl * g2;
+}
+
+__global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs jobs) {
+  extern __shared__ __align__(16) unsigned char vsm[];
+  const JacobiJob job = jobs.j[blockIdx.y];
+  const int B = job.B, Bp = jacobi_cluster_bp(B), g = Bp / (2 * kCl), g2 = 2 * g, ngroups = 2 * kCl;
+  const int k0 = blockIdx.x * kVbRows;
+  if (k0 >= B) return;  // uniform over the CTA
+  const int bsz = g2 * g2;
+  double2* Wsm = reinterpret_cast<double2*>(vsm);  // kCl blocks of the round
+  double2* rows = Wsm + kCl * bsz;                  // kVbRows x Bp
+  int* idx = reinterpret_cast<int*>(rows + kVbRows * Bp);  // kCl x 2g logical index of each block position
+  const double2* __restrict__ wlog = reinterpret_cast<const double2*>(job.rot);
+  for (int i = threadIdx.x; i < kVbRows * Bp; i += blockDim.x) {
+    const int r = i / Bp, c = i - r * Bp;
+    rows[i] = make_double2(k0 + r == c ? 1.0 : 0.0, 0.0);
+  }
+  const int rounds = job.jst[0] / (Bp - 1) * (ngroups - 1);
+  const int items = kVbRows * kCl * g2;
+  for (int rd = 0; rd < rounds; ++rd) {
+    const int r = rd % (ngroups - 1);
+    __syncthreads();  // the previous round's rows are written
+    const double2* src = wlog + (size_t)rd * kCl * bsz;
+    for (int i = threadIdx.x; i < kCl * bsz; i += blockDim.x) __pipeline_memcpy_async(Wsm + i, src + i, sizeof(double2));
+    __pipeline_commit();
+    for (int i = threadIdx.x; i < kCl * g2; i += blockDim.x) {
+      const int e = i / g2, l = i - e * g2;
+      int ga, gb;
+      jacobi_pair(r, e, ngroups, ga, gb);
+      idx[i] = cluster_index(l, ga, gb, g);
+    }
+    __pipeline_wait_prior(0);
+    __syncthreads();
+    double2 y[kVbItems];
+#pragma unroll
+    for (int it = 0; it < kVbItems; ++it) {
+      const int item = threadIdx.x + it * kVbThreads;
+      y[it] = make_double2(0.0, 0.0);
+      if (item < items) {
+        const int m = item % g2, e = (item / g2) % kCl, rr = item / (g2 * kCl);
+        const double2* x = rows + rr * Bp;
+        const int* ix = idx + e * g2;
+        const double2* w = Wsm + e * bsz + m;
+        double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+        for (int l = 0; l < g2; l += 2) {
+          a0 = zfma(x[ix[l]], w[l * g2], a0);
+          a1 = zfma(x[ix[l + 1]], w[(l + 1) * g2], a1);
+        }
+        y[it] = zadd(a0, a1);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int it = 0; it < kVbItems; ++it) {
+      const int item = threadIdx.x + it * kVbThreads;
+      if (item < items) {
+        const int m = item % g2, e = (item / g2) % kCl, rr = item / (g2 * kCl);
+        rows[rr * Bp + idx[e * g2 + m]] = y[it];
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kVbRows * B; i += blockDim.x) {
+    const int rr = i / B, c = i - rr * B, k = k0 + rr;
+    if (k < B) job.Q[(size_t)k * B + job.jst[1 + c]] = rows[rr * Bp + c];
   }
 }
 
@@ -768,7 +857,7 @@ __global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jo
   const double4* __restrict__ rot = job.rot;
   const int* __restrict__ jst = job.jst;
   double2* __restrict__ Q = job.Q;
-  const int Bp = job.ptab ? jacobi_cluster_bp(B) : B + (B & 1), npairs = Bp / 2;
+  const int Bp = B + (B & 1), npairs = Bp / 2;
   double4* lg = reinterpret_cast<double4*>(vsm);                   // chunk x npairs
   double2* rows = reinterpret_cast<double2*>(lg + chunk * npairs);  // kVecWarps x B
   uchar2* ptab = reinterpret_cast<uchar2*>(rows + kVecWarps * B);   // (Bp - 1) x npairs
@@ -776,10 +865,7 @@ __global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jo
   const int k = blockIdx.x * kVecWarps + warp;
   double2* row = rows + warp * B;
   for (int p = lane; p < B; p += 32) row[p] = make_double2(p == k ? 1.0 : 0.0, 0.0);
-  if (job.ptab)
-    for (int i = threadIdx.x; i < (Bp - 1) * npairs; i += blockDim.x) ptab[i] = job.ptab[i];
-  else
-    jacobi_pair_table(ptab, Bp);
+  jacobi_pair_table(ptab, Bp);
   const int nsteps = jst[0];
   int step = 0;
   for (int s0 = 0; s0 < nsteps; s0 += chunk) {
@@ -822,7 +908,6 @@ __global__ void k_to_kernels(const double2* __restrict__ U, int N, int ldu, int 
 struct Workspace {
   double2 *X = nullptr, *W = nullptr, *Z = nullptr, *G = nullptr, *Rinv = nullptr, *Q = nullptr;
   double4* rot = nullptr;
-  uchar2* ptab = nullptr;
   double* w = nullptr;
   int *status = nullptr, *jst = nullptr;
   cudaStream_t st = nullptr;
@@ -867,15 +952,101 @@ bool jacobi_use_cluster(int B) {
   }
   return ok == 1;
 }
+// c_cluster_sched: the host walks the same state the kernel's groups move
+// through.  After each round every CTA keeps one of its groups and takes the
+// other group of its next edge from the CTA holding it; following the
+// alternating cycles of the two matchings (edge of CTA c -> the next-round
+// edge at the group c keeps -> the CTA holding that edge's other group ...)
+// gives every CTA exactly one group to send and one to receive.
+std::vector<uint32_t> cluster_schedule() {
+  const int ng = 2 * kCl, rounds = ng - 1;
+  std::vector<uint32_t> tab((size_t)kJacobiMaxSweeps * rounds * kCl);
+  int grp[kCl][2], gcta[2 * kCl], gslot[2 * kCl], fre[kCl];
+  for (int c = 0; c < kCl; ++c) {
+    int a, b;
+    jacobi_pair(0, c, ng, a, b);
+    grp[c][0] = a;
+    grp[c][1] = b;
+    gcta[a] = gcta[b] = c;
+    gslot[a] = 0;
+    gslot[b] = 1;
+    fre[c] = 2;
+  }
+  for (int t = 0; t < kJacobiMaxSweeps * rounds; ++t) {
+    const int nr = (t + 1) % rounds;
+    int np[2 * kCl], ne[2 * kCl], keep[kCl], recv[kCl], src[kCl], srcslot[kCl], dst[kCl], nfree[kCl];
+    bool seen[kCl];
+    for (int x = 0; x < kCl; ++x) {
+      int a, b;
+      jacobi_pair(nr, x, ng, a, b);
+      np[a] = b;
+      np[b] = a;
+      ne[a] = ne[b] = x;
+      seen[x] = false;
+    }
+    for (int c0 = 0; c0 < kCl; ++c0) {
+      if (seen[c0]) continue;
+      int c = c0, kp = grp[c0][0];
+      for (int guard = 0; guard < kCl; ++guard) {
+        const int rv = np[kp];
+        keep[c] = kp;
+        recv[c] = rv;
+        seen[c] = true;
+        const int c2 = gcta[rv];
+        if (seen[c2]) break;
+        kp = grp[c2][0] == rv ? grp[c2][1] : grp[c2][0];
+        c = c2;
+      }
+    }
+    for (int c = 0; c < kCl; ++c) {
+      src[c] = gcta[recv[c]];
+      srcslot[c] = gslot[recv[c]];
+      if (src[c] == c) {
+        dst[c] = srcslot[c];
+        nfree[c] = fre[c];
+      } else {
+        const int sent = grp[c][0] == keep[c] ? grp[c][1] : grp[c][0];
+        dst[c] = fre[c];
+        nfree[c] = gslot[sent];
+      }
+    }
+    for (int c = 0; c < kCl; ++c) {
+      gcta[recv[c]] = c;
+      gslot[recv[c]] = dst[c];
+      fre[c] = nfree[c];
+      grp[c][0] = std::min(keep[c], recv[c]);
+      grp[c][1] = std::max(keep[c], recv[c]);
+    }
+    for (int c = 0; c < kCl; ++c) {
+      const int a = grp[c][0], b = grp[c][1];
+      tab[(size_t)t * kCl + c] = (uint32_t)a | (uint32_t)b << 4 | (uint32_t)ne[keep[c]] << 8 |
+                                 (uint32_t)gslot[a] << 11 | (uint32_t)gslot[b] << 13 | (uint32_t)src[c] << 15 |
+                                 (uint32_t)srcslot[c] << 18 | (uint32_t)dst[c] << 20 | (uint32_t)(src[c] != c) << 22;
+    }
+  }
+  return tab;
+}
+
+// uploads c_cluster_sched once per device, ordered before work later queued on st
+int ensure_cluster_schedule(cudaStream_t st) {
+  static const std::vector<uint32_t> tab = cluster_schedule();
+  static bool done[64] = {};
+  int dev = 0;
+  KL_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 64 && done[dev]) return KL_OK;
+  KL_CUDA_TRY(cudaMemcpyToSymbolAsync(c_cluster_sched, tab.data(), sizeof(uint32_t) * tab.size(), 0,
+                                      cudaMemcpyHostToDevice, st));
+  KL_CUDA_TRY(cudaStreamSynchronize(st));
+  if (dev < 64) done[dev] = true;
+  return KL_OK;
+}
+
 // padded order of the sweep (pairs per step = order / 2, steps per sweep = order - 1)
 int jacobi_order(int B) { return jacobi_use_cluster(B) ? jacobi_cluster_bp(B) : B + (B & 1); }
-size_t jacobi_log_elems(int B) {
+size_t jacobi_log_elems(int B) {  // double4 units
+  if (jacobi_use_cluster(B)) return (cluster_log_elems(B, kJacobiMaxSweeps) + 1) / 2;
   const int Bp = jacobi_order(B);
   return (size_t)kJacobiMaxSweeps * (Bp - 1) * (Bp / 2) + 1;
-}
-size_t jacobi_ptab_elems(int B) {
-  const int Bp = jacobi_order(B);
-  return jacobi_use_cluster(B) ? (size_t)(Bp - 1) * (Bp / 2) : 1;
 }
 
 // X (N x B) <- orth(X) by CholeskyQR2; the first pass shifted for safety
@@ -907,22 +1078,26 @@ int jacobi_batch(const std::vector<JacobiJob>& all, cudaStream_t st) {
       int bmax = 1, bpmax = 2;
       for (int j = 0; j < nj; ++j) {
         jobs.j[j] = v[j0 + j];
-        if (!cluster) jobs.j[j].ptab = nullptr;
-        KL_CHECK_ARG(!cluster || jobs.j[j].ptab, "jacobi: the cluster solver needs a pair table");
         bmax = std::max(bmax, jobs.j[j].B);
         bpmax = std::max(bpmax, jacobi_order(jobs.j[j].B));
       }
       if (cluster) {
+        if (int rc = ensure_cluster_schedule(st)) return rc;
         const size_t sm = ClusterSmem(bmax).total;
         KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_jacobi_cluster<<<nj * kCl, kClThreads, sm, st>>>(jobs, kJacobiMaxSweeps);
-      } else {
-        const bool in_smem = jacobi_h_in_smem(bmax);
-        const size_t sm = JacobiSmem(bmax).total_no_h + (in_smem ? sizeof(double2) * (size_t)bmax * bmax : 0);
-        if (sm > 48 * 1024)
-          KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_jacobi<<<nj, kJacobiThreads, sm, st>>>(jobs, in_smem ? 1 : 0, kJacobiMaxSweeps);
+        KL_CUDA_TRY(cudaGetLastError());
+        const size_t vsm = jacobi_vectors_blocks_smem(bmax);
+        KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_vectors_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
+        k_jacobi_vectors_blocks<<<dim3((bmax + kVbRows - 1) / kVbRows, nj), kVbThreads, vsm, st>>>(jobs);
+        KL_CUDA_TRY(cudaGetLastError());
+        continue;
       }
+      const bool in_smem = jacobi_h_in_smem(bmax);
+      const size_t sm = JacobiSmem(bmax).total_no_h + (in_smem ? sizeof(double2) * (size_t)bmax * bmax : 0);
+      if (sm > 48 * 1024)
+        KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      k_jacobi<<<nj, kJacobiThreads, sm, st>>>(jobs, in_smem ? 1 : 0, kJacobiMaxSweeps);
       KL_CUDA_TRY(cudaGetLastError());
       const size_t vsm = jacobi_vectors_smem(bmax, bpmax);
       if (vsm > 48 * 1024)
@@ -936,10 +1111,8 @@ int jacobi_batch(const std::vector<JacobiJob>& all, cudaStream_t st) {
 }
 
 // Q (B x B, column j = eigenvector j) and w (descending) of the Hermitian H
-int jacobi(double2* H, int B, double4* rot, uchar2* ptab, int* jst, double2* Q, double* w, cudaStream_t st) {
-  JacobiJob j{H, rot, Q, w, jst, B};
-  j.ptab = ptab;
-  return jacobi_batch({j}, st);
+int jacobi(double2* H, int B, double4* rot, int* jst, double2* Q, double* w, cudaStream_t st) {
+  return jacobi_batch({JacobiJob{H, rot, Q, w, jst, B}}, st);
 }
 
 // Generic driver.  apply(X, W): W = TCC X (N x B); project(X, H): H = X^H TCC X (B x B).
@@ -953,7 +1126,6 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   if ((arc = ws.get(&ws.X, (size_t)N * B)) || (arc = ws.get(&ws.W, (size_t)N * B)) ||
       (arc = ws.get(&ws.G, (size_t)B * B)) || (arc = ws.get(&ws.Rinv, (size_t)B * B)) ||
       (arc = ws.get(&ws.Q, (size_t)B * B)) || (arc = ws.get(&ws.rot, jacobi_log_elems(B))) ||
-      (arc = ws.get(&ws.ptab, jacobi_ptab_elems(B))) ||
       (arc = ws.get(&ws.jst, (size_t)B + 1)) || (arc = ws.get(&ws.w, (size_t)B)) ||
       (arc = ws.get(&ws.status, 1)))
     return arc;
@@ -977,7 +1149,7 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   for (it = 1; it <= opt.max_iter; ++it) {
     if (it % check_every == 0) {
       if ((rc = project(ws.X, ws.G))) return rc;
-      if ((rc = jacobi(ws.G, B, ws.rot, ws.ptab, ws.jst, ws.Q, ws.w, st))) return rc;
+      if ((rc = jacobi(ws.G, B, ws.rot, ws.jst, ws.Q, ws.w, st))) return rc;
       KL_CUDA_TRY(cudaMemcpyAsync(cur.data(), ws.w, sizeof(double) * B, cudaMemcpyDeviceToHost, st));
       KL_CUDA_TRY(cudaStreamSynchronize(st));
       change = 0.0;
@@ -1002,7 +1174,7 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
   // final Rayleigh-Ritz on the current block (G holds the eigvecs in Q)
   if (!converged) {
     if ((rc = project(ws.X, ws.G))) return rc;
-    if ((rc = jacobi(ws.G, B, ws.rot, ws.ptab, ws.jst, ws.Q, ws.w, st))) return rc;
+    if ((rc = jacobi(ws.G, B, ws.rot, ws.jst, ws.Q, ws.w, st))) return rc;
   }
   // U = X Q[:, :K] (N x K, row-major), eigenvalues
   if ((rc = zgemm<G_NN>(ws.X, B, ws.Q, B, ws.W, B, N, B, B, st))) return rc;
@@ -1063,14 +1235,12 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
     w.st = st;
     int arc;
     if ((arc = w.get(&w.G, (size_t)S * S)) || (arc = w.get(&w.Q, (size_t)S * S)) ||
-        (arc = w.get(&w.rot, jacobi_log_elems(S))) || (arc = w.get(&w.ptab, jacobi_ptab_elems(S))) ||
-        (arc = w.get(&w.jst, (size_t)S + 1)) ||
+        (arc = w.get(&w.rot, jacobi_log_elems(S))) || (arc = w.get(&w.jst, (size_t)S + 1)) ||
         (arc = w.get(&w.W, (size_t)S * K)) || (arc = w.get(&w.w, (size_t)S)))
       return arc;
     int rc = zgemm<G_AHA>(pr[i].A, S, pr[i].A, S, w.G, S, S, S, pr[i].N, st);
     if (rc) return rc;
     jobs[i] = JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S};
-    jobs[i].ptab = w.ptab;
   }
   int rc = jacobi_batch(jobs, st);
   if (rc) return rc;
