@@ -551,9 +551,9 @@ def bench_tcc_eigen(args):
 def bench_tcc_eigen_large(args):
     """TCC + top-K eigen at the stress field: 4096^2, cross-quadrupole
     (0.75, 0.12) on an 81^2 grid (196 source points), NA 1.35 water, K = 64,
-    block 96.  Fast path: FP32 factor + subspace iteration on A(A^H X) with
-    FP64 CholeskyQR2 and Rayleigh-Ritz (S > 128, so no one-step Gram solve);
-    five focus values.  Plain FP64 GPU path: FP64 TCC by direct accumulation
+    block 96.  Fast path: FP32 factor + the one-step Rayleigh-Ritz solve on
+    span(A) (FP64 Gram A^H A, 196 x 196, eigensolved by the thread-block-cluster
+    Jacobi); five focus values.  Plain FP64 GPU path: FP64 TCC by direct accumulation
     (N = 11449, 2.1 GB) and FP64 subspace iteration on the dense TCC, at one
     focus value (seconds per focus)."""
     import torch

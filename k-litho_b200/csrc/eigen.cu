@@ -470,7 +470,10 @@ __global__ void __launch_bounds__(kJacobiThreads) k_jacobi(JacobiJobs jobs, int 
 // k_jacobi_vectors_blocks forms the eigenvectors from these blocks.
 // ---------------------------------------------------------------------------
 constexpr int kCl = 8;            // CTAs per matrix (portable cluster size)
-constexpr int kClThreads = 512;
+constexpr int kClUpdThreads = 480;                // warps that update H
+constexpr int kClThreads = kClUpdThreads + 32;     // + one warp for the rotations
+constexpr int kClRotBufs = 3;                      // rotation slots: steps s, s + 1 and s + 2 in flight
+constexpr unsigned long long kClWaitNs = 2000000000ull;  // bound on one rotation wait
 constexpr int kClMaxG = kGramMaxS / (2 * kCl);  // largest group
 
 __host__ __device__ inline int jacobi_cluster_bp(int B) { return (B + 2 * kCl - 1) / (2 * kCl) * (2 * kCl); }
@@ -483,9 +486,9 @@ struct ClusterSmem {
     g = Bp / (2 * kCl);
     npairs = Bp / 2;
     rows = 0;                                                      // 3 slots x g rows x B
-    rot = sizeof(double2) * 3 * (size_t)g * B;                     // 2 x npairs double4
-    pq = rot + sizeof(double4) * 2 * npairs;                       // 2 x npairs uchar2
-    w = (pq + sizeof(uchar2) * 2 * npairs + 15) & ~size_t(15);     // 2g x 2g double2
+    rot = sizeof(double2) * 3 * (size_t)g * B;                     // kClRotBufs x npairs double4
+    pq = rot + sizeof(double4) * kClRotBufs * npairs;              // kClRotBufs x npairs uchar2
+    w = (pq + sizeof(uchar2) * kClRotBufs * npairs + 15) & ~size_t(15);  // 2g x 2g double2
     r0 = w + sizeof(double2) * 4 * (size_t)g * g;                  // (2g - 1) x g uchar2
     part = (r0 + sizeof(uchar2) * (2 * g - 1) * g + 15) & ~size_t(15);  // kCl x 2 double
     diag = part + sizeof(double) * 2 * kCl;                        // Bp double (rank 0)
@@ -511,11 +514,54 @@ __device__ __forceinline__ int cluster_index(int l, int ga, int gb, int g) {
   return l < g ? ga * g + l : gb * g + l - g;
 }
 
+// local positions of pair j at step k of a round
+__device__ __forceinline__ void cluster_local_pair(const uchar2* r0, int round, int k, int j, int g, int& lp, int& lq) {
+  if (round == 0) {
+    const uchar2 v = r0[k * g + j];
+    lp = v.x;
+    lq = v.y;
+  } else {
+    lp = j;
+    lq = j + k < g ? g + j + k : j + k;  // g + (j + k) mod g
+  }
+}
+
 // row[p], row[q] <- the pair's columns of row . U (U as in rot_block's right factor)
 __device__ __forceinline__ void rot_cols(double2& vp, double2& vq, double4 u) {
   const double2 e = zmul(vq, make_double2(u.z, -u.w)), a = vp;
   vp = make_double2(u.x * a.x - u.y * e.x, u.x * a.y - u.y * e.y);
   vq = make_double2(u.y * a.x + u.x * e.x, u.y * a.y + u.x * e.y);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// relaxed arrive on the barrier at the same offset in CTA `cta` (the caller
+// orders its earlier stores with fence.acq_rel.cluster)
+__device__ __forceinline__ void mbar_arrive_relaxed(uint64_t* bar, uint32_t cta) {
+  uint32_t remote;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(bar)), "r"(cta));
+  asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// bounded wait for a barrier phase; false if it did not complete in kClWaitNs
+__device__ __forceinline__ bool mbar_wait_cluster(uint64_t* bar, uint32_t parity) {
+  if (mbar_try_cluster(bar, parity)) return true;
+  unsigned long long t0, t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+  while (!mbar_try_cluster(bar, parity)) {
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (t - t0 > kClWaitNs) return false;
+  }
+  return true;
 }
 
 __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
@@ -538,10 +584,22 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
   double* diag = reinterpret_cast<double*>(csm + L.diag);
   double2* wlog = reinterpret_cast<double2*>(job.rot);
   __shared__ int s_rowoff[2 * kClMaxG];  // element offset of local position l's row, -1: padding
-  __shared__ int4 s_own[kClMaxG];        // own pair j of the step: row offsets of p, q (-1: padding), lp, lq
+  __shared__ int4 s_own[2][kClMaxG];     // own pair j of the step: row offsets of p, q (-1: padding), lp, lq
+  __shared__ double s_newdiag[2 * kClMaxG];  // diagonal at local position l after the last rotations
+  __shared__ int s_pairof[2 * kClMaxG];      // own pair holding local position l (+256: second index)
   __shared__ double s_red[2][kClThreads / 32];
+  // rotation slot b is complete when every CTA's g rotation lanes have arrived
+  __shared__ __align__(8) uint64_t s_bar[kClRotBufs];
+  __shared__ int s_fail, s_anyfail;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
   const double2 zero = make_double2(0.0, 0.0), one = make_double2(1.0, 0.0);
+  if (tid == 0) {
+    for (int b = 0; b < kClRotBufs; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_bar[b])), "r"(g * kCl) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+    s_anyfail = 0;
+  }
   // this CTA's groups (ga < gb), their slots and its matching edge; round 0 starts with edge me
   int ga, gb, sa = 0, sb = 1, e = me;
   jacobi_pair(0, me, ngroups, ga, gb);
@@ -562,8 +620,9 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
     s_rowoff[tid] = gl < B ? ((tid < g ? sa : sb) * g + l) * B : -1;
   }
   __syncthreads();
-  // the H update: thread (jg, t2) applies column pair t2 to own row pairs jg, jg + ngrp, ...
-  const int ngrp = nthr / npairs, t2 = tid % npairs, jg = tid / npairs;
+  // the H update: thread (jg, t2) applies column pair t2 to own row pairs jg, jg + ngrp, ...;
+  // the last warp computes the rotations
+  const int rwarp = kClUpdThreads / 32, ngrp = kClUpdThreads / npairs, t2 = tid % npairs, jg = tid / npairs;
 
   int nsteps = 0, sweep = 0, round = 0, nrounds = 0;
   while (true) {
@@ -605,54 +664,140 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
     }
     const int nk = round == 0 ? g2 - 1 : g;
     for (int k = 0; k < nk; ++k, ++nsteps) {
-      const int par = nsteps & 1;
-      double4* rb = rotx + par * npairs;
-      uchar2* pb = pqx + par * npairs;
-      // this CTA's g rotations, stored into every CTA (thread i: pair i % g, CTA i / g)
-      for (int i = tid; i < g * kCl; i += nthr) {
-        const int dst = i / g, j = i - dst * g;
-        int lp, lq;
-        if (round == 0) {
-          const uchar2 v = r0[k * g + j];
-          lp = v.x;
-          lq = v.y;
-        } else {
-          lp = j;
-          lq = j + k < g ? g + j + k : j + k;  // g + (j + k) mod g
+      const int par = nsteps & 1, bsel = nsteps % kClRotBufs, bnext = bsel + 1 == kClRotBufs ? 0 : bsel + 1;
+      double4* rb = rotx + bsel * npairs;
+      uchar2* pb = pqx + bsel * npairs;
+      const int4* own = s_own[par];
+      // rotation warp: lane L handles own pair j = L % 16 and pushes it to CTAs
+      // 4 (L / 16) .. 4 (L / 16) + 3 (every slot entry has one writer that
+      // arrives once on the receiving CTA's barrier: g kCl arrivals a step)
+      const int j = lane & 15, c0 = (lane >> 4) * (kCl / 2);
+      const bool rlane = warp == rwarp && j < g;
+      // before the wait: the step's own rotations at a round start, then the
+      // entries (of the not yet updated H) that fix the next step's rotations:
+      // pair j of step k + 1 joins position lpn of own pair ja with lqn of own
+      // pair jb, and H'[p'][q'] is one entry of the rotated block (ja, jb)
+      int ja = 0, jb = 0, lpn = 0, lqn = 0;
+      double2 X00 = zero, X01 = zero, X10 = zero, X11 = zero;
+      if (warp == rwarp) {
+        if (k == 0 && rlane) {
+          int lp, lq;
+          cluster_local_pair(r0, round, 0, j, g, lp, lq);
+          const int p = cluster_index(lp, ga, gb, g), q = cluster_index(lq, ga, gb, g);
+          const int op = s_rowoff[lp], oq = s_rowoff[lq];
+          double4 u = make_double4(1.0, 0.0, 1.0, 0.0);
+          double na = 0.0, nd = 0.0;
+          if (q < B) {
+            double tb;
+            const double a = slots[op + p].x, d = slots[oq + q].x;
+            u = jacobi_rotation(a, d, slots[op + q], &tb);
+            na = a - tb;
+            nd = d + tb;
+          } else if (p < B) {
+            na = slots[op + p].x;
+          }
+          if (lane < 16) {
+            if (p < B) s_newdiag[lp] = na;
+            if (q < B) s_newdiag[lq] = nd;
+            s_own[par][j] = make_int4(op, q < B ? oq : -1, lp, lq);
+          }
+          for (int c = c0; c < c0 + kCl / 2; ++c) {
+            cl.map_shared_rank(rb, c)[e * g + j] = u;
+            cl.map_shared_rank(pb, c)[e * g + j] = make_uchar2((unsigned char)p, (unsigned char)q);
+          }
+          asm volatile("fence.acq_rel.cluster;" ::: "memory");
+          for (int c = c0; c < c0 + kCl / 2; ++c) mbar_arrive_relaxed(&s_bar[bsel], c);
         }
-        const int p = cluster_index(lp, ga, gb, g), q = cluster_index(lq, ga, gb, g);
-        const int op = s_rowoff[lp], oq = s_rowoff[lq];
-        double4 u = make_double4(1.0, 0.0, 1.0, 0.0);
-        if (q < B) {
-          double tb;
-          u = jacobi_rotation(slots[op + p].x, slots[oq + q].x, slots[op + q], &tb);
+        __syncwarp();
+        if (k + 1 < nk) {
+          if (lane < g) {
+            const int4 o = own[lane];
+            s_pairof[o.z] = lane;
+            s_pairof[o.w] = lane | 256;
+          }
+          __syncwarp();
+          if (rlane) {
+            cluster_local_pair(r0, round, k + 1, j, g, lpn, lqn);
+            ja = s_pairof[lpn];
+            jb = s_pairof[lqn];
+            const int4 oa = own[ja & 255], ob = own[jb & 255];
+            const int pc = cluster_index(ob.z, ga, gb, g), qc = cluster_index(ob.w, ga, gb, g);
+            if (oa.x >= 0 && pc < B) {
+              const double2* rp = slots + oa.x;
+              X00 = rp[pc];
+              if (qc < B) X01 = rp[qc];
+              if (oa.y >= 0) {
+                const double2* rw = slots + oa.y;
+                X10 = rw[pc];
+                if (qc < B) X11 = rw[qc];
+              }
+            }
+          }
         }
-        const int t = e * g + j;
-        cl.map_shared_rank(rb, dst)[t] = u;
-        cl.map_shared_rank(pb, dst)[t] = make_uchar2((unsigned char)p, (unsigned char)q);
-        if (dst == me) s_own[j] = make_int4(op, q < B ? oq : -1, lp, lq);
       }
-      cl.sync();
-      // W <- W U over the own pairs (row r of W, columns lp and lq)
-      for (int i = tid; i < g * g2; i += nthr) {
-        const int j = i / g2, r = i - j * g2;
-        const int4 o = s_own[j];
-        double2* wr = W + r * g2;
-        double2 vp = wr[o.z], vq = wr[o.w];
-        rot_cols(vp, vq, rb[e * g + j]);
-        wr[o.z] = vp;
-        wr[o.w] = vq;
+      // this step's rotations from every CTA (the slot's phase: uses of the slot so far);
+      // after one timeout the CTA stops waiting, finishes quickly and reports it
+      if (!*(volatile int*)&s_fail && !mbar_wait_cluster(&s_bar[bsel], (uint32_t)((nsteps / kClRotBufs) & 1)))
+        s_fail = 1;
+      if (warp != rwarp) {
+        // W <- W U over the own pairs (row r, columns lp and lq; W is kept
+        // column-major so that consecutive rows are consecutive words)
+        for (int i = tid; i < g * g2; i += kClUpdThreads) {
+          const int jj = i / g2, r = i - jj * g2;
+          const int4 o = own[jj];
+          double2 vp = W[o.z * g2 + r], vq = W[o.w * g2 + r];
+          rot_cols(vp, vq, rb[e * g + jj]);
+          W[o.z * g2 + r] = vp;
+          W[o.w * g2 + r] = vq;
+        }
       }
-      // U_j^H H[rows of own pair j, columns of pair t2] U_t2
-      if (jg < ngrp) {
+      // the rotation warp has read its entries of H: the update may begin
+      asm volatile("bar.sync 1, %0;" ::"r"(kClThreads) : "memory");
+      if (warp == rwarp) {
+        if (k + 1 < nk && rlane) {
+          // the next step's rotation and diagonal, pushed while the other warps update H
+          const int pn = cluster_index(lpn, ga, gb, g), qn = cluster_index(lqn, ga, gb, g);
+          const int opn = s_rowoff[lpn], oqn = s_rowoff[lqn];
+          double4 u = make_double4(1.0, 0.0, 1.0, 0.0);
+          double na = 0.0, nd = 0.0;
+          if (qn < B) {
+            rot_block(X00, X01, X10, X11, rb[e * g + (ja & 255)], rb[e * g + (jb & 255)]);
+            const double2 x = (ja & 256) ? ((jb & 256) ? X11 : X10) : ((jb & 256) ? X01 : X00);
+            const double a = s_newdiag[lpn], d = s_newdiag[lqn];
+            double tb;
+            u = jacobi_rotation(a, d, x, &tb);
+            na = a - tb;
+            nd = d + tb;
+          }
+          // both half-warps have read s_newdiag before the lower half rewrites it
+          const unsigned rmask = (1u << g) - 1u;
+          __syncwarp(rmask | rmask << 16);
+          if (lane < 16) {
+            if (qn < B) {
+              s_newdiag[lpn] = na;
+              s_newdiag[lqn] = nd;
+            }
+            s_own[par ^ 1][j] = make_int4(opn, qn < B ? oqn : -1, lpn, lqn);
+          }
+          double4* rn = rotx + bnext * npairs;
+          uchar2* pn_ = pqx + bnext * npairs;
+          for (int c = c0; c < c0 + kCl / 2; ++c) {
+            cl.map_shared_rank(rn, c)[e * g + j] = u;
+            cl.map_shared_rank(pn_, c)[e * g + j] = make_uchar2((unsigned char)pn, (unsigned char)qn);
+          }
+          asm volatile("fence.acq_rel.cluster;" ::: "memory");
+          for (int c = c0; c < c0 + kCl / 2; ++c) mbar_arrive_relaxed(&s_bar[bnext], c);
+        }
+      } else if (jg < ngrp) {
+        // U_j^H H[rows of own pair j, columns of pair t2] U_t2
         const uchar2 pc = pb[t2];
         const int p2 = pc.x, q2 = pc.y;
         const bool cq = q2 < B;
         const double4 u2 = rb[t2];
         if (p2 < B)
-          for (int j = jg; j < g; j += ngrp) {
-            const int t1 = e * g + j;
-            const int4 o = s_own[j];
+          for (int jr = jg; jr < g; jr += ngrp) {
+            const int t1 = e * g + jr;
+            const int4 o = own[jr];
             if (o.x < 0) continue;
             const bool rq = o.y >= 0;
             double2* rp = slots + o.x;
@@ -681,11 +826,13 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
     }
     // log this round's block and restart it from the identity
     {
-      double2* out = wlog + ((size_t)nrounds * kCl + e) * g2 * g2;
+      double2* out = wlog + ((size_t)nrounds * kCl + e) * g2 * g2;  // row-major
       for (int i = tid; i < g2 * g2; i += nthr) {
-        out[i] = W[i];
-        W[i] = (i / g2 == i % g2) ? one : zero;
+        const int l = i / g2, m = i - l * g2;
+        out[i] = W[m * g2 + l];
       }
+      __syncthreads();
+      for (int i = tid; i < g2 * g2; i += nthr) W[i] = (i / g2 == i % g2) ? one : zero;
     }
     ++nrounds;
     // next round: every CTA keeps one group and pulls the other from its holder
@@ -720,6 +867,7 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
     if (round == 0) ++sweep;
   }
   // eigenvalues: every CTA sends its diagonal to rank 0, which ranks them
+  if (tid == 0 && s_fail) *cl.map_shared_rank(&s_anyfail, 0) = 1;
   {
     for (int l = tid; l < g2; l += nthr) {
       const int gl = cluster_index(l, ga, gb, g), o = s_rowoff[l];
@@ -738,7 +886,7 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
       job.w[r] = vi;
       job.jst[1 + i] = r;
     }
-    if (tid == 0) job.jst[0] = nsteps;
+    if (tid == 0) job.jst[0] = s_anyfail ? -1 : nsteps;  // -1: a rotation exchange timed out
   }
 }
 
@@ -930,11 +1078,13 @@ struct Workspace {
 constexpr size_t kJacobiSmemCap = 220 * 1024;
 bool jacobi_h_in_smem(int B) { return JacobiSmem(B).total_no_h + sizeof(double2) * (size_t)B * B <= kJacobiSmemCap; }
 
-// larger matrices (up to kGramMaxS) go to the cluster solver when the device
-// can co-schedule a cluster of kCl CTAs of its size; otherwise k_jacobi works
-// on H in place in global memory
+// matrices of kClusterMinB .. kGramMaxS go to the cluster solver when the
+// device can co-schedule a cluster of kCl CTAs of its size (eight SMs beat one
+// from about 64 up); otherwise k_jacobi keeps H in shared memory or works on
+// it in place in global memory
+constexpr int kClusterMinB = 64;
 bool jacobi_use_cluster(int B) {
-  if (jacobi_h_in_smem(B) || B > kGramMaxS) return false;
+  if (B < kClusterMinB || B > kGramMaxS) return false;
   static int ok = -1;
   if (ok < 0) {
     ok = 0;
@@ -1150,8 +1300,14 @@ int subspace_iteration(int N, const EigenOptions& opt, int B, Apply apply, Proje
     if (it % check_every == 0) {
       if ((rc = project(ws.X, ws.G))) return rc;
       if ((rc = jacobi(ws.G, B, ws.rot, ws.jst, ws.Q, ws.w, st))) return rc;
+      int jsteps = 0;
       KL_CUDA_TRY(cudaMemcpyAsync(cur.data(), ws.w, sizeof(double) * B, cudaMemcpyDeviceToHost, st));
+      KL_CUDA_TRY(cudaMemcpyAsync(&jsteps, ws.jst, sizeof(int), cudaMemcpyDeviceToHost, st));
       KL_CUDA_TRY(cudaStreamSynchronize(st));
+      if (jsteps < 0) {
+        set_error("subspace iteration: the cluster Jacobi eigensolve timed out exchanging rotations");
+        return KL_ERR_CUDA;
+      }
       change = 0.0;
       for (int k = 0; k < K; ++k) {
         const double den = std::max(std::fabs(cur[k]), 1e-300 + std::fabs(cur[0]) * 1e-16);
@@ -1256,6 +1412,10 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
   KL_CUDA_TRY(cudaStreamSynchronize(st));
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S;
+    if (nsteps[i] < 0) {
+      set_error("eig_topk_factor: the cluster Jacobi eigensolve timed out exchanging rotations");
+      return KL_ERR_CUDA;
+    }
     const int sweeps = nsteps[i] / (jacobi_order(S) - 1);
     if (sweeps >= kJacobiMaxSweeps) {
       set_error("eig_topk_factor: Jacobi eigensolve of the Gram matrix did not converge in " +
