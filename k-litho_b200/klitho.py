@@ -128,6 +128,14 @@ def _fp(a: np.ndarray):
     return a.ctypes.data_as(_c_float_p)
 
 
+def _planes_to_complex(re: np.ndarray, im: np.ndarray, shape) -> np.ndarray:
+    """complex64 array of `shape` from separate real and imaginary float32 planes."""
+    out = np.empty(shape, dtype=np.complex64)
+    out.real = re.reshape(shape)
+    out.imag = im.reshape(shape)
+    return out
+
+
 def _stream_ptr(stream) -> int | None:
     if stream is None:
         return None
@@ -404,24 +412,23 @@ class TccPlan:
     def topk(self, nk: int, block: int = 0):
         """(kernels nk x N complex64 in the reference layout, scales float32,
         eigenvalues float64, iterations)."""
-        re = np.zeros(nk * self.N, dtype=np.float32)
-        im = np.zeros(nk * self.N, dtype=np.float32)
+        re = np.empty(nk * self.N, dtype=np.float32)  # every entry is written
+        im = np.empty(nk * self.N, dtype=np.float32)
         sc = np.zeros(nk, dtype=np.float32)
         ev = np.zeros(nk, dtype=np.float64)
         it = ctypes.c_int()
         check(lib().kl_topk_eig(self._h, int(nk), int(block), _fp(re), _fp(im), _fp(sc),
                                 ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                 ctypes.byref(it)), "kl_topk_eig")
-        k = (re + 1j * im).astype(np.complex64).reshape(nk, self.N)
-        return k, sc, ev, it.value
+        return _planes_to_complex(re, im, (nk, self.N)), sc, ev, it.value
 
     @staticmethod
     def topk_batch(plans, nk: int, block: int = 0):
         """kl_topk_eig over several plans sharing N (e.g. a focus sweep) in one
         call: lists of (kernels, scales, eigenvalues, iterations) per plan."""
         n, N = len(plans), plans[0].N
-        re = np.zeros(n * nk * N, dtype=np.float32)
-        im = np.zeros(n * nk * N, dtype=np.float32)
+        re = np.empty(n * nk * N, dtype=np.float32)  # every entry is written
+        im = np.empty(n * nk * N, dtype=np.float32)
         sc = np.zeros(n * nk, dtype=np.float32)
         ev = np.zeros(n * nk, dtype=np.float64)
         it = np.zeros(n, dtype=np.int32)
@@ -429,7 +436,7 @@ class TccPlan:
         check(lib().kl_topk_eig_batch(hs, n, int(nk), int(block), _fp(re), _fp(im), _fp(sc),
                                       ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                       it.ctypes.data_as(_c_int_p)), "kl_topk_eig_batch")
-        k = (re + 1j * im).astype(np.complex64).reshape(n, nk, N)
+        k = _planes_to_complex(re, im, (n, nk, N))
         return ([k[i] for i in range(n)], list(sc.reshape(n, nk)), list(ev.reshape(n, nk)),
                 [int(x) for x in it])
 
