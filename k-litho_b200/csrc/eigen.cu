@@ -487,8 +487,8 @@ struct ClusterSmem {
     npairs = Bp / 2;
     rows = 0;                                                      // 3 slots x g rows x B
     rot = sizeof(double2) * 3 * (size_t)g * B;                     // kClRotBufs x npairs double4
-    pq = rot + sizeof(double4) * kClRotBufs * npairs;              // kClRotBufs x npairs uchar2
-    w = (pq + sizeof(uchar2) * kClRotBufs * npairs + 15) & ~size_t(15);  // 2g x 2g double2
+    pq = rot + sizeof(double4) * kClRotBufs * npairs;              // kClRotBufs x npairs (p | q << 16)
+    w = (pq + sizeof(uint32_t) * kClRotBufs * npairs + 15) & ~size_t(15);  // 2g x 2g double2
     r0 = w + sizeof(double2) * 4 * (size_t)g * g;                  // (2g - 1) x g uchar2
     part = (r0 + sizeof(uchar2) * (2 * g - 1) * g + 15) & ~size_t(15);  // kCl x 2 double
     diag = part + sizeof(double) * 2 * kCl;                        // Bp double (rank 0)
@@ -534,12 +534,34 @@ __device__ __forceinline__ void rot_cols(double2& vp, double2& vq, double4 u) {
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-// relaxed arrive on the barrier at the same offset in CTA `cta` (the caller
-// orders its earlier stores with fence.acq_rel.cluster)
-__device__ __forceinline__ void mbar_arrive_relaxed(uint64_t* bar, uint32_t cta) {
-  uint32_t remote;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(remote) : "r"(smem_u32(bar)), "r"(cta));
-  asm volatile("mbarrier.arrive.relaxed.cluster.shared::cluster.b64 _, [%0];" ::"r"(remote) : "memory");
+// address of `p`'s counterpart in the shared memory of CTA `cta` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(const void* p, uint32_t cta) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(p)), "r"(cta));
+  return r;
+}
+// bytes one step's rotations deliver to every CTA: npairs x (double4 + packed pair)
+__host__ __device__ inline uint32_t cluster_step_bytes(int npairs) {
+  return (uint32_t)npairs * (uint32_t)(sizeof(double4) + sizeof(uint32_t));
+}
+// rotation t (and its pair p | q << 16) into slot (rbuf, pbuf) of CTA `cta`;
+// each store completes its bytes on that CTA's barrier `bar`
+__device__ __forceinline__ void push_rotation(double4* rbuf, uint32_t* pbuf, uint64_t* bar, int t, double4 u,
+                                              uint32_t pq, uint32_t cta) {
+  const uint32_t rr = cluster_addr(&rbuf[t], cta), rp = cluster_addr(&pbuf[t], cta), rbar = cluster_addr(bar, cta);
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(rr),
+               "d"(u.x), "d"(u.y), "r"(rbar)
+               : "memory");
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(rr + 16),
+               "d"(u.z), "d"(u.w), "r"(rbar)
+               : "memory");
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];" ::"r"(rp), "r"(pq),
+               "r"(rbar)
+               : "memory");
+}
+// this CTA expects `bytes` on its barrier in the barrier's current phase
+__device__ __forceinline__ void mbar_arm(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
 __device__ __forceinline__ bool mbar_try_cluster(uint64_t* bar, uint32_t parity) {
   uint32_t ok;
@@ -577,7 +599,7 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
   const int slot_elems = g * B;
   double2* slots = reinterpret_cast<double2*>(csm + L.rows);
   double4* rotx = reinterpret_cast<double4*>(csm + L.rot);
-  uchar2* pqx = reinterpret_cast<uchar2*>(csm + L.pq);
+  uint32_t* pqx = reinterpret_cast<uint32_t*>(csm + L.pq);
   double2* W = reinterpret_cast<double2*>(csm + L.w);
   uchar2* r0 = reinterpret_cast<uchar2*>(csm + L.r0);
   double* part = reinterpret_cast<double*>(csm + L.part);
@@ -588,15 +610,17 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
   __shared__ double s_newdiag[2 * kClMaxG];  // diagonal at local position l after the last rotations
   __shared__ int s_pairof[2 * kClMaxG];      // own pair holding local position l (+256: second index)
   __shared__ double s_red[2][kClThreads / 32];
-  // rotation slot b is complete when every CTA's g rotation lanes have arrived
+  // rotation slot b: its phase completes when the step's rotations from every
+  // CTA have landed (st.async completes their bytes; this CTA arms each use)
   __shared__ __align__(8) uint64_t s_bar[kClRotBufs];
   __shared__ int s_fail, s_anyfail;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nthr = blockDim.x;
   const double2 zero = make_double2(0.0, 0.0), one = make_double2(1.0, 0.0);
   if (tid == 0) {
     for (int b = 0; b < kClRotBufs; ++b)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_bar[b])), "r"(g * kCl) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&s_bar[b])), "r"(1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int b = 0; b < kClRotBufs; ++b) mbar_arm(&s_bar[b], cluster_step_bytes(npairs));
     s_fail = 0;
     s_anyfail = 0;
   }
@@ -666,11 +690,11 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
     for (int k = 0; k < nk; ++k, ++nsteps) {
       const int par = nsteps & 1, bsel = nsteps % kClRotBufs, bnext = bsel + 1 == kClRotBufs ? 0 : bsel + 1;
       double4* rb = rotx + bsel * npairs;
-      uchar2* pb = pqx + bsel * npairs;
+      uint32_t* pb = pqx + bsel * npairs;
       const int4* own = s_own[par];
       // rotation warp: lane L handles own pair j = L % 16 and pushes it to CTAs
-      // 4 (L / 16) .. 4 (L / 16) + 3 (every slot entry has one writer that
-      // arrives once on the receiving CTA's barrier: g kCl arrivals a step)
+      // 4 (L / 16) .. 4 (L / 16) + 3 (every slot entry has one writer; the
+      // receiving barrier counts the bytes of all npairs entries)
       const int j = lane & 15, c0 = (lane >> 4) * (kCl / 2);
       const bool rlane = warp == rwarp && j < g;
       // before the wait: the step's own rotations at a round start, then the
@@ -701,12 +725,8 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
             if (q < B) s_newdiag[lq] = nd;
             s_own[par][j] = make_int4(op, q < B ? oq : -1, lp, lq);
           }
-          for (int c = c0; c < c0 + kCl / 2; ++c) {
-            cl.map_shared_rank(rb, c)[e * g + j] = u;
-            cl.map_shared_rank(pb, c)[e * g + j] = make_uchar2((unsigned char)p, (unsigned char)q);
-          }
-          asm volatile("fence.acq_rel.cluster;" ::: "memory");
-          for (int c = c0; c < c0 + kCl / 2; ++c) mbar_arrive_relaxed(&s_bar[bsel], c);
+          for (int c = c0; c < c0 + kCl / 2; ++c)
+            push_rotation(rb, pb, &s_bar[bsel], e * g + j, u, (uint32_t)p | (uint32_t)q << 16, c);
         }
         __syncwarp();
         if (k + 1 < nk) {
@@ -739,9 +759,14 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
       // after one timeout the CTA stops waiting, finishes quickly and reports it
       if (!*(volatile int*)&s_fail && !mbar_wait_cluster(&s_bar[bsel], (uint32_t)((nsteps / kClRotBufs) & 1)))
         s_fail = 1;
-      if (warp != rwarp) {
-        // W <- W U over the own pairs (row r, columns lp and lq; W is kept
-        // column-major so that consecutive rows are consecutive words)
+      // the slot's next use (three steps on) is armed before this CTA's next
+      // rotations leave, so no sender can complete bytes of an unarmed phase
+      if (tid == 0) mbar_arm(&s_bar[bsel], cluster_step_bytes(npairs));
+      // W <- W U over the own pairs (row r, columns lp and lq; W is kept
+      // column-major so that consecutive rows are consecutive words).  The own
+      // pairs of a round's first step are written by the rotation warp just
+      // before the barrier below; later steps' were written a step earlier.
+      auto update_w = [&]() {
         for (int i = tid; i < g * g2; i += kClUpdThreads) {
           const int jj = i / g2, r = i - jj * g2;
           const int4 o = own[jj];
@@ -750,8 +775,10 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
           W[o.z * g2 + r] = vp;
           W[o.w * g2 + r] = vq;
         }
-      }
-      // the rotation warp has read its entries of H: the update may begin
+      };
+      if (warp != rwarp && k > 0) update_w();
+      // the rotation warp has read its entries of H (and, at a round start,
+      // written the step's own pairs): the update may begin
       asm volatile("bar.sync 1, %0;" ::"r"(kClThreads) : "memory");
       if (warp == rwarp) {
         if (k + 1 < nk && rlane) {
@@ -780,18 +807,17 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
             s_own[par ^ 1][j] = make_int4(opn, qn < B ? oqn : -1, lpn, lqn);
           }
           double4* rn = rotx + bnext * npairs;
-          uchar2* pn_ = pqx + bnext * npairs;
-          for (int c = c0; c < c0 + kCl / 2; ++c) {
-            cl.map_shared_rank(rn, c)[e * g + j] = u;
-            cl.map_shared_rank(pn_, c)[e * g + j] = make_uchar2((unsigned char)pn, (unsigned char)qn);
-          }
-          asm volatile("fence.acq_rel.cluster;" ::: "memory");
-          for (int c = c0; c < c0 + kCl / 2; ++c) mbar_arrive_relaxed(&s_bar[bnext], c);
+          uint32_t* pn_ = pqx + bnext * npairs;
+          for (int c = c0; c < c0 + kCl / 2; ++c)
+            push_rotation(rn, pn_, &s_bar[bnext], e * g + j, u, (uint32_t)pn | (uint32_t)qn << 16, c);
         }
-      } else if (jg < ngrp) {
+      } else if (k == 0) {
+        update_w();
+      }
+      if (warp != rwarp && jg < ngrp) {
         // U_j^H H[rows of own pair j, columns of pair t2] U_t2
-        const uchar2 pc = pb[t2];
-        const int p2 = pc.x, q2 = pc.y;
+        const uint32_t pc = pb[t2];
+        const int p2 = (int)(pc & 0xffffu), q2 = (int)(pc >> 16);
         const bool cq = q2 < B;
         const double4 u2 = rb[t2];
         if (p2 < B)
