@@ -10,6 +10,8 @@
 #include <cooperative_groups.h>
 #include <cuda_pipeline.h>
 
+#include <mutex>
+
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -1109,9 +1111,19 @@ bool jacobi_h_in_smem(int B) { return JacobiSmem(B).total_no_h + sizeof(double2)
 // from about 64 up); otherwise k_jacobi keeps H in shared memory or works on
 // it in place in global memory
 constexpr int kClusterMinB = 64;
+std::mutex g_cluster_mu;  // guards the per-device answers below (host threads may share the library)
+
 bool jacobi_use_cluster(int B) {
   if (B < kClusterMinB || B > kGramMaxS) return false;
-  static int ok = -1;
+  static std::vector<int> known;  // per device: -1 unknown, 0 no, 1 yes
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  std::lock_guard<std::mutex> lock(g_cluster_mu);
+  if ((int)known.size() <= dev) known.resize(dev + 1, -1);
+  int& ok = known[dev];
   if (ok < 0) {
     ok = 0;
     const size_t sm = ClusterSmem(kGramMaxS).total;
@@ -1206,14 +1218,16 @@ std::vector<uint32_t> cluster_schedule() {
 // uploads c_cluster_sched once per device, ordered before work later queued on st
 int ensure_cluster_schedule(cudaStream_t st) {
   static const std::vector<uint32_t> tab = cluster_schedule();
-  static bool done[64] = {};
+  static std::vector<char> done;  // per device
   int dev = 0;
   KL_CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 64 && done[dev]) return KL_OK;
+  std::lock_guard<std::mutex> lock(g_cluster_mu);
+  if ((int)done.size() > dev && done[dev]) return KL_OK;
   KL_CUDA_TRY(cudaMemcpyToSymbolAsync(c_cluster_sched, tab.data(), sizeof(uint32_t) * tab.size(), 0,
                                       cudaMemcpyHostToDevice, st));
   KL_CUDA_TRY(cudaStreamSynchronize(st));
-  if (dev < 64) done[dev] = true;
+  if ((int)done.size() <= dev) done.resize(dev + 1, 0);
+  done[dev] = 1;
   return KL_OK;
 }
 
