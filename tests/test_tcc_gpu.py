@@ -237,3 +237,39 @@ def test_topk_batch_rejects_mixed_band(cuda):
     b = K.TccPlan(src, 1.35, 0.0, 1024, 1024, n_medium=1.44)
     with pytest.raises(RuntimeError, match="same N"):
         K.TccPlan.topk_batch([a, b], 8)
+
+
+def custom_source(S, size=41, seed=0):
+    """A source map of exactly S points (uniform weights) inside 0.9 of the pupil radius."""
+    rng = np.random.default_rng(seed)
+    sh = (size - 1) // 2
+    cand = [(p, q) for q in range(-sh, sh + 1) for p in range(-sh, sh + 1) if p * p + q * q <= (0.9 * sh) ** 2]
+    pick = rng.choice(len(cand), size=S, replace=False)
+    src = np.zeros((size, size), dtype=np.float32)
+    for i in pick:
+        p, q = cand[i]
+        src[q + sh, p + sh] = 1.0 / S
+    return src
+
+
+@pytest.mark.parametrize("S", [63, 64, 250])
+def test_topk_gram_size_boundaries(cuda, S):
+    # Gram orders at the solver's boundaries: 63 (one CTA), 64 (the smallest
+    # cluster, 4 indices per group) and 250 (padded to 256: 16 per group, the
+    # largest cluster layout, with padding indices)
+    L, nk = 1024, 24
+    src = custom_source(S, seed=S)
+    sig = O.outer_sigma(src)
+    assert O.source_point_count(src, sig) == S
+    Nx, Ny = O.band(1.35, L, L, sig)
+    plan = K.TccPlan(src, 1.35, synth.defocus_arg(15.0), L, L, n_medium=1.44)
+    assert plan.S == S
+    krn, sc, ev, it = plan.topk(nk)
+    tcc = O.calc_tcc(src, sig, 1.35, synth.defocus_arg(15.0), L, L, Nx, Ny, n_medium=1.44)
+    kr, _, er = O.calc_kernels(tcc, nk)
+    assert np.abs(ev - er).max() <= 1e-6 * np.abs(er).max(), it
+    assert eig_residual(krn, ev, tcc) <= 1e-4
+    n = gap_cut(np.linalg.eigvalsh(tcc)[::-1], nk)
+    Pr = weighted_projector(kr[:n], er[:n])
+    assert np.linalg.norm(weighted_projector(krn[:n], ev[:n]) - Pr) / np.linalg.norm(Pr) <= 1e-5
+    assert 0 < it < 40
