@@ -7,16 +7,18 @@
 // 3-term BF16 split (hi*hi + hi*lo + lo*hi), FP32 accumulation in TMEM:
 //     TCC_re = [Ar Ai](hi,hi,lo) . [Ar Ai](hi,lo,hi)^T
 //     TCC_im = [Ai -Ar](hi,hi,lo) . [Ar Ai](hi,lo,hi)^T
-// One CTA per 128 x 128 upper tile: a TMA producer thread streams 128 x 64
-// bf16 tiles (128-byte swizzle) through a 4-stage mbarrier pipeline, one
-// thread issues tcgen05.mma into two TMEM accumulators (re, im), and four
-// warps drain TMEM with tcgen05.ld, writing the tile and its conjugate
-// transpose (coalesced) so the result is exactly Hermitian.
+// 128 x 128 upper tiles on persistent CTAs (one per SM): a TMA producer
+// thread streams 128 x 64 bf16 tiles (128-byte swizzle) through a 4-stage
+// mbarrier pipeline, one thread issues tcgen05.mma into one of two TMEM
+// accumulator sets (each re, im), and four warps drain the other set with
+// tcgen05.ld, writing the tile and its conjugate transpose (coalesced) so the
+// result is exactly Hermitian.
 // FP64 path: the same sum accumulated in FP64 on the CUDA cores from the
 // reference-identical pupil table.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -176,11 +178,9 @@ int tcc_split_operands(const float2* A, int N, int S, int Kp, void* X1, void* X2
 // tcgen05 Hermitian GEMM
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int TM = 128, TN = 128, TK = 64, STAGES = 2;  // 2 CTAs per SM: one's epilogue overlaps the other's MMAs
+constexpr int TM = 128, TN = 128, TK = 64;
 constexpr int TILE_BYTES = TM * TK * 2;         // 16 KB, one 128 x 64 bf16 tile
 constexpr int STAGE_BYTES = 3 * TILE_BYTES;     // X1, X2, Y
-constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 + 256;
-constexpr uint32_t TMEM_COLS = 256;             // re: [0,128), im: [128,256)
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s bound on any pipeline wait
 
 // instruction descriptor: dense, f32 accumulate, bf16 A/B, both K-major, M=128, N=128
@@ -201,6 +201,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   uint32_t ok;
@@ -263,38 +266,85 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
 }
 }  // namespace
 
-__global__ void __launch_bounds__(128, 2)
-    k_tcc_gemm(const __grid_constant__ CUtensorMap tmX1, const __grid_constant__ CUtensorMap tmX2,
-               const __grid_constant__ CUtensorMap tmY, int N, int nkb, int nt,
-               float2* __restrict__ tcc, int* __restrict__ err) {
-  extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint64_t* empty = full + STAGES;
-  uint64_t* done = empty + STAGES;
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// Persistent, warp-specialised: one CTA per SM walks the upper tiles
+// blockIdx.x, blockIdx.x + gridDim.x, ...  Warp 0 (one thread) streams the
+// operand tiles through kStages shared-memory stages with TMA; warp 1 (one
+// thread) issues the MMAs of a tile into one of two TMEM accumulator sets
+// while warps 2..5 drain the other set (tcgen05.ld, then the tile and its
+// conjugate transpose to global memory through their own staging buffers), so
+// loads, MMAs and stores of consecutive tiles overlap.  Every wait is bounded:
+// a timeout records `err`, raises the CTA's abort flag and every role stops.
+namespace {
+constexpr int kStages = 4;
+constexpr int kEpiWarps = 4;
+constexpr int kGemmThreads = 32 * (2 + kEpiWarps);
+constexpr int EPI_BYTES = kEpiWarps * 32 * 33 * 8;  // per epilogue warp a 32 x 33 float2 tile
+constexpr int PSMEM_BYTES = kStages * STAGE_BYTES + EPI_BYTES + 1024 + 256;
+constexpr uint32_t PTMEM_COLS = 512;  // two accumulator sets of (re 128 | im 128)
 
-  // upper-triangular tile (ib <= jb) of this CTA
-  int t = blockIdx.x, ib = 0, rowlen = nt;
+// bounded wait that also gives up when another role has aborted
+__device__ __forceinline__ bool mbar_wait_ab(uint32_t bar, uint32_t parity, int* err, int code,
+                                             volatile int* abort) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = now_ns();
+  while (true) {
+    if (mbar_try(bar, parity)) return true;
+    if (*abort) return false;
+    if (now_ns() - t0 > WAIT_NS) {
+      atomicExch(err, code);
+      *abort = 1;
+      return false;
+    }
+    __nanosleep(64);
+  }
+}
+
+__device__ __forceinline__ void upper_tile(int t, int nt, int& ib, int& jb) {
+  int rowlen = nt;
+  ib = 0;
   while (t >= rowlen) {
     t -= rowlen;
     ++ib;
     --rowlen;
   }
-  const int jb = ib + t;
+  jb = ib + t;
+}
+}  // namespace
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    k_tcc_gemm(const __grid_constant__ CUtensorMap tmX1, const __grid_constant__ CUtensorMap tmX2,
+               const __grid_constant__ CUtensorMap tmY, int N, int nkb, int nt,
+               float2* __restrict__ tcc, int* __restrict__ err) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  float2* epi = reinterpret_cast<float2*>(smem + kStages * STAGE_BYTES);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kStages * STAGE_BYTES + EPI_BYTES);
+  uint64_t* empty = full + kStages;
+  uint64_t* tfull = empty + kStages;   // accumulator set ready for the epilogue
+  uint64_t* tempty = tfull + 2;        // accumulator set drained
+  uint64_t* drain = tempty + 2;        // the MMA thread's last MMAs (abort path)
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  __shared__ int s_abort;
+  volatile int* abort = &s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tiles = nt * (nt + 1) / 2;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < kStages; ++s) {
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    mbar_init(smem_u32(done), 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(smem_u32(&tfull[a]), 1);
+      mbar_init(smem_u32(&tempty[a]), kEpiWarps);
+    }
+    mbar_init(smem_u32(drain), 1);
+    s_abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(TMEM_COLS)
+                 "r"(PTMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -303,100 +353,119 @@ __global__ void __launch_bounds__(128, 2)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
 
-  if (threadIdx.x == 0) {
-    // TMA producer
-    int armed[STAGES];
-    for (int s = 0; s < STAGES; ++s) armed[s] = -1;
+  if (warp == 0 && lane == 0) {
+    // TMA producer: k-block `it` of the CTA's run goes to stage it % kStages
+    int armed[kStages];
+    for (int s = 0; s < kStages; ++s) armed[s] = -1;
     bool ok = true;
-    for (int kb = 0; kb < nkb && ok; ++kb) {
-      const int s = kb % STAGES, use = kb / STAGES;
-      if (use > 0) ok = mbar_wait(smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 1);
-      if (!ok) break;
-      const uint32_t bar = smem_u32(&full[s]);
-      mbar_expect_tx(bar, STAGE_BYTES);
-      uint8_t* st = smem + s * STAGE_BYTES;
-      tma_load_2d(smem_u32(st), &tmX1, kb * TK, ib * TM, bar);
-      tma_load_2d(smem_u32(st + TILE_BYTES), &tmX2, kb * TK, ib * TM, bar);
-      tma_load_2d(smem_u32(st + 2 * TILE_BYTES), &tmY, kb * TK, jb * TN, bar);
-      armed[s] = use;
-    }
-    if (!ok) {
-      // let copies already issued land before the CTA can retire
-      for (int s = 0; s < STAGES; ++s)
-        if (armed[s] >= 0) mbar_wait(smem_u32(&full[s]), (uint32_t)(armed[s] & 1), err, 4);
-    }
-  } else if (threadIdx.x == 32) {
-    // MMA issuer
-    bool ok = true;
-    for (int kb = 0; kb < nkb && ok; ++kb) {
-      const int s = kb % STAGES, use = kb / STAGES;
-      ok = mbar_wait(smem_u32(&full[s]), (uint32_t)(use & 1), err, 2);
-      if (!ok) break;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const uint32_t a1 = smem_u32(smem + s * STAGE_BYTES);
-      const uint32_t a2 = a1 + TILE_BYTES, b = a1 + 2 * TILE_BYTES;
-#pragma unroll
-      for (int k = 0; k < TK / 16; ++k) {
-        const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
-        const uint32_t off = (uint32_t)(k * 32);  // 16 bf16 along K inside the swizzle atom
-        mma_bf16(tmem, smem_desc(a1 + off), smem_desc(b + off), acc);
-        mma_bf16(tmem + 128, smem_desc(a2 + off), smem_desc(b + off), acc);
+    int it = 0;
+    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+      int ib, jb;
+      upper_tile(t, nt, ib, jb);
+      for (int kb = 0; kb < nkb; ++kb, ++it) {
+        const int s = it % kStages, use = it / kStages;
+        if (use > 0 && !(ok = mbar_wait_ab(smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 1, abort))) break;
+        const uint32_t bar = smem_u32(&full[s]);
+        mbar_expect_tx(bar, STAGE_BYTES);
+        uint8_t* st = smem + s * STAGE_BYTES;
+        tma_load_2d(smem_u32(st), &tmX1, kb * TK, ib * TM, bar);
+        tma_load_2d(smem_u32(st + TILE_BYTES), &tmX2, kb * TK, ib * TM, bar);
+        tma_load_2d(smem_u32(st + 2 * TILE_BYTES), &tmY, kb * TK, jb * TN, bar);
+        armed[s] = use;
       }
-      mma_commit(smem_u32(&empty[s]));
     }
-    mma_commit(smem_u32(done));
-  }
-  __syncwarp();
-
-  // epilogue: four warps, warp w owns TMEM lanes (tile rows) [32w, 32w+32)
-  const bool ready = mbar_wait(smem_u32(done), 0u, err, 3);
-  __syncwarp();
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (ready) {
-    const int r = warp * 32 + lane;
-    const int i = ib * TM + r;
-    const bool diag = ib == jb;
-#pragma unroll 1
-    for (int c0 = 0; c0 < TN; c0 += 32) {
-      uint32_t re[32], im[32];
-      const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16);
-      tmem_ld32(base + (uint32_t)c0, re);
-      tmem_ld32(base + 128u + (uint32_t)c0, im);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      // direct tile: the warp's 32 x 32 block goes through shared memory (the
-      // pipeline stages are free once `done` has fired) so that each store
-      // writes 32 consecutive columns of one row
-      float2* stage = reinterpret_cast<float2*>(smem) + warp * 32 * 33;
+    // every issued copy lands before the CTA can retire (its stage parity is known)
+    for (int s = 0; s < kStages; ++s)
+      if (armed[s] >= 0) mbar_wait(smem_u32(&full[s]), (uint32_t)(armed[s] & 1), err, 4);
+  } else if (warp == 1 && lane == 0) {
+    // MMA issuer: tile number `tl` of the run accumulates into set tl & 1
+    bool ok = true;
+    int it = 0, tl = 0;
+    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x, ++tl) {
+      const int a = tl & 1, ause = tl >> 1;
+      if (ause > 0 && !(ok = mbar_wait_ab(smem_u32(&tempty[a]), (uint32_t)((ause - 1) & 1), err, 5, abort))) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t acc = tmem + (uint32_t)(a * 256);
+      for (int kb = 0; kb < nkb; ++kb, ++it) {
+        const int s = it % kStages, use = it / kStages;
+        if (!(ok = mbar_wait_ab(smem_u32(&full[s]), (uint32_t)(use & 1), err, 2, abort))) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t a1 = smem_u32(smem + s * STAGE_BYTES);
+        const uint32_t a2 = a1 + TILE_BYTES, b = a1 + 2 * TILE_BYTES;
 #pragma unroll
-      for (int c = 0; c < 32; ++c) stage[lane * 33 + c] = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
+        for (int k = 0; k < TK / 16; ++k) {
+          const uint32_t accum = (kb > 0 || k > 0) ? 1u : 0u;
+          const uint32_t off = (uint32_t)(k * 32);  // 16 bf16 along K inside the swizzle atom
+          mma_bf16(acc, smem_desc(a1 + off), smem_desc(b + off), accum);
+          mma_bf16(acc + 128, smem_desc(a2 + off), smem_desc(b + off), accum);
+        }
+        mma_commit(smem_u32(&empty[s]));
+      }
+      if (ok) mma_commit(smem_u32(&tfull[a]));
+    }
+    // the MMAs issued so far complete before TMEM can be released
+    mma_commit(smem_u32(drain));
+    mbar_wait(smem_u32(drain), 0u, err, 6);
+  } else if (warp >= 2) {
+    // epilogue: warp w drains TMEM lanes (tile rows) 32 (w % 4) .. + 31
+    const int q = warp & 3;
+    float2* stage = epi + (warp - 2) * 32 * 33;
+    int tl = 0;
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++tl) {
+      const int a = tl & 1, ause = tl >> 1;
+      const bool ready = mbar_wait_ab(smem_u32(&tfull[a]), (uint32_t)(ause & 1), err, 3, abort);
       __syncwarp();
-      {
-        const int j = jb * TN + c0 + lane;
+      if (!__all_sync(0xffffffffu, ready)) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      int ib, jb;
+      upper_tile(t, nt, ib, jb);
+      const int r = q * 32 + lane;
+      const int i = ib * TM + r;
+      const bool diag = ib == jb;
+      const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * 256);
+#pragma unroll 1
+      for (int c0 = 0; c0 < TN; c0 += 32) {
+        uint32_t re[32], im[32];
+        tmem_ld32(base + (uint32_t)c0, re);
+        tmem_ld32(base + 128u + (uint32_t)c0, im);
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        // the warp's 32 x 32 block goes through its staging buffer so that each
+        // store writes 32 consecutive columns of one row
+#pragma unroll
+        for (int c = 0; c < 32; ++c) stage[lane * 33 + c] = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
+        __syncwarp();
+        {
+          const int j = jb * TN + c0 + lane;
 #pragma unroll 4
-        for (int rr = 0; rr < 32; ++rr) {
-          const int row = warp * 32 + rr, ii = ib * TM + row;
-          if (ii < N && j < N && (!diag || c0 + lane >= row)) {
-            float2 v = stage[rr * 33 + lane];
-            if (diag && c0 + lane == row) v.y = 0.f;
-            tcc[(size_t)ii * N + j] = v;
+          for (int rr = 0; rr < 32; ++rr) {
+            const int row = q * 32 + rr, ii = ib * TM + row;
+            if (ii < N && j < N && (!diag || c0 + lane >= row)) {
+              float2 v = stage[rr * 33 + lane];
+              if (diag && c0 + lane == row) v.y = 0.f;
+              tcc[(size_t)ii * N + j] = v;
+            }
           }
         }
-      }
-      __syncwarp();
-      // conjugate transpose: tcc[j][i], consecutive lanes write consecutive i
+        __syncwarp();
+        // conjugate transpose: tcc[j][i], consecutive lanes write consecutive i
 #pragma unroll
-      for (int c = 0; c < 32; ++c) {
-        const int j = jb * TN + c0 + c;
-        if (j < N && i < N && (!diag || c0 + c > r))
-          tcc[(size_t)j * N + i] = make_float2(__uint_as_float(re[c]), -__uint_as_float(im[c]));
+        for (int c = 0; c < 32; ++c) {
+          const int j = jb * TN + c0 + c;
+          if (j < N && i < N && (!diag || c0 + c > r))
+            tcc[(size_t)j * N + i] = make_float2(__uint_as_float(re[c]), -__uint_as_float(im[c]));
+        }
       }
+      // this set's TMEM is read: the MMAs of tile tl + 2 may overwrite it
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&tempty[a]));
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(PTMEM_COLS)
                  : "memory");
   }
 }
@@ -449,8 +518,12 @@ int tcc_gemm_tc(const void* X1, const void* X2, const void* Y, int N, int Kp, fl
   if ((rc = make_map(&m1, X1, N, Kp)) || (rc = make_map(&m2, X2, N, Kp)) || (rc = make_map(&my, Y, N, Kp))) return rc;
   const int nt = (N + TM - 1) / TM;
   const int tiles = nt * (nt + 1) / 2;
-  KL_CUDA_TRY(cudaFuncSetAttribute(k_tcc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-  k_tcc_gemm<<<tiles, 128, SMEM_BYTES, st>>>(m1, m2, my, N, Kp / TK, nt, tcc, err_dev);
+  int dev = 0, sms = 0;
+  KL_CUDA_TRY(cudaGetDevice(&dev));
+  KL_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  KL_CUDA_TRY(cudaFuncSetAttribute(k_tcc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, PSMEM_BYTES));
+  k_tcc_gemm<<<std::min(tiles, std::max(1, sms)), kGemmThreads, PSMEM_BYTES, st>>>(m1, m2, my, N, Kp / TK, nt, tcc,
+                                                                                    err_dev);
   KL_CUDA_TRY(cudaGetLastError());
   return KL_OK;
 }
