@@ -6,7 +6,9 @@
 // A (A^H X) at cost 2 N S B) or a materialised TCC (N^2 B).  All block
 // arithmetic is complex FP64 on the CUDA cores; products of the FP32 factor
 // are formed exactly in FP64.  The B x B problems (Cholesky, triangular
-// inverse, Hermitian eigensolve by cyclic Jacobi) run in one CTA each.
+// inverse, Hermitian eigensolve by cyclic Jacobi) run in one CTA each, except
+// Jacobi eigensolves of order 64..256, which run on a thread-block cluster of
+// eight CTAs holding the matrix in their shared memory (k_jacobi_cluster).
 #include <cooperative_groups.h>
 #include <cuda_pipeline.h>
 
