@@ -928,20 +928,23 @@ constexpr int kVbRows = 2;
 constexpr int kVbThreads = 256;
 constexpr int kVbItems = (kVbRows * kCl * 2 * kClMaxG + kVbThreads - 1) / kVbThreads;
 
-size_t jacobi_vectors_blocks_smem(int B) {
+// shared memory of k_jacobi_vectors_blocks with nbuf staging buffers for the round's blocks
+size_t jacobi_vectors_blocks_smem(int B, int nbuf) {
   const int Bp = jacobi_cluster_bp(B), g2 = Bp / kCl;
-  return sizeof(double2) * ((size_t)kCl * g2 * g2 + (size_t)kVbRows * Bp) + sizeof(int) * kCl * g2;
+  return sizeof(double2) * ((size_t)nbuf * kCl * g2 * g2 + (size_t)kVbRows * Bp) + sizeof(int) * kCl * g2;
 }
+// two buffers (the next round's blocks load while this round's are applied) when they fit
+int jacobi_vectors_blocks_nbuf(int B) { return jacobi_vectors_blocks_smem(B, 2) <= 220 * 1024 ? 2 : 1; }
 
-__global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs jobs) {
+__global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs jobs, int nbuf) {
   extern __shared__ __align__(16) unsigned char vsm[];
   const JacobiJob job = jobs.j[blockIdx.y];
   const int B = job.B, Bp = jacobi_cluster_bp(B), g = Bp / (2 * kCl), g2 = 2 * g, ngroups = 2 * kCl;
   const int k0 = blockIdx.x * kVbRows;
   if (k0 >= B) return;  // uniform over the CTA
   const int bsz = g2 * g2;
-  double2* Wsm = reinterpret_cast<double2*>(vsm);  // kCl blocks of the round
-  double2* rows = Wsm + kCl * bsz;                  // kVbRows x Bp
+  double2* Wsm = reinterpret_cast<double2*>(vsm);  // nbuf x kCl blocks of a round
+  double2* rows = Wsm + nbuf * kCl * bsz;           // kVbRows x Bp
   int* idx = reinterpret_cast<int*>(rows + kVbRows * Bp);  // kCl x 2g logical index of each block position
   const double2* __restrict__ wlog = reinterpret_cast<const double2*>(job.rot);
   for (int i = threadIdx.x; i < kVbRows * Bp; i += blockDim.x) {
@@ -950,20 +953,31 @@ __global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs
   }
   const int rounds = job.jst[0] / (Bp - 1) * (ngroups - 1);
   const int items = kVbRows * kCl * g2;
+  auto stage = [&](int rd) {  // the round's blocks into buffer rd % nbuf
+    const double2* src = wlog + (size_t)rd * kCl * bsz;
+    double2* dst = Wsm + (rd % nbuf) * kCl * bsz;
+    for (int i = threadIdx.x; i < kCl * bsz; i += blockDim.x) __pipeline_memcpy_async(dst + i, src + i, sizeof(double2));
+    __pipeline_commit();
+  };
+  if (rounds > 0) stage(0);
   for (int rd = 0; rd < rounds; ++rd) {
     const int r = rd % (ngroups - 1);
-    __syncthreads();  // the previous round's rows are written
-    const double2* src = wlog + (size_t)rd * kCl * bsz;
-    for (int i = threadIdx.x; i < kCl * bsz; i += blockDim.x) __pipeline_memcpy_async(Wsm + i, src + i, sizeof(double2));
-    __pipeline_commit();
+    __syncthreads();  // the previous round's rows and idx are written, its buffer is free
+    if (nbuf > 1 && rd + 1 < rounds) {
+      stage(rd + 1);
+      __pipeline_wait_prior(1);  // this round's blocks have landed
+    } else {
+      if (nbuf == 1 && rd > 0) stage(rd);
+      __pipeline_wait_prior(0);
+    }
     for (int i = threadIdx.x; i < kCl * g2; i += blockDim.x) {
       const int e = i / g2, l = i - e * g2;
       int ga, gb;
       jacobi_pair(r, e, ngroups, ga, gb);
       idx[i] = cluster_index(l, ga, gb, g);
     }
-    __pipeline_wait_prior(0);
     __syncthreads();
+    const double2* Wr = Wsm + (rd % nbuf) * kCl * bsz;
     double2 y[kVbItems];
 #pragma unroll
     for (int it = 0; it < kVbItems; ++it) {
@@ -973,7 +987,7 @@ __global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs
         const int m = item % g2, e = (item / g2) % kCl, rr = item / (g2 * kCl);
         const double2* x = rows + rr * Bp;
         const int* ix = idx + e * g2;
-        const double2* w = Wsm + e * bsz + m;
+        const double2* w = Wr + e * bsz + m;
         double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
         for (int l = 0; l < g2; l += 2) {
           a0 = zfma(x[ix[l]], w[l * g2], a0);
@@ -1279,9 +1293,10 @@ int jacobi_batch(const std::vector<JacobiJob>& all, cudaStream_t st) {
         KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_cluster, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_jacobi_cluster<<<nj * kCl, kClThreads, sm, st>>>(jobs, kJacobiMaxSweeps);
         KL_CUDA_TRY(cudaGetLastError());
-        const size_t vsm = jacobi_vectors_blocks_smem(bmax);
+        const int nbuf = jacobi_vectors_blocks_nbuf(bmax);
+        const size_t vsm = jacobi_vectors_blocks_smem(bmax, nbuf);
         KL_CUDA_TRY(cudaFuncSetAttribute(k_jacobi_vectors_blocks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm));
-        k_jacobi_vectors_blocks<<<dim3((bmax + kVbRows - 1) / kVbRows, nj), kVbThreads, vsm, st>>>(jobs);
+        k_jacobi_vectors_blocks<<<dim3((bmax + kVbRows - 1) / kVbRows, nj), kVbThreads, vsm, st>>>(jobs, nbuf);
         KL_CUDA_TRY(cudaGetLastError());
         continue;
       }
