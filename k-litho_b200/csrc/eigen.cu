@@ -931,7 +931,7 @@ constexpr int kVbItems = (kVbRows * kCl * 2 * kClMaxG + kVbThreads - 1) / kVbThr
 // shared memory of k_jacobi_vectors_blocks with nbuf staging buffers for the round's blocks
 size_t jacobi_vectors_blocks_smem(int B, int nbuf) {
   const int Bp = jacobi_cluster_bp(B), g2 = Bp / kCl;
-  return sizeof(double2) * ((size_t)nbuf * kCl * g2 * g2 + (size_t)kVbRows * Bp) + sizeof(int) * kCl * g2;
+  return sizeof(double2) * ((size_t)nbuf * kCl * g2 * g2 + (size_t)kVbRows * Bp + (size_t)kVbRows * kCl * g2);
 }
 // two buffers (the next round's blocks load while this round's are applied) when they fit
 int jacobi_vectors_blocks_nbuf(int B) { return jacobi_vectors_blocks_smem(B, 2) <= 220 * 1024 ? 2 : 1; }
@@ -945,7 +945,7 @@ __global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs
   const int bsz = g2 * g2;
   double2* Wsm = reinterpret_cast<double2*>(vsm);  // nbuf x kCl blocks of a round
   double2* rows = Wsm + nbuf * kCl * bsz;           // kVbRows x Bp
-  int* idx = reinterpret_cast<int*>(rows + kVbRows * Bp);  // kCl x 2g logical index of each block position
+  double2* xg = rows + kVbRows * Bp;                // kVbRows x kCl x 2g: the round's entries of each block
   const double2* __restrict__ wlog = reinterpret_cast<const double2*>(job.rot);
   for (int i = threadIdx.x; i < kVbRows * Bp; i += blockDim.x) {
     const int r = i / Bp, c = i - r * Bp;
@@ -953,6 +953,12 @@ __global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs
   }
   const int rounds = job.jst[0] / (Bp - 1) * (ngroups - 1);
   const int items = kVbRows * kCl * g2;
+  // logical index of position l of block e in round r
+  auto index_of = [&](int r, int e, int l) {
+    int ga, gb;
+    jacobi_pair(r, e, ngroups, ga, gb);
+    return cluster_index(l, ga, gb, g);
+  };
   auto stage = [&](int rd) {  // the round's blocks into buffer rd % nbuf
     const double2* src = wlog + (size_t)rd * kCl * bsz;
     double2* dst = Wsm + (rd % nbuf) * kCl * bsz;
@@ -962,7 +968,7 @@ __global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs
   if (rounds > 0) stage(0);
   for (int rd = 0; rd < rounds; ++rd) {
     const int r = rd % (ngroups - 1);
-    __syncthreads();  // the previous round's rows and idx are written, its buffer is free
+    __syncthreads();  // the previous round's rows are written, its buffer is free
     if (nbuf > 1 && rd + 1 < rounds) {
       stage(rd + 1);
       __pipeline_wait_prior(1);  // this round's blocks have landed
@@ -970,11 +976,10 @@ __global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs
       if (nbuf == 1 && rd > 0) stage(rd);
       __pipeline_wait_prior(0);
     }
-    for (int i = threadIdx.x; i < kCl * g2; i += blockDim.x) {
-      const int e = i / g2, l = i - e * g2;
-      int ga, gb;
-      jacobi_pair(r, e, ngroups, ga, gb);
-      idx[i] = cluster_index(l, ga, gb, g);
+    // each row's entries of each block, gathered contiguously
+    for (int i = threadIdx.x; i < items; i += blockDim.x) {
+      const int l = i % g2, e = (i / g2) % kCl, rr = i / (g2 * kCl);
+      xg[i] = rows[rr * Bp + index_of(r, e, l)];
     }
     __syncthreads();
     const double2* Wr = Wsm + (rd % nbuf) * kCl * bsz;
@@ -985,24 +990,24 @@ __global__ void __launch_bounds__(kVbThreads) k_jacobi_vectors_blocks(JacobiJobs
       y[it] = make_double2(0.0, 0.0);
       if (item < items) {
         const int m = item % g2, e = (item / g2) % kCl, rr = item / (g2 * kCl);
-        const double2* x = rows + rr * Bp;
-        const int* ix = idx + e * g2;
+        const double2* x = xg + (rr * kCl + e) * g2;
         const double2* w = Wr + e * bsz + m;
         double2 a0 = make_double2(0.0, 0.0), a1 = make_double2(0.0, 0.0);
+#pragma unroll 2
         for (int l = 0; l < g2; l += 2) {
-          a0 = zfma(x[ix[l]], w[l * g2], a0);
-          a1 = zfma(x[ix[l + 1]], w[(l + 1) * g2], a1);
+          a0 = zfma(x[l], w[l * g2], a0);
+          a1 = zfma(x[l + 1], w[(l + 1) * g2], a1);
         }
         y[it] = zadd(a0, a1);
       }
     }
-    __syncthreads();
+    // rows are read only by the gather, so each thread writes its outputs back at once
 #pragma unroll
     for (int it = 0; it < kVbItems; ++it) {
       const int item = threadIdx.x + it * kVbThreads;
       if (item < items) {
         const int m = item % g2, e = (item / g2) % kCl, rr = item / (g2 * kCl);
-        rows[rr * Bp + idx[e * g2 + m]] = y[it];
+        rows[rr * Bp + index_of(r, e, m)] = y[it];
       }
     }
   }
