@@ -41,7 +41,7 @@ __device__ __forceinline__ float2 expi2pi_frac(long long num, long long den) {
 }
 
 // ---------------------------------------------------------------------------
-// compile-time twiddles: cos/sin(2*pi*k/64) evaluated by the compiler from a
+// compile-time twiddles: cos/sin(2*pi*k/256) evaluated by the compiler from a
 // Taylor series on the octant-reduced angle, stored in constant memory.
 // ---------------------------------------------------------------------------
 namespace cx {
@@ -87,7 +87,7 @@ constexpr double sin2pi(long k, long n) {
 }
 }  // namespace cx
 
-constexpr int kTwN = 128;
+constexpr int kTwN = 256;
 struct TwTable {
   float c[kTwN];
   float s[kTwN];
@@ -98,14 +98,14 @@ struct TwTable {
     }
   }
 };
-// e^{+2*pi*i*k/128}; other power-of-two lengths use a stride
+// e^{+2*pi*i*k/256}; other power-of-two lengths use a stride
 __constant__ const TwTable c_tw = TwTable();
 
 // the same table in global memory, for lane-dependent indices (the constant
 // cache serialises divergent addresses)
 __device__ const TwTable g_twd = TwTable();
 
-// e^{+2*pi*i*num/den} for den a power of two dividing 128
+// e^{+2*pi*i*num/den} for den a power of two dividing 256
 __device__ __forceinline__ float2 expi2pi_pow2(int num, int den) {
   const int idx = (num & (den - 1)) * (kTwN / den);
   return make_float2(g_twd.c[idx], g_twd.s[idx]);
@@ -250,6 +250,26 @@ struct WarpFFT {
         v[q] = r;
       }
     }
+  }
+  // The transpose of run(): input v[q1] = x[q1 + R * brev5(lane)] (the
+  // layout run() produces), output v[j] = X[lane + 32 j], the same DFT.  The
+  // lane stages run in reverse order as decimation-in-time butterflies
+  // (x + w y, x - w y), then the diagonal twiddle, then the register DFT.
+  __device__ __forceinline__ void run_rev(float2 (&v)[R], int lane) const {
+#pragma unroll
+    for (int s = 4; s >= 0; --s) {
+      const int h = 16 >> s;
+      const bool upper = (lane & h) != 0;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const float2 t = upper ? cmul(v[q], tws[s]) : v[q];
+        const float2 o = make_float2(__shfl_xor_sync(0xffffffffu, t.x, h), __shfl_xor_sync(0xffffffffu, t.y, h));
+        v[q] = upper ? csub(o, t) : cadd(v[q], o);
+      }
+    }
+#pragma unroll
+    for (int q = 1; q < R; ++q) v[q] = cmul(v[q], tw4[q]);
+    if (R > 1) fft_reg<R, SIGN>(v);
   }
 };
 

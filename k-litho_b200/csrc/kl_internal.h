@@ -88,6 +88,65 @@ int socs_launch_inverse(const SocsGeom& g, const float2* tx, const float2* ty, c
 int socs_launch_band(const SocsGeom& g, const float2* partial, int nclips, float2* band,
                      cudaStream_t st);
 
+// ---------------------------------------------------------------------------
+// General-geometry fused SOCS pipeline (socs_gen.cu, socs_gen_vjp.cu): any
+// period Lx x Ly, bands up to 4N+1 <= 256.  Five stream-ordered stages:
+//   row_fwd  mask rows -> row bins R[y][fx], fx in [0, Nx]       (HBM-bound)
+//   col_fwd  R -> band spectrum, |fy| <= Ny                      (small)
+//   spectral band -> intensity spectrum T (cluster of G/32 CTAs per image)
+//   col_inv  T -> per-row coefficients Q[y][b], b in [0, 2Nx]    (small)
+//   row_inv  Q rows -> image rows                                (HBM-bound)
+// ---------------------------------------------------------------------------
+struct GenGeom {
+  int Lx, Ly, Nx, Ny;
+  int nbx, nby, nf;  // 2Nx+1, 2Ny+1, Nx+1
+  int ntx, nty;      // 2Nx+1, 4Ny+1 (intensity half plane)
+  int G, RG;         // spectral grid G = 32 RG (power of two >= 4N+1); RG CTAs per image
+  int P, V;          // row synthesis: Lx = P V, P a power of two <= 64
+  int Pf, Vf;        // row transforms of masks and of dL/dI: Pf = min(P, 32)
+  int nC;            // lane chunks of 32 covering max(V, Vf)
+  int NBX;           // bin count of the x tables (multiple of 32 and of P, >= 2Nx+1)
+  int ystrip;        // 1: Ly % 32 == 0, strips of 32 rows spaced nS apart; 0: 32-row blocks
+  int nS;            // strips (ystrip) or row blocks per clip
+  int dx, dy;        // one-pixel output shift of odd periods (0 or 1)
+};
+
+constexpr int kGenMaxSplit = 8;
+
+int gen_geometry(int Lx, int Ly, int Nx, int Ny, GenGeom* g);
+size_t gen_rowbins_bytes(const GenGeom& g, int nrows_img, int nbins);  // R / Q buffers
+size_t gen_band_bytes(const GenGeom& g, int n, int nparts, int nrows, int ncols);
+size_t gen_T_bytes(const GenGeom& g, int nimg, int nsplit);
+size_t gen_table_elems(const GenGeom& g);  // twb + twl + tw2 + rootLy (float2)
+int gen_build_tables(const GenGeom& g, float2* tables, cudaStream_t st);
+int gen_choose_split(const GenGeom& g, int nimg, int K);
+int gen_choose_parts(const GenGeom& g, int n, int ncols);
+
+// stage launchers (device pointers, stream-ordered)
+int gen_launch_rowfwd(const GenGeom& g, const float2* tables, const float* src, int nrows, float2* R,
+                      cudaStream_t st);
+int gen_launch_colfwd(const GenGeom& g, const float2* tables, const float2* R, int n, int ncols, int Yb,
+                      float scale, int nparts, float2* band, cudaStream_t st);
+int gen_launch_spectral(const GenGeom& g, const float2* band, int nparts, int nclips, const float2* H,
+                        const float* lam, int K, int nsets, int nsplit, float2* T, cudaStream_t st);
+int gen_launch_colinv(const GenGeom& g, const float2* tables, const float2* T, int nimg, int nsplit, int A,
+                      int nbins, float2* Q, cudaStream_t st);
+int gen_launch_rowinv(const GenGeom& g, const float2* tables, const float2* Q, int nimg, int nbins,
+                      float* images, cudaStream_t st);
+int gen_launch_bandout(const GenGeom& g, const float2* band, int nparts, int nclips, float2* out,
+                       cudaStream_t st);
+// adjoint stages (socs_gen_vjp.cu).  row_vjp overwrites Q (2Nx+1 bins per row)
+// with the row bins of dL/dI; col_fwd then gives its band (|gy| <= 2Ny).
+int gen_launch_rowvjp(const GenGeom& g, const float2* tables, float2* Q, int nimg, int nsets, const float* targets,
+                      float alpha, float thr, float* images, double* loss, cudaStream_t st);
+int gen_launch_vjp_spectral(const GenGeom& g, const float2* band, int nparts, const float2* gband, int gparts,
+                            int nclips, const float2* H, const float* lam, int K, int nsets, int nsplit, float2* gam,
+                            cudaStream_t st);
+int gen_launch_gradT(const GenGeom& g, const float2* gam, int nclips, int nparts, float2* Tg, cudaStream_t st);
+int gen_launch_vjp_source(const GenGeom& g, const float2* band, int nparts, const float2* gband, int gparts,
+                          int nimg, int nsets, const float2* Hs, int S, const float* Jw, const int* src_id,
+                          int nsplit, float* grad_src, cudaStream_t st);
+
 }  // namespace kl
 
 // Internal: upload kernel set `set` of a SOCS plan from device memory

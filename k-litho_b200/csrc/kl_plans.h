@@ -36,6 +36,20 @@ struct kl_socs_plan_s {
   // launch shape chosen by kl_socs_autotune for batches of tune_clips clips
   int tcap = 0;  // clip x kernel-slice products the spectra buffer holds
   int tune_clips = 0, tune_nsplit = 0, tune_spc = 0;
+  // general-geometry pipeline (socs_gen.cu): any period, bands up to 4N+1 <= 256.
+  // Used when the specialised kernels above do not cover the geometry (or on
+  // request); `g` then only carries the sizes.
+  bool gen = false;
+  kl::GenGeom gg{};
+  float2* gtab = nullptr;   // x twiddles, chunk twiddles, roots of unity of Ly
+  float2* R = nullptr;      // row bins of the masks (Nx+1 per row)
+  float2* band = nullptr;   // band partials of the masks
+  float2* Q = nullptr;      // per-row synthesis coefficients of every image; the
+                            // adjoint overwrites them with the row bins of dL/dI
+  int nparts_max = 0;       // band partials per clip the band buffer holds
+  float2* gband = nullptr;  // adjoint: band partials of dL/dI per image
+  int gparts_max = 0;
+  int last_nparts = 0, last_gparts = 0;  // partial counts of the last kl_socs_vjp
 };
 
 namespace kl {
