@@ -112,11 +112,28 @@ typedef struct kl_tcc_plan_s* kl_tcc_plan; /* see the TCC section below */
 /* Plan for clips of period Lx x Ly imaged with `nsets` kernel sets (e.g. one
  * per focus) of `nk` kernels of band (2Nx+1) x (2Ny+1), for batches of up to
  * `max_clips` clips.  Allocates the plan's device workspace on the current
- * device.  Returns KL_ERR_UNSUPPORTED (with a message) for geometries the
- * compiled kernels do not cover. */
+ * device.  Any period is accepted, as the reference accepts any Lx, Ly
+ * (K-Litho-SOCS/klitho_socs.cpp:256-270): periods whose pixels split into 32
+ * lanes of 8, 16 or 32 (Lx in {256, 512, 768, 1024, 1536, 2048, 3072}, Ly a
+ * multiple of the strip height) with 4N+1 <= 128 run on the specialised
+ * kernels, every other period and bands up to 4*max(Nx,Ny)+1 <= 256 (4096^2
+ * at NA 1.35) on the general pipeline.  Returns KL_ERR_UNSUPPORTED (with a
+ * message) beyond that, or when the SOCS grid 4N+1 exceeds half the period. */
 int kl_socs_plan_create(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
                         int max_clips);
 int kl_socs_plan_destroy(kl_socs_plan plan);
+
+/* kl_socs_plan_create with options: KL_SOCS_ADJOINT makes the plan that
+ * kl_socs_plan_create_adjoint makes; KL_SOCS_GENERAL puts the plan on the
+ * general pipeline even where the specialised kernels cover the geometry
+ * (same results within the FP32 tolerance; for cross-checks and timing).
+ * No counterpart in the reference. */
+#define KL_SOCS_ADJOINT 1
+#define KL_SOCS_GENERAL 2
+int kl_socs_plan_create_ex(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
+                           int max_clips, int flags);
+/* 0 if the plan runs on the specialised kernels, 1 on the general pipeline. */
+int kl_socs_plan_engine(kl_socs_plan plan);
 
 /* Upload kernel set `set`: nk planes of the kernel layout, real and imaginary
  * parts separately (as krn_<i>_r.bin / krn_<i>_i.bin hold them), and nk
@@ -178,8 +195,10 @@ int kl_socs_batch_graph_builds(kl_socs_batch batch);
 /* ------------------------------------------------------------------------- */
 
 /* A SOCS plan that also supports kl_socs_vjp (taller strips so the band of
- * dL/dI fits; clips up to 1024^2 at NA 1.35).  Its kl_socs_forward gives the
- * same images as kl_socs_plan_create's. */
+ * dL/dI fits).  Clips up to 1024^2 at NA 1.35 run on the specialised
+ * kernels, larger bands and other periods on the general pipeline, with the
+ * limits of kl_socs_plan_create.  Its kl_socs_forward gives the same images
+ * as kl_socs_plan_create's within the FP32 tolerance. */
 int kl_socs_plan_create_adjoint(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk,
                                 int nsets, int max_clips);
 
@@ -332,6 +351,10 @@ int kl_hopkins_image_host(kl_tcc_plan plan, const float* mask_host, float* image
  * of KL_PREC_FP64 precision only. */
 int kl_fp64_hopkins_image(kl_tcc_plan plan, const float* masks_dev, int nclips, double* images_dev,
                           void* stream);
+/* One FP64 Hopkins image from and to host memory, stored as float as the
+ * reference stores image.bin (klitho_tcc.cpp:537-544); KL_PREC_FP64 plans,
+ * Lx and Ly powers of two.  Synchronous. */
+int kl_fp64_hopkins_image_host(kl_tcc_plan plan, const float* mask_host, float* image_host);
 
 #ifdef __cplusplus
 }

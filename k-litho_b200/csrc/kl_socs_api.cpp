@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <new>
 #include <string>
@@ -37,6 +38,11 @@ void free_plan(kl_socs_plan p) {
   cudaFree(p->gpart);
   cudaFree(p->gam);
   cudaFree(p->Tg);
+  cudaFree(p->gtab);
+  cudaFree(p->R);
+  cudaFree(p->band);
+  cudaFree(p->Q);
+  cudaFree(p->gband);
   delete p;
 }
 
@@ -82,8 +88,33 @@ void launch_shape(kl_socs_plan p, int nclips, int* nsplit, int* spc) {
   }
 }
 
+// general-geometry pipeline: row transform, column transform, spectral core,
+// column synthesis, row synthesis
+int run_forward_gen(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st,
+                    const cudaEvent_t* ev4) {
+  const kl::GenGeom& g = p->gg;
+  const int nimg = nclips * p->nsets;
+  int nsplit = kl::gen_choose_split(g, nimg, p->K);
+  if (p->tune_clips == nclips && p->tune_nsplit > 0) nsplit = p->tune_nsplit;
+  const int nparts = kl::gen_choose_parts(g, nclips, g.nf);
+  int rc;
+  if ((rc = stage_mark(p, st, ev4, 0))) return rc;
+  if ((rc = kl::gen_launch_rowfwd(g, p->gtab, masks, nclips * g.Ly, p->R, st))) return rc;
+  if ((rc = kl::gen_launch_colfwd(g, p->gtab, p->R, nclips, g.nf, g.Ny, 1.0f / ((float)g.Lx * (float)g.Ly), nparts,
+                                  p->band, st)))
+    return rc;
+  if ((rc = stage_mark(p, st, ev4, 1))) return rc;
+  if ((rc = kl::gen_launch_spectral(g, p->band, nparts, nclips, p->H, p->lam, p->K, p->nsets, nsplit, p->T, st)))
+    return rc;
+  if ((rc = stage_mark(p, st, ev4, 2))) return rc;
+  if ((rc = kl::gen_launch_colinv(g, p->gtab, p->T, nimg, nsplit, 2 * g.Ny, g.ntx, p->Q, st))) return rc;
+  if ((rc = kl::gen_launch_rowinv(g, p->gtab, p->Q, nimg, g.ntx, images, st))) return rc;
+  return stage_mark(p, st, ev4, 3);
+}
+
 int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st,
                 const cudaEvent_t* ev4 = nullptr) {
+  if (p->gen) return run_forward_gen(p, masks, nclips, images, st, ev4);
   int rc;
   if ((rc = stage_mark(p, st, ev4, 0))) return rc;
   int nsplit, spc;
@@ -98,15 +129,94 @@ int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, c
   if (rc) return rc;
   return stage_mark(p, st, ev4, 3);
 }
+// plan on the general-geometry pipeline
+int create_gen_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets, int max_clips,
+                    bool adjoint) {
+  kl::GenGeom gg;
+  int rc = kl::gen_geometry(Lx, Ly, Nx, Ny, &gg);
+  if (rc) return rc;
+  kl_socs_plan p = new (std::nothrow) kl_socs_plan_s;
+  if (!p) {
+    kl::set_error("kl_socs_plan_create: out of host memory");
+    return KL_ERR_NOMEM;
+  }
+  p->gen = true;
+  p->adjoint = adjoint;
+  p->gg = gg;
+  // sizes only, for callers that read them
+  p->g.Lx = Lx;
+  p->g.Ly = Ly;
+  p->g.Nx = Nx;
+  p->g.Ny = Ny;
+  p->g.nbx = gg.nbx;
+  p->g.nby = gg.nby;
+  p->g.nf = gg.nf;
+  p->g.ntx = gg.ntx;
+  p->g.nty = gg.nty;
+  p->g.G = gg.G;
+  p->g.nS = gg.nS;
+  p->g.dx = gg.dx;
+  p->g.dy = gg.dy;
+  p->K = nk;
+  p->nsets = nsets;
+  p->max_clips = max_clips;
+  cudaGetDevice(&p->device);
+  const size_t nb2 = (size_t)gg.nby * gg.nbx;
+  // spectra buffer: the largest (image, kernel slice) count any batch size or
+  // autotuned split needs
+  int tcap = 0, pmax = 0;
+  for (int n = 1; n <= max_clips; ++n) {
+    tcap = std::max(tcap, n * nsets * kl::gen_choose_split(gg, n * nsets, nk));
+    pmax = std::max(pmax, kl::gen_choose_parts(gg, n, gg.nf));
+  }
+  for (int ns = 1; ns <= kl::kGenMaxSplit; ns *= 2) tcap = std::max(tcap, std::min(ns, nk) * nsets);
+  p->tcap = tcap;
+  p->nparts_max = pmax;
+  if ((rc = alloc((void**)&p->H, sizeof(float2) * nb2 * nk * nsets, "kernels")) ||
+      (rc = alloc((void**)&p->lam, sizeof(float) * (size_t)nk * nsets, "eigenvalues")) ||
+      (rc = alloc((void**)&p->gtab, sizeof(float2) * kl::gen_table_elems(gg), "tables")) ||
+      (rc = alloc((void**)&p->R, kl::gen_rowbins_bytes(gg, max_clips, gg.nf), "row bins")) ||
+      (rc = alloc((void**)&p->band, kl::gen_band_bytes(gg, max_clips, pmax, gg.nby, gg.nf), "band partials")) ||
+      (rc = alloc((void**)&p->T, kl::gen_T_bytes(gg, tcap, 1), "spectra")) ||
+      (rc = alloc((void**)&p->Q, kl::gen_rowbins_bytes(gg, max_clips * nsets, gg.ntx), "row coefficients")) ||
+      (rc = kl::gen_build_tables(gg, p->gtab, nullptr))) {
+    free_plan(p);
+    return rc;
+  }
+  if (adjoint) {
+    int gmax = 0;
+    for (int n = 1; n <= max_clips; ++n) gmax = std::max(gmax, kl::gen_choose_parts(gg, n * nsets, gg.ntx));
+    p->gparts_max = gmax;
+    if ((rc = alloc((void**)&p->gband, kl::gen_band_bytes(gg, max_clips * nsets, gmax, gg.nty, gg.ntx),
+                    "dL/dI bands")) ||
+        (rc = alloc((void**)&p->gam, sizeof(float2) * nb2 * tcap, "adjoint partials")) ||
+        (rc = alloc((void**)&p->Tg, sizeof(float2) * (size_t)max_clips * gg.nf * gg.nby, "gradient spectra"))) {
+      free_plan(p);
+      return rc;
+    }
+  }
+  if (cudaStreamSynchronize(nullptr) != cudaSuccess) {
+    kl::set_error(std::string("kl_socs_plan_create: ") + cudaGetErrorString(cudaGetLastError()));
+    free_plan(p);
+    return KL_ERR_CUDA;
+  }
+  cudaMemset(p->H, 0, sizeof(float2) * nb2 * nk * nsets);
+  cudaMemset(p->lam, 0, sizeof(float) * (size_t)nk * nsets);
+  *plan = p;
+  return KL_OK;
+}
+
 int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
-                int max_clips, bool adjoint) {
+                int max_clips, bool adjoint, bool general = false) {
   KL_CHECK_ARG(plan != nullptr, "kl_socs_plan_create: plan is NULL");
   *plan = nullptr;
   KL_CHECK_ARG(nk > 0 && nsets > 0 && max_clips > 0, "kl_socs_plan_create: nk, nsets, max_clips must be positive");
   kl::SocsGeom g;
-  int rc = kl::socs_geometry(Lx, Ly, Nx, Ny, &g, adjoint);
+  int rc = general ? KL_ERR_UNSUPPORTED : kl::socs_geometry(Lx, Ly, Nx, Ny, &g, adjoint);
+  if (!rc && adjoint) rc = kl::vjp_supported(g);
+  // geometries outside the specialised kernels run on the general pipeline
+  if (rc == KL_ERR_UNSUPPORTED) return create_gen_plan(plan, Lx, Ly, Nx, Ny, nk, nsets, max_clips, adjoint);
   if (rc) return rc;
-  if (adjoint && (rc = kl::vjp_supported(g))) return rc;
   kl_socs_plan p = new (std::nothrow) kl_socs_plan_s;
   if (p) p->adjoint = adjoint;
   if (!p) {
@@ -160,6 +270,41 @@ int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int 
 }
 }  // namespace
 
+namespace {
+// adjoint on the general pipeline: forward to T, image + resist + dL/dI row
+// bins, dL/dI band, Gam, gradient spectrum, gradient image
+int vjp_gen(kl_socs_plan p, const float* masks, const float* targets, int nclips, float alpha, float threshold,
+            float* images, float* grad, double* loss, cudaStream_t st) {
+  const kl::GenGeom& g = p->gg;
+  const int nimg = nclips * p->nsets;
+  const int ns = kl::gen_choose_split(g, nimg, p->K);
+  const int nparts = kl::gen_choose_parts(g, nclips, g.nf);
+  const int gparts = kl::gen_choose_parts(g, nimg, g.ntx);
+  int rc;
+  if ((rc = kl::gen_launch_rowfwd(g, p->gtab, masks, nclips * g.Ly, p->R, st))) return rc;
+  if ((rc = kl::gen_launch_colfwd(g, p->gtab, p->R, nclips, g.nf, g.Ny, 1.0f / ((float)g.Lx * (float)g.Ly), nparts,
+                                  p->band, st)))
+    return rc;
+  if ((rc = kl::gen_launch_spectral(g, p->band, nparts, nclips, p->H, p->lam, p->K, p->nsets, ns, p->T, st)))
+    return rc;
+  if ((rc = kl::gen_launch_colinv(g, p->gtab, p->T, nimg, ns, 2 * g.Ny, g.ntx, p->Q, st))) return rc;
+  KL_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(double) * (size_t)nimg, st));
+  if ((rc = kl::gen_launch_rowvjp(g, p->gtab, p->Q, nimg, p->nsets, targets, alpha, threshold, images, loss, st)))
+    return rc;
+  if ((rc = kl::gen_launch_colfwd(g, p->gtab, p->Q, nimg, g.ntx, 2 * g.Ny, 1.0f, gparts, p->gband, st))) return rc;
+  if ((rc = kl::gen_launch_vjp_spectral(g, p->band, nparts, p->gband, gparts, nclips, p->H, p->lam, p->K, p->nsets,
+                                        ns, p->gam, st)))
+    return rc;
+  if ((rc = kl::gen_launch_gradT(g, p->gam, nclips, p->nsets * ns, p->Tg, st))) return rc;
+  if ((rc = kl::gen_launch_colinv(g, p->gtab, p->Tg, nclips, 1, g.Ny, g.nf, p->Q, st))) return rc;
+  if ((rc = kl::gen_launch_rowinv(g, p->gtab, p->Q, nclips, g.nf, grad, st))) return rc;
+  p->last_vjp_clips = nclips;
+  p->last_nparts = nparts;
+  p->last_gparts = gparts;
+  return KL_OK;
+}
+}  // namespace
+
 int kl::socs_run_forward(kl_socs_plan_s* p, const float* masks, int nclips, float* images, cudaStream_t st,
                          const cudaEvent_t* ev4) {
   return run_forward(p, masks, nclips, images, st, ev4);
@@ -177,6 +322,15 @@ int kl_socs_plan_create_adjoint(kl_socs_plan* plan, int Lx, int Ly, int Nx, int 
   return create_plan(plan, Lx, Ly, Nx, Ny, nk, nsets, max_clips, true);
 }
 
+int kl_socs_plan_create_ex(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int nsets,
+                           int max_clips, int flags) {
+  KL_CHECK_ARG((flags & ~(KL_SOCS_ADJOINT | KL_SOCS_GENERAL)) == 0, "kl_socs_plan_create_ex: unknown flags");
+  return create_plan(plan, Lx, Ly, Nx, Ny, nk, nsets, max_clips, (flags & KL_SOCS_ADJOINT) != 0,
+                     (flags & KL_SOCS_GENERAL) != 0);
+}
+
+int kl_socs_plan_engine(kl_socs_plan plan) { return plan ? (plan->gen ? 1 : 0) : -1; }
+
 int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nclips, float alpha,
                 float threshold, float* images, float* grad, double* loss, void* stream) {
   KL_CHECK_ARG(p && masks && targets && grad && loss, "kl_socs_vjp: NULL argument");
@@ -185,6 +339,7 @@ int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nc
   KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_socs_vjp: nclips exceeds the plan");
   cudaStream_t st = (cudaStream_t)stream;
   if (nclips == 0) return KL_OK;
+  if (p->gen) return vjp_gen(p, masks, targets, nclips, alpha, threshold, images, grad, loss, st);
   const kl::SocsGeom& g = p->g;
   int rc;
   const int ns1 = kl::socs_choose_split(g, nclips, p->nsets, p->K);
@@ -324,6 +479,16 @@ int kl_mask_spectrum(kl_socs_plan p, const float* masks, int nclips, float* band
   KL_CHECK_ARG(p && masks && band, "kl_mask_spectrum: NULL argument");
   KL_CHECK_ARG(nclips >= 0 && nclips <= p->max_clips, "kl_mask_spectrum: nclips exceeds the plan");
   cudaStream_t st = (cudaStream_t)stream;
+  if (p->gen) {
+    const kl::GenGeom& g = p->gg;
+    const int nparts = kl::gen_choose_parts(g, nclips, g.nf);
+    int rc = kl::gen_launch_rowfwd(g, p->gtab, masks, nclips * g.Ly, p->R, st);
+    if (!rc)
+      rc = kl::gen_launch_colfwd(g, p->gtab, p->R, nclips, g.nf, g.Ny, 1.0f / ((float)g.Lx * (float)g.Ly), nparts,
+                                 p->band, st);
+    if (!rc) rc = kl::gen_launch_bandout(g, p->band, nparts, nclips, reinterpret_cast<float2*>(band), st);
+    return rc;
+  }
   int rc = kl::socs_launch_forward(p->g, p->tx, p->ty, masks, nclips, p->partial, st);
   if (rc) return rc;
   return kl::socs_launch_band(p->g, p->partial, nclips, reinterpret_cast<float2*>(band), st);

@@ -81,9 +81,14 @@ int kl_socs_autotune(kl_socs_plan p, const float* masks, int nclips, float* imag
   const bool timing = p->timing;
   p->timing = false;
   std::vector<int> splits, spcs;
+  // the spectra buffer holds tcap (clip, slice) pairs per kernel set on the
+  // specialised kernels, tcap (image, slice) pairs on the general pipeline
+  const int per_slice = p->gen ? nclips * p->nsets : nclips;
   for (int ns = 1; ns <= kl::kSocsMaxSplit; ns *= 2)
-    if (ns * nclips <= p->tcap && ns <= p->K) splits.push_back(ns);
-  for (int c = 1; c <= 16 && c <= p->g.nS; c *= 2) spcs.push_back(c);
+    if (ns * per_slice <= p->tcap && ns <= p->K) splits.push_back(ns);
+  // strips per CTA of the synthesis: specialised kernels only
+  if (!p->gen)
+    for (int c = 1; c <= 16 && c <= p->g.nS; c *= 2) spcs.push_back(c);
   cudaEvent_t e0, e1;
   KL_CUDA_TRY(cudaEventCreate(&e0));
   KL_CUDA_TRY(cudaEventCreate(&e1));

@@ -440,7 +440,10 @@ int kl_socs_vjp_source(kl_socs_plan sp, kl_tcc_plan tp, float* grad_src, void* s
   int nsplit = 1;
   while (nsplit < S && nimg * nsplit < 2 * 148) nsplit *= 2;
   if (nsplit > S) nsplit = S;
-  if (!rc)
+  if (!rc && sp->gen)
+    rc = kl::gen_launch_vjp_source(sp->gg, sp->band, sp->last_nparts, sp->gband, sp->last_gparts, nimg, sp->nsets, H,
+                                   S, tp->J, tp->src_id, nsplit, grad_src, st);
+  else if (!rc)
     rc = kl::vjp_launch_source(sp->g, sp->partial, sp->gpart, nimg, sp->nsets, H, tp->J, tp->src_id,
                                S, nsplit, grad_src, st);
   cudaStreamSynchronize(st);
@@ -464,6 +467,35 @@ int kl_hopkins_image_host(kl_tcc_plan p, const float* mask_host, float* image_ho
     kl::set_error(std::string("kl_hopkins_image_host: ") + cudaGetErrorString(cudaGetLastError()));
     rc = KL_ERR_CUDA;
   }
+  dfree(md);
+  dfree(id);
+  return rc;
+}
+
+int kl_fp64_hopkins_image_host(kl_tcc_plan p, const float* mask_host, float* image_host) {
+  KL_CHECK_ARG(p && mask_host && image_host, "kl_fp64_hopkins_image_host: NULL argument");
+  KL_CHECK_ARG(p->precision == KL_PREC_FP64, "kl_fp64_hopkins_image_host: needs a plan of KL_PREC_FP64 precision");
+  const size_t n = (size_t)p->Lx * p->Ly;
+  float* md = nullptr;
+  double* id = nullptr;
+  int rc;
+  if ((rc = dalloc((void**)&md, sizeof(float) * n, "mask")) || (rc = dalloc((void**)&id, sizeof(double) * n, "image"))) {
+    dfree(md);
+    return rc;
+  }
+  std::vector<double> img(n);
+  if (cudaMemcpy(md, mask_host, sizeof(float) * n, cudaMemcpyHostToDevice) != cudaSuccess) {
+    kl::set_error(std::string("kl_fp64_hopkins_image_host: ") + cudaGetErrorString(cudaGetLastError()));
+    rc = KL_ERR_CUDA;
+  }
+  if (!rc) rc = kl_fp64_hopkins_image(p, md, 1, id, nullptr);
+  if (!rc && cudaMemcpy(img.data(), id, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess) {
+    kl::set_error(std::string("kl_fp64_hopkins_image_host: ") + cudaGetErrorString(cudaGetLastError()));
+    rc = KL_ERR_CUDA;
+  }
+  // the reference stores the float cast of its double image (klitho_tcc.cpp:537-544)
+  if (!rc)
+    for (size_t i = 0; i < n; ++i) image_host[i] = (float)img[i];
   dfree(md);
   dfree(id);
   return rc;

@@ -25,6 +25,8 @@ KL_ERR_NOMEM = 3
 KL_ERR_UNSUPPORTED = 4
 KL_ERR_NOT_CONVERGED = 5
 KL_ERR_IO = 6
+KL_SOCS_ADJOINT = 1
+KL_SOCS_GENERAL = 2
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_float_p = ctypes.POINTER(ctypes.c_float)
@@ -70,6 +72,8 @@ def lib() -> ctypes.CDLL:
         L.kl_socs_plan_create.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_int]
+        L.kl_socs_plan_create_ex.argtypes = L.kl_socs_plan_create.argtypes + [ctypes.c_int]
+        L.kl_socs_plan_engine.argtypes = [_vp]
         L.kl_socs_plan_destroy.argtypes = [_vp]
         L.kl_socs_set_kernels.argtypes = [_vp, ctypes.c_int, _c_float_p, _c_float_p, _c_float_p]
         L.kl_socs_forward.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
@@ -225,14 +229,22 @@ class SocsPlan:
     """GPU SOCS imaging for clips of one period (calcSOCS + FI on device)."""
 
     def __init__(self, Lx: int, Ly: int, Nx: int, Ny: int, nk: int, nsets: int = 1,
-                 max_clips: int = 1, adjoint: bool = False):
+                 max_clips: int = 1, adjoint: bool = False, general: bool = False):
+        """`general` puts the plan on the general-geometry pipeline even where
+        the specialised kernels cover the period (kl_socs_plan_create_ex)."""
         self.Lx, self.Ly, self.Nx, self.Ny = int(Lx), int(Ly), int(Nx), int(Ny)
         self.nk, self.nsets, self.max_clips = int(nk), int(nsets), int(max_clips)
         h = _vp()
-        create = lib().kl_socs_plan_create_adjoint if adjoint else lib().kl_socs_plan_create
-        check(create(ctypes.byref(h), self.Lx, self.Ly, self.Nx, self.Ny, self.nk, self.nsets,
-                     self.max_clips), "kl_socs_plan_create")
+        flags = (KL_SOCS_ADJOINT if adjoint else 0) | (KL_SOCS_GENERAL if general else 0)
+        check(lib().kl_socs_plan_create_ex(ctypes.byref(h), self.Lx, self.Ly, self.Nx, self.Ny,
+                                           self.nk, self.nsets, self.max_clips, flags),
+              "kl_socs_plan_create")
         self._h = h
+
+    @property
+    def engine(self) -> str:
+        """'specialised' or 'general' (kl_socs_plan_engine)."""
+        return "general" if lib().kl_socs_plan_engine(self._h) == 1 else "specialised"
 
     def close(self) -> None:
         if getattr(self, "_h", None):

@@ -57,12 +57,15 @@ def rect_mask_fill(L: int, seed: int, density: float) -> np.ndarray:
     return rect_mask(L, R, seed)
 
 
-def smooth_mask(L: int, seed: int, sigma_px: float = 12.0, gain: float = 6.0) -> np.ndarray:
-    """Continuous mask in [0, 1]: periodic Gaussian-filtered noise through a sigmoid."""
+def smooth_mask(L: int, seed: int, sigma_px: float = 12.0, gain: float = 6.0,
+                Ly: int | None = None) -> np.ndarray:
+    """Continuous mask in [0, 1]: periodic Gaussian-filtered noise through a
+    sigmoid, L x Ly (square by default)."""
+    Ly = L if Ly is None else Ly
     rng = np.random.default_rng(seed)
-    n = rng.standard_normal((L, L))
-    f = np.fft.fftfreq(L)
-    g = np.exp(-2.0 * (np.pi * sigma_px) ** 2 * (f[:, None] ** 2 + f[None, :] ** 2))
+    n = rng.standard_normal((Ly, L))
+    fx, fy = np.fft.fftfreq(L), np.fft.fftfreq(Ly)
+    g = np.exp(-2.0 * (np.pi * sigma_px) ** 2 * (fy[:, None] ** 2 + fx[None, :] ** 2))
     s = np.real(np.fft.ifft2(np.fft.fft2(n) * g))
     s /= s.std() + 1e-30
     return (1.0 / (1.0 + np.exp(-gain * s))).astype(np.float32)

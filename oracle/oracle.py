@@ -378,23 +378,78 @@ def _band_index(L, N):
 
 def socs_fields_torch(mask, krn, Nx, Ny):
     """Coherent fields E_k on the full Lx x Ly grid (complex128), the
-    band-limited evaluation the reference's calcSOCS + FI produces."""
+    band-limited evaluation the reference's calcSOCS + FI produces.  Runs on
+    the device of `mask` when it is a torch tensor (CPU otherwise)."""
     import torch
     m = mask if isinstance(mask, torch.Tensor) else torch.as_tensor(mask, dtype=torch.float64)
+    dev = m.device
     Ly, Lx = m.shape
     D = torch.fft.fft2(m.to(torch.float64))
-    iy, ix = _band_index(Ly, Ny), _band_index(Lx, Nx)
+    iy, ix = _band_index(Ly, Ny).to(dev), _band_index(Lx, Nx).to(dev)
     M = D[iy][:, ix] / (Lx * Ly)
-    H = torch.as_tensor(np.asarray(krn, dtype=np.complex128)).reshape(-1, 2 * Ny + 1, 2 * Nx + 1)
+    H = torch.as_tensor(np.asarray(krn, dtype=np.complex128), device=dev).reshape(-1, 2 * Ny + 1, 2 * Nx + 1)
     # odd periods: the reference's shifts place the image one pixel later
     dy, dx = 2 * ((Ly + 1) // 2) - Ly, 2 * ((Lx + 1) // 2) - Lx
-    fy = torch.arange(-Ny, Ny + 1, dtype=torch.float64)[:, None]
-    fx = torch.arange(-Nx, Nx + 1, dtype=torch.float64)[None, :]
+    fy = torch.arange(-Ny, Ny + 1, dtype=torch.float64, device=dev)[:, None]
+    fx = torch.arange(-Nx, Nx + 1, dtype=torch.float64, device=dev)[None, :]
     ph = torch.exp(-2j * np.pi * (fy * dy / Ly + fx * dx / Lx))
     C = H * (M * ph)[None]
-    full = torch.zeros((H.shape[0], Ly, Lx), dtype=torch.complex128)
+    full = torch.zeros((H.shape[0], Ly, Lx), dtype=torch.complex128, device=dev)
     full[:, iy[:, None], ix[None, :]] = C
     return torch.fft.ifft2(full) * (Lx * Ly)
+
+
+def socs_vjp_reference_chunked(mask, target, krn, scales, Nx, Ny, alpha=50.0, thr=0.225,
+                               device="cpu", chunk=8):
+    """(loss, dL/dmask, image, dL/dI) in FP64 like socs_vjp_reference, with the
+    kernels taken `chunk` at a time (the image first, then one
+    vector-Jacobian product per chunk), so large clips with many kernels fit
+    in memory.  `device` may be a CUDA device: torch's FP64 FFTs then serve as
+    the cross-check."""
+    import torch
+    krn = np.asarray(krn)
+    lam = np.asarray(scales, dtype=np.float64)
+    m = torch.as_tensor(np.asarray(mask, dtype=np.float64), device=device)
+    t = torch.as_tensor(np.asarray(target, dtype=np.float64), device=device)
+    nk = krn.shape[0]
+    with torch.no_grad():
+        I = torch.zeros_like(m)
+        for k0 in range(0, nk, chunk):
+            E = socs_fields_torch(m, krn[k0:k0 + chunk], Nx, Ny)
+            lk = torch.as_tensor(lam[k0:k0 + chunk], device=device)
+            I += (lk[:, None, None] * (E.real ** 2 + E.imag ** 2)).sum(0)
+            del E
+        s = torch.sigmoid(alpha * (I - thr))
+        loss = float(((s - t) ** 2).sum())
+        G = 2.0 * (s - t) * s * (1.0 - s) * alpha
+    grad = torch.zeros_like(m)
+    for k0 in range(0, nk, chunk):
+        mm = m.clone().requires_grad_(True)
+        E = socs_fields_torch(mm, krn[k0:k0 + chunk], Nx, Ny)
+        lk = torch.as_tensor(lam[k0:k0 + chunk], device=device)
+        Ic = (lk[:, None, None] * (E.real ** 2 + E.imag ** 2)).sum(0)
+        (Ic * G).sum().backward()
+        grad += mm.grad
+        del E, Ic, mm
+    return loss, grad.cpu().numpy(), I.cpu().numpy(), G.cpu().numpy()
+
+
+def socs_loss_chunked(mask, target, krn, scales, Nx, Ny, alpha=50.0, thr=0.225, device="cpu", chunk=8):
+    """FP64 loss of socs_vjp_reference_chunked (for finite differences)."""
+    import torch
+    krn = np.asarray(krn)
+    lam = np.asarray(scales, dtype=np.float64)
+    with torch.no_grad():
+        m = torch.as_tensor(np.asarray(mask, dtype=np.float64), device=device)
+        t = torch.as_tensor(np.asarray(target, dtype=np.float64), device=device)
+        I = torch.zeros_like(m)
+        for k0 in range(0, krn.shape[0], chunk):
+            E = socs_fields_torch(m, krn[k0:k0 + chunk], Nx, Ny)
+            lk = torch.as_tensor(lam[k0:k0 + chunk], device=device)
+            I += (lk[:, None, None] * (E.real ** 2 + E.imag ** 2)).sum(0)
+            del E
+        s = torch.sigmoid(alpha * (I - thr))
+        return float(((s - t) ** 2).sum())
 
 
 def socs_image_torch(mask, krn, scales, Nx, Ny):

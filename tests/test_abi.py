@@ -41,11 +41,13 @@ def test_version_and_error_string():
 
 
 def test_unsupported_geometry_rejected_before_gpu():
+    # any period is accepted; a SOCS grid 4N+1 above 256, or above half the
+    # period, is refused on the host before any device work
     with pytest.raises(K.KLError) as e:
-        K.SocsPlan(300, 300, 3, 3, 2)
+        K.SocsPlan(8192, 8192, 70, 70, 2)
     assert e.value.code == K.KL_ERR_UNSUPPORTED
     with pytest.raises(K.KLError) as e:
-        K.SocsPlan(1024, 1024, 40, 40, 2)
+        K.SocsPlan(256, 256, 40, 40, 2)
     assert e.value.code == K.KL_ERR_UNSUPPORTED
     with pytest.raises(K.KLError) as e:
         K.SocsPlan(1024, 1024, 13, 13, 0)

@@ -144,7 +144,9 @@ def test_socs_host_entry_pipelined_chunks(cuda):
     assert np.array_equal(host, again)
 
 
-def test_socs_unsupported_geometry_is_an_error(cuda):
-    with pytest.raises(K.KLError) as e:
-        K.SocsPlan(300, 300, 3, 3, 2)
-    assert e.value.code == K.KL_ERR_UNSUPPORTED
+def test_socs_engine_choice(cuda):
+    # the specialised kernels take the periods they were built for; any other
+    # period goes to the general pipeline rather than failing
+    assert K.SocsPlan(1024, 1024, 13, 13, 2).engine == "specialised"
+    assert K.SocsPlan(300, 300, 3, 3, 2).engine == "general"
+    assert K.SocsPlan(1024, 1024, 13, 13, 2, general=True).engine == "general"
