@@ -4,7 +4,9 @@
 // console output, same inputs (kernel_info.txt + krn_<i>_{r,i}.bin from the
 // kernel directory, float32 mask) and the same ./out/image.bin.  The image is
 // computed on the GPU by the fused SOCS pipeline of libklitho_gpu
-// (kl_socs_forward_host) instead of FFTW.  PNG previews are not written.
+// (kl_socs_forward_host) instead of FFTW, for any period Lx x Ly.  The
+// reference's PNG previews (mask.png, image.png, image_s.png) are written by
+// the library's own PNG writer; KLITHO_PNG=0 skips them.
 #include <cstdlib>
 #include <string>
 #include <vector>

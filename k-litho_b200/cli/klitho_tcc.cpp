@@ -3,14 +3,20 @@
 // Same 22 positional arguments (klitho_tcc.cpp:386-429), validation and
 // console output; writes ./out/image.bin (Hopkins image), and, for nk > 0,
 // ./out/kernels/krn_<i>_{r,i}.bin and ./out/kernels/kernel_info.txt in the
-// reference's formats.  The TCC is assembled on the tensor cores, the SOCS
-// kernels come from blocked subspace iteration on the GPU, and the image from
-// the fused imaging pipeline (libklitho_gpu).  PNG previews are not written.
+// reference's formats, plus the reference's PNG previews (KLITHO_PNG=0 skips
+// them).  The TCC is assembled on the tensor cores, the SOCS kernels come from
+// the GPU eigensolver, and the image from the fused imaging pipeline
+// (libklitho_gpu), for any period Lx x Ly the reference accepts.
+//
+// The kernels are computed and written before the image, so that a failure of
+// one stage leaves the other's files in place; the console reports the two
+// stages in the reference's order (calcImage, then calcKernels).
 //
 // Extensions that leave the argv form unchanged (environment variables):
 //   KLITHO_N_MEDIUM   immersion index n (default 1 = the reference's pupil);
 //                     NA up to n is then accepted instead of NA <= 1
-//   KLITHO_PRECISION  "fast" (default) or "fp64" (plain FP64 TCC + eigen)
+//   KLITHO_PRECISION  "fast" (default) or "fp64": plain FP64 TCC + eigen, and
+//                     the FP64 Hopkins image where Lx and Ly are powers of two
 #include <cstdlib>
 #include <string>
 #include <vector>
@@ -142,19 +148,12 @@ int main(int argc, char* argv[]) {
     std::cout << "Max. TCC Imag Value: " << (float)mm[2] << std::endl;
   }
 
-  klcli::banner_section("Starting calcImage...");
-  {
-    std::vector<float> img((size_t)Lx * Ly);
-    if (kl_hopkins_image_host(plan, msk.data(), img.data()) != KL_OK) return klcli::fail("kl_hopkins_image_host");
-    const float mx = klcli::max_of(img), mn = klcli::min_of(img);
-    std::cout << "Max. Intensity: " << mx << std::endl;
-    if (kl_write_float_file("./out/image.bin", img.data(), Lx * Ly) != KL_OK) std::exit(1);
-    klcli::png("./out/image.png", img, Lx, Ly, mn, mx, KL_PNG_CONTINUOUS);
-    klcli::png("./out/image_s.png", img, Lx, Ly, 0.0f, kTargetIntensity, KL_PNG_7COLORS);
-  }
-
+  // calcKernels first (its files are written even if the image fails)
+  std::vector<float> kre((size_t)nk * tccSize), kim((size_t)nk * tccSize), scales(nk);
+  std::vector<double> ev(nk);
+  int eig_rc = KL_OK;
+  std::string eig_err;
   if (nk > 0) {
-    klcli::banner_section("Starting calcKernels...");
     kl_tcc_plan eplan = plan;
     kl_tcc_plan plan64 = nullptr;
     if (precision == KL_PREC_FP64) {
@@ -162,32 +161,68 @@ int main(int argc, char* argv[]) {
         return klcli::fail("kl_tcc_plan_create");
       eplan = plan64;
     }
-    std::vector<float> kre((size_t)nk * tccSize), kim((size_t)nk * tccSize), scales(nk);
-    std::vector<double> ev(nk);
-    std::cout << "Solving eigenproblem..." << std::endl;
     int iters = 0;
-    const int rc = kl_topk_eig(eplan, nk, 0, kre.data(), kim.data(), scales.data(), ev.data(), &iters);
-    if (rc != KL_OK) {
-      std::cerr << "Kernels derivation failed with info = " << rc << " (" << kl_last_error() << ")" << std::endl;
+    eig_rc = kl_topk_eig(eplan, nk, 0, kre.data(), kim.data(), scales.data(), ev.data(), &iters);
+    if (eig_rc != KL_OK) eig_err = kl_last_error();
+    if (plan64) kl_tcc_plan_destroy(plan64);
+    if (eig_rc == KL_OK) {
+      for (int i = 0; i < nk; ++i) {
+        const std::string b = "./out/kernels/krn_" + std::to_string(i);
+        if (kl_write_float_file((b + "_r.bin").c_str(), kre.data() + (size_t)i * tccSize, tccSize) != KL_OK ||
+            kl_write_float_file((b + "_i.bin").c_str(), kim.data() + (size_t)i * tccSize, tccSize) != KL_OK)
+          std::exit(1);
+        const std::vector<float> kr(kre.begin() + (size_t)i * tccSize, kre.begin() + (size_t)(i + 1) * tccSize);
+        const std::vector<float> ki(kim.begin() + (size_t)i * tccSize, kim.begin() + (size_t)(i + 1) * tccSize);
+        const std::string pb = "./out/kernels/png/krn_" + std::to_string(i);
+        klcli::png(pb + "_r.png", kr, 2 * Nx + 1, 2 * Ny + 1, klcli::min_of(kr), klcli::max_of(kr), KL_PNG_CONTINUOUS);
+        klcli::png(pb + "_i.png", ki, 2 * Nx + 1, 2 * Ny + 1, klcli::min_of(ki), klcli::max_of(ki), KL_PNG_CONTINUOUS);
+      }
+      if (kl_write_kernel_info("./out/kernels/kernel_info.txt", 2 * Nx + 1, 2 * Ny + 1, nk, scales.data()) != KL_OK)
+        std::exit(1);
+    }
+  }
+
+  klcli::banner_section("Starting calcImage...");
+  int img_rc = KL_OK;
+  {
+    std::vector<float> img((size_t)Lx * Ly);
+    const bool pow2 = (Lx & (Lx - 1)) == 0 && (Ly & (Ly - 1)) == 0;
+    if (precision == KL_PREC_FP64 && pow2) {
+      kl_tcc_plan plan64 = nullptr;
+      img_rc = kl_tcc_plan_create(&plan64, src.data(), srcSize, NA, defocus, n_medium, Lx, Ly, KL_PREC_FP64);
+      if (img_rc == KL_OK) img_rc = kl_fp64_hopkins_image_host(plan64, msk.data(), img.data());
+      if (plan64) kl_tcc_plan_destroy(plan64);
+    } else {
+      if (precision == KL_PREC_FP64)
+        std::cerr << "Note: the FP64 Hopkins image needs power-of-two periods; using the fast path." << std::endl;
+      img_rc = kl_hopkins_image_host(plan, msk.data(), img.data());
+    }
+    if (img_rc != KL_OK) {
+      std::cerr << "Error: calcImage failed: " << kl_last_error() << std::endl;
+    } else {
+      const float mx = klcli::max_of(img), mn = klcli::min_of(img);
+      std::cout << "Max. Intensity: " << mx << std::endl;
+      if (kl_write_float_file("./out/image.bin", img.data(), Lx * Ly) != KL_OK) std::exit(1);
+      klcli::png("./out/image.png", img, Lx, Ly, mn, mx, KL_PNG_CONTINUOUS);
+      klcli::png("./out/image_s.png", img, Lx, Ly, 0.0f, kTargetIntensity, KL_PNG_7COLORS);
+    }
+  }
+
+  if (nk > 0) {
+    klcli::banner_section("Starting calcKernels...");
+    std::cout << "Solving eigenproblem..." << std::endl;
+    if (eig_rc != KL_OK) {
+      std::cerr << "Kernels derivation failed with info = " << eig_rc << " (" << eig_err << ")" << std::endl;
+      kl_tcc_plan_destroy(plan);
       return 1;
     }
     std::cout << "Eigenvalues: " << std::endl;
     for (int j = 0; j < nk; ++j) std::cout << ev[j] << " ";
     std::cout << std::endl;
-    for (int i = 0; i < nk; ++i) {
-      const std::string b = "./out/kernels/krn_" + std::to_string(i);
-      if (kl_write_float_file((b + "_r.bin").c_str(), kre.data() + (size_t)i * tccSize, tccSize) != KL_OK ||
-          kl_write_float_file((b + "_i.bin").c_str(), kim.data() + (size_t)i * tccSize, tccSize) != KL_OK)
-        std::exit(1);
-      const std::vector<float> kr(kre.begin() + (size_t)i * tccSize, kre.begin() + (size_t)(i + 1) * tccSize);
-      const std::vector<float> ki(kim.begin() + (size_t)i * tccSize, kim.begin() + (size_t)(i + 1) * tccSize);
-      const std::string pb = "./out/kernels/png/krn_" + std::to_string(i);
-      klcli::png(pb + "_r.png", kr, 2 * Nx + 1, 2 * Ny + 1, klcli::min_of(kr), klcli::max_of(kr), KL_PNG_CONTINUOUS);
-      klcli::png(pb + "_i.png", ki, 2 * Nx + 1, 2 * Ny + 1, klcli::min_of(ki), klcli::max_of(ki), KL_PNG_CONTINUOUS);
-    }
-    if (kl_write_kernel_info("./out/kernels/kernel_info.txt", 2 * Nx + 1, 2 * Ny + 1, nk, scales.data()) != KL_OK)
-      std::exit(1);
-    if (plan64) kl_tcc_plan_destroy(plan64);
+  }
+  if (img_rc != KL_OK) {
+    kl_tcc_plan_destroy(plan);
+    return 1;
   }
   kl_tcc_plan_destroy(plan);
   klcli::banner_end(start);

@@ -96,13 +96,10 @@ def read_kernel_dir(d):
     return kx, ky, np.array(ks), sc
 
 
-@pytest.mark.gpu
-def test_tcc_cli_matches_reference_program(tmp_path, ref_built):
-    L, ms = 512, 256
-    mask = synth.rect_mask(ms, 12, seed=21)
-    mfile = tmp_path / "mask.bin"
-    mask.astype(np.float32).tofile(mfile)
-    args = tcc_args(L, ms, str(mfile))
+def run_both_tcc(tmp_path, args, Lx, Ly, pngs=True):
+    """Run klitho_tcc with `args` through the reference build and the drop-in;
+    compare image.bin (1e-5 of clear field), the console's parameter block,
+    kernel_info.txt and the kernels as weighted projectors."""
     dref, dours = workdir(tmp_path, "ref"), workdir(tmp_path, "ours")
     rr = run(os.path.join(REFBIN, "klitho_tcc"), args, dref)
     ro = run(os.path.join(BIN, "klitho_tcc"), args, dours)
@@ -115,7 +112,7 @@ def test_tcc_cli_matches_reference_program(tmp_path, ref_built):
         assert lr == lo, (key, lr, lo)
     ir = np.fromfile(dref / "out" / "image.bin", dtype=np.float32)
     io = np.fromfile(dours / "out" / "image.bin", dtype=np.float32)
-    assert ir.size == io.size == L * L
+    assert ir.size == io.size == Lx * Ly
     assert np.abs(ir - io).max() <= 1e-5
     kxr, kyr, kr, sr = read_kernel_dir(dref / "out" / "kernels")
     kxo, kyo, ko, so = read_kernel_dir(dours / "out" / "kernels")
@@ -129,14 +126,93 @@ def test_tcc_cli_matches_reference_program(tmp_path, ref_built):
     tr = (dref / "out" / "kernels" / "kernel_info.txt").read_text().splitlines()
     to = (dours / "out" / "kernels" / "kernel_info.txt").read_text().splitlines()
     assert len(tr) == len(to) and tr[:5] == to[:5]
-    # PNG outputs (common/file_io.cpp:7-135): identical inputs give identical pixels,
-    # images and TCC planes agree to the colour-map quantisation
-    compare_pngs(dref / "out", dours / "out", ["source.png", "mask.png"],
-                 ["image.png", "image_s.png", "tcc_r.png", "tcc_i.png"])
-    for i in range(len(so)):
-        for part in ("r", "i"):  # kernel phases are arbitrary: same size, valid PNG
-            a = read_png(dours / "out" / "kernels" / "png" / f"krn_{i}_{part}.png")
-            assert a.shape == (kyo, kxo, 3)
+    if pngs:
+        # PNG outputs (common/file_io.cpp:7-135): identical inputs give identical pixels,
+        # images and TCC planes agree to the colour-map quantisation
+        compare_pngs(dref / "out", dours / "out", ["source.png", "mask.png"],
+                     ["image.png", "image_s.png", "tcc_r.png", "tcc_i.png"])
+        for i in range(len(so)):
+            for part in ("r", "i"):  # kernel phases are arbitrary: same size, valid PNG
+                a = read_png(dours / "out" / "kernels" / "png" / f"krn_{i}_{part}.png")
+                assert a.shape == (kyo, kxo, 3)
+    return dref, dours
+
+
+@pytest.mark.gpu
+def test_tcc_cli_matches_reference_program(tmp_path, ref_built):
+    L, ms = 512, 256
+    mask = synth.rect_mask(ms, 12, seed=21)
+    mfile = tmp_path / "mask.bin"
+    mask.astype(np.float32).tofile(mfile)
+    run_both_tcc(tmp_path, tcc_args(L, ms, str(mfile)), L, L)
+
+
+# periods the reference accepts (klitho_tcc.cpp:391-429) beyond powers of two:
+# factors of 5, an odd period, non-square
+@pytest.mark.gpu
+@pytest.mark.parametrize("Lx,Ly,ms", [(1000, 1000, 512), (2000, 2000, 1024), (1024, 999, 512)])
+def test_tcc_cli_periods_match_reference(tmp_path, ref_built, Lx, Ly, ms):
+    mask = synth.rect_mask(ms, int(40 * (ms / 1024) ** 2) + 4, seed=Lx + Ly)
+    mfile = tmp_path / "mask.bin"
+    mask.astype(np.float32).tofile(mfile)
+    args = tcc_args(Lx, ms, str(mfile), nk=6)
+    args[1] = Ly
+    run_both_tcc(tmp_path, args, Lx, Ly, pngs=False)
+
+
+# the reference's own example command lines (K-Litho-TCC/test_tcc.sh:49,
+# K-Litho-SOCS/test_socs.sh:24): 2048 period, a 1024^2 imported mask (a seeded
+# synthetic one stands in for the absent T1.bin), 101^2 annular source, NA 0.8,
+# defocus 0.2, 3 kernels; then klitho_socs on the kernels klitho_tcc wrote and
+# on the kernel directory the reference ships
+@pytest.mark.gpu
+def test_reference_example_command_lines(tmp_path, ref_built):
+    mask = synth.rect_mask_fill(1024, seed=1, density=0.3)
+    mfile = tmp_path / "T1.bin"
+    mask.astype(np.float32).tofile(mfile)
+    args = [2048, 2048, 1024, 1024, "Import", 128, 128, 0, str(mfile), 101, "Annular", 0.6, 0.9, 0.1,
+            0.5, 1, 0.6, 0.2, "./source/src_test1_size101.bin", 0.8, 0.2, 3]
+    dref, dours = run_both_tcc(tmp_path, args, 2048, 2048, pngs=False)
+    for kd in (str(dref / "out" / "kernels") + "/", os.path.join(GOLDEN, "shipped_kernels") + "/"):
+        sargs = [2048, 2048, 1024, 1024, "Import", 128, 128, 0, str(mfile), kd]
+        sr, so = workdir(tmp_path, "sref" + str(len(kd))), workdir(tmp_path, "sours" + str(len(kd)))
+        rr = run(os.path.join(REFBIN, "klitho_socs"), sargs, sr)
+        ro = run(os.path.join(BIN, "klitho_socs"), sargs, so)
+        assert rr.returncode == 0, rr.stderr
+        assert ro.returncode == 0, ro.stderr
+        ir = np.fromfile(sr / "out" / "image.bin", dtype=np.float32)
+        io = np.fromfile(so / "out" / "image.bin", dtype=np.float32)
+        assert np.abs(ir - io).max() <= 1e-5 * max(float(np.abs(ir).max()), 1.0)
+
+
+# klitho_socs at periods only the general pipeline takes, including 4096
+@pytest.mark.gpu
+@pytest.mark.parametrize("Lx,Ly,ms", [(1000, 1000, 768), (2000, 2000, 1024), (4096, 4096, 2048),
+                                      (1001, 999, 640)])
+def test_socs_cli_periods_match_reference(tmp_path, ref_built, Lx, Ly, ms):
+    mask = synth.rect_mask(ms, int(40 * (ms / 1024) ** 2) + 4, seed=Lx)
+    mfile = tmp_path / "mask.bin"
+    mask.astype(np.float32).tofile(mfile)
+    src = K.createSource(41, "Annular", 0.6, 0.9)
+    plan = K.TccPlan(src, 1.35, synth.defocus_arg(25.0), Lx, Ly, n_medium=1.44)
+    krn, sc, _, _ = plan.topk(8)
+    kd = str(tmp_path / "kgen")
+    os.makedirs(kd)
+    for i in range(8):
+        krn[i].real.astype(np.float32).tofile(os.path.join(kd, f"krn_{i}_r.bin"))
+        krn[i].imag.astype(np.float32).tofile(os.path.join(kd, f"krn_{i}_i.bin"))
+    K.writeKernelInfo(os.path.join(kd, "kernel_info.txt"), 2 * plan.Nx + 1, 2 * plan.Ny + 1, sc)
+    args = [Lx, Ly, ms, ms, "Import", 128, 128, 0, str(mfile), kd + "/"]
+    dref, dours = workdir(tmp_path, "ref"), workdir(tmp_path, "ours")
+    env = {"KLITHO_PNG": "0"}
+    rr = run(os.path.join(REFBIN, "klitho_socs"), args, dref)
+    ro = run(os.path.join(BIN, "klitho_socs"), args, dours, env=env)
+    assert rr.returncode == 0, rr.stderr
+    assert ro.returncode == 0, ro.stderr
+    ir = np.fromfile(dref / "out" / "image.bin", dtype=np.float32)
+    io = np.fromfile(dours / "out" / "image.bin", dtype=np.float32)
+    assert ir.size == io.size == Lx * Ly
+    assert np.abs(ir - io).max() <= 1e-5 * max(float(np.abs(ir).max()), 1.0)
 
 
 @pytest.mark.gpu
