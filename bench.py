@@ -75,17 +75,40 @@ def make_masks(L, n, seed):
 
 
 class ClockSampler:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled during the timed region.
+
+    Polls NVML every few milliseconds from a thread (so that even a timed
+    region of some tens of milliseconds gets samples); falls back to
+    `nvidia-smi -lms 200` where NVML cannot be loaded.  Only reads state."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
-    def __init__(self, dev_index=0):
+    def __init__(self, dev_index=0, period_s=0.004):
         self.dev = dev_index
+        self.period = period_s
         self.proc = None
+        self.th = None
         self.lines = []
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
+        self._run = False
+        self._nvml = None
 
     def start(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.dev)
+            self._nvml = (pynvml, h)
+            self._smax = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self._run = True
+            self.th = threading.Thread(target=self._poll, daemon=True)
+            self.th.start()
+            return
+        except Exception:
+            self._nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.Q}",
@@ -96,11 +119,33 @@ class ClockSampler:
         except OSError:
             self.proc = None
 
+    def _poll(self):
+        pynvml, h = self._nvml
+        while self._run:
+            try:
+                sm = float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM))
+                rs = int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))
+                self.samples.append((sm, self._smax, rs))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
     def _read(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
 
+    def clear(self):
+        self.lines.clear()
+        self.samples.clear()
+
     def stop(self):
+        if self._nvml is not None:
+            self._run = False
+            self.th.join(timeout=2)
+            sm = [x[0] for x in self.samples]
+            reasons = sorted(nm for nm, bit in self.REASONS.items() if any(x[2] & bit for x in self.samples))
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self._smax,
+                    "reasons": reasons, "samples": len(sm), "source": "NVML polled every 4 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -124,7 +169,7 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": float(max(smax)) if smax else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi -lms 200"}
 
 
 def dist_setup():
@@ -152,8 +197,23 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     stream = torch.cuda.current_stream()
+    if ws > 1:
+        print(f"[bench] rank {rank} of {ws} on cuda:{local}, communicator nccl "
+              f"(world size {dist.get_world_size()}), {args.scaling} scaling", file=sys.stderr)
 
-    # weak scaling: every rank images its own full batch (clips are independent)
+    # weak scaling: every rank images its own full batch (clips are independent);
+    # strong scaling: the one batch is split over the ranks by shard.partition
+    # (clips balanced by pixels), no collective on the data path
+    full_px = sum(L * L * n * len(FOCUS_NM) for L, n in CLASSES)
+    if args.scaling == "strong" and ws > 1:
+        import shard
+        sizes, cls_of = [], []
+        for ci, (L, n) in enumerate(CLASSES):
+            sizes += [L * L] * n
+            cls_of += [ci] * n
+        mine = shard.partition(sizes, ws)[rank]
+        counts = [sum(1 for i in mine if cls_of[i] == ci) for ci in range(len(CLASSES))]
+        CLASSES[:] = [(L, c) for (L, _), c in zip(CLASSES, counts) if c > 0]
     # kernel sets: config-0 optics (annular 0.6/0.9 on 41^2, NA 1.35, water) at
     # each clip size and focus, K=24, from the GPU TCC + subspace iteration
     src = K.createSource(41, "Annular", 0.6, 0.9)
@@ -209,8 +269,7 @@ def run_ours(args):
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
-    time.sleep(0.5)  # let the sampler start before the timed region
-    clocks.lines.clear()
+    clocks.clear()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -261,7 +320,9 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     ms_per_step = ms / args.steps
-    value = img_equiv * ws / (ms_per_step / 1e3)
+    # whole-job rate: every rank's pixels over the slowest rank's time
+    total_equiv = (full_px / float(1024 * 1024)) if (args.scaling == "strong" and ws > 1) else img_equiv * ws
+    value = total_equiv / (ms_per_step / 1e3)
 
     # roofline of the dominant kernel (largest share of device time)
     names = ["socs_forward", "socs_spectral", "socs_inverse"]
@@ -303,7 +364,7 @@ def run_ours(args):
             other[names[i]]["frac_of_peak"] = round(bw / peak, 4)
 
     # end-to-end through the host entry point (pinned host buffers)
-    e2e = None if args.no_e2e else run_e2e(plans, masks_h, args, ws, img_equiv)
+    e2e = None if args.no_e2e else run_e2e(plans, masks_h, args, total_equiv / img_equiv, img_equiv)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -311,7 +372,7 @@ def run_ours(args):
 
     fp64 = None
     if not args.no_secondary:
-        fp64 = fp64_baseline(masks_d, kset0, value / ws, img_equiv)
+        fp64 = fp64_baseline(masks_d, imgs_d, kset0, value / ws, img_equiv)
 
     batch.close()
     for bp in bplans:
@@ -324,6 +385,10 @@ def run_ours(args):
         del masks_d, imgs_d
         torch.cuda.empty_cache()
         secondary["fwd_adj"] = bench_fwd_adj(args, stream, peaks()[0])
+        secondary["socs_4096"] = bench_socs_4096(args, stream, peaks()[0])
+        torch.cuda.empty_cache()
+        secondary["fwd_adj_4096"] = bench_fwd_adj_4096(args, stream, peaks()[0])
+        torch.cuda.empty_cache()
         secondary["tcc_eigen"] = bench_tcc_eigen(args)
         secondary["tcc_eigen_large"] = bench_tcc_eigen_large(args)
         secondary["tcc_gemm"] = bench_tcc_gemm(args)
@@ -332,7 +397,8 @@ def run_ours(args):
         out = {
             "metric": METRIC, "value": round(value, 2), "unit": UNIT, "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": args.scaling if ws > 1 else "weak", "vs_baseline": None,
+            "dtype": "f32",
             "data": "synthetic (seeded random-rectangle masks; kernels from the GPU TCC + "
                     "subspace iteration of the annular NA 1.35 optics, K=24 per size and focus)",
             "config": {"workload": "batched SOCS forward: 128x512^2 + 192x1024^2 + 64x2048^2 "
@@ -340,8 +406,10 @@ def run_ours(args):
                        "clips_per_gpu": sum(n for _, n in CLASSES), "focus_nm": FOCUS_NM,
                        "image_equiv_1024_per_step_per_gpu": img_equiv,
                        "l2": "inputs larger than L2 (1.9 GB masks, 5.8 GB images per GPU)",
-                       "parallelism": f"clip sharding, {ws} GPU(s), no collective on the data path"},
+                       "parallelism": f"clip sharding ({args.scaling if ws > 1 else 'weak'}), {ws} GPU(s), "
+                                      f"no collective on the data path"},
             "roofline": roof, "stages": other, "per_class": per_class, "graph_branches": branches,
+            "image_err_vs_fp64_of_clear_field": (fp64 or {}).get("image_max_err_of_clear_field"),
             "clocks": clk, "e2e": e2e,
             "gpu_launches": int(3 * len(bplans) * args.steps),
             "cpu_baseline": cpu,
@@ -363,16 +431,24 @@ TRAFFIC_PER_ALGORITHMIC_BYTE = {"socs_inverse": (3.376 + 544.117 + 4.802 + 749.6
                                 "socs_forward": (201.372 + 4.389) / 201.33}
 
 
-def fp64_baseline(masks_d, kset0, value_per_gpu, img_equiv):
+def clear_field(krn, sc, Nx, Ny):
+    """Clear-field intensity of a kernel set: sum_k lambda_k |H_k(0)|^2."""
+    c = (2 * Ny + 1) * (2 * Nx + 1) // 2
+    return float(np.sum(np.asarray(sc, np.float64) * np.abs(np.asarray(krn)[:, c].astype(np.complex128)) ** 2))
+
+
+def fp64_baseline(masks_d, imgs_d, kset0, value_per_gpu, img_equiv):
     """The plain FP64 GPU path (kl_fp64_socs_forward: full FP64 FFTs, K fields
     materialised) on 8 clips of each size class (4 of 2048^2) with one kernel
     set, timed with CUDA events after a warm-up call; its 1024^2-equivalent
     rate for the same mixed workload (every clip x every focus) is the
-    baseline of the fused path."""
+    baseline of the fused path.  The same FP64 images give the error of the
+    timed workload's images (kernel set 0) as max |fused - FP64| over the
+    clear-field intensity."""
     import torch
     import klitho as K
-    t_clip = []
-    for (L, n), md, (krn, sc) in zip(CLASSES, masks_d, kset0):
+    t_clip, errs = [], []
+    for (L, n), md, im, (krn, sc) in zip(CLASSES, masks_d, imgs_d, kset0):
         Nx, Ny = class_band(L)
         kd = torch.from_numpy(np.stack([krn.real, krn.imag], -1).astype(np.float32).copy()).cuda()
         sd = torch.from_numpy(np.asarray(sc, dtype=np.float32)).cuda()
@@ -388,11 +464,15 @@ def fp64_baseline(masks_d, kset0, value_per_gpu, img_equiv):
         e1.record()
         torch.cuda.synchronize()
         t_clip.append(e0.elapsed_time(e1) / (2 * nf) / 1e3)
+        cf = clear_field(krn, sc, Nx, Ny)
+        errs.append(float((im[:nf, 0].double() - out).abs().max()) / cf)
         del out
     step_s = sum(t * n * len(FOCUS_NM) for t, (L, n) in zip(t_clip, CLASSES))
     rate = img_equiv / step_s
     return {"value": round(rate, 2), "unit": UNIT, "speedup_of_fused_path": round(value_per_gpu / rate, 2),
             "seconds_per_clip": {str(L): round(t, 6) for t, (L, n) in zip(t_clip, CLASSES)},
+            "image_max_err_of_clear_field": max(errs) if errs else None,
+            "image_err_per_class": {str(L): e for e, (L, n) in zip(errs, CLASSES)},
             "sample": "8 clips per size class (4 of 2048^2), one focus, 2 passes after a warm-up call, "
                       "CUDA events; step time = sum over classes of clips x focus x seconds per clip"}
 
@@ -463,6 +543,211 @@ def bench_fwd_adj(args, stream, peak_gbs):
             "gpu_launches_per_step": 6}
 
 
+QUAD4096 = dict(srcSize=81, kind="CrossQuadrupole", radius=0.12, offset=0.75)
+FOCUS4096_NM = [-50.0, -25.0, 0.0, 25.0, 50.0]
+
+
+def quad4096_kernels(nk=64):
+    """K kernels per focus of the stress configuration (4096^2, cross-quadrupole
+    0.75/0.12 on 81^2, NA 1.35 water) from the library's TCC + eigen path."""
+    import klitho as K
+    import synth
+    src = K.createSource(81, "CrossQuadrupole", radius=0.12, offset=0.75)
+    sets = []
+    for f_nm in FOCUS4096_NM:
+        tp = K.TccPlan(src, 1.35, synth.defocus_arg(f_nm), 4096, 4096, n_medium=synth.N_WATER)
+        krn, sc, _, _ = tp.topk(nk)
+        Nx, Ny = tp.Nx, tp.Ny
+        tp.close()
+        sets.append((krn, sc))
+    return src, Nx, Ny, sets
+
+
+def smooth_masks_gpu(L, n, seed, sigma_px=12.0, gain=6.0):
+    """Continuous masks in [0, 1] (Gaussian-filtered noise through a sigmoid,
+    the construction of synth.smooth_mask) generated on the device, so that
+    4096^2 inputs take no CPU minutes; setup only, never timed."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    f = torch.fft.fftfreq(L, dtype=torch.float64, device="cuda")
+    filt = torch.exp(-2.0 * (np.pi * sigma_px) ** 2 * (f[:, None] ** 2 + f[None, :] ** 2))
+    out = torch.empty((n, L, L), dtype=torch.float32, device="cuda")
+    for i in range(n):
+        noise = torch.randn((L, L), generator=g, dtype=torch.float64).cuda()
+        sm = torch.fft.ifft2(torch.fft.fft2(noise) * filt).real
+        sm /= sm.std() + 1e-30
+        out[i] = torch.sigmoid(gain * sm).float()
+    return out
+
+
+def stage_report(plan):
+    t, c = plan.stage_times()
+    return [x / max(n, 1) for x, n in zip(t, c)]
+
+
+def bench_socs_4096(args, stream, peak_gbs):
+    """Stress configuration, forward: 16 seeded 4096^2 random-rectangle clips
+    (25-40 % density) at 5 focus values, K = 64 kernels per focus (N = 11449,
+    SOCS grid 213: the general pipeline).  A step images every clip at every
+    focus; algorithmic traffic 4 B per mask pixel + 4 B per image pixel.  The
+    error of clip 0 at focus 0 against the plain FP64 GPU path
+    (kl_fp64_socs_forward) is reported as a fraction of clear field, and that
+    path's time per image is the baseline."""
+    import torch
+    import klitho as K
+    L, n, nk = 4096, (args.clips if args.part == "socs_4096" and args.clips else 16), 64
+    nf = len(FOCUS4096_NM)
+    _, Nx, Ny, sets = quad4096_kernels(nk)
+    plan = K.SocsPlan(L, L, Nx, Ny, nk, nsets=nf, max_clips=n)
+    for i, (k, sc) in enumerate(sets):
+        plan.set_kernels(i, k, sc)
+    masks = torch.from_numpy(make_masks(L, n, SEED + 4096)).cuda()
+    imgs = torch.empty((n, nf, L, L), dtype=torch.float32, device="cuda")
+    for _ in range(3):
+        plan.forward(masks, imgs, stream=stream)
+    torch.cuda.synchronize()
+    steps = max(3, min(args.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.forward(masks, imgs, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    plan.enable_timing(True)
+    for _ in range(3):
+        plan.forward(masks, imgs, stream=stream)
+    st = stage_report(plan)
+    plan.enable_timing(False)
+    px = L * L
+    bytes_step = 4 * px * n + 4 * px * n * nf
+    gbs = bytes_step / (ms / 1e3) / 1e9
+    syn_gbs = 4 * px * n * nf / (st[2] / 1e3) / 1e9
+    # FP64 GPU path on clip 0, focus 0
+    krn, sc = sets[2]
+    kd = torch.from_numpy(np.stack([krn.real, krn.imag], -1).astype(np.float32).copy()).cuda()
+    sd = torch.from_numpy(np.asarray(sc, dtype=np.float32)).cuda()
+    out = torch.empty((1, L, L), dtype=torch.float64, device="cuda")
+    K.fp64_socs_forward(masks[:1], Nx, Ny, kd, sd, out)
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    K.fp64_socs_forward(masks[:1], Nx, Ny, kd, sd, out)
+    f1.record()
+    torch.cuda.synchronize()
+    t64 = f0.elapsed_time(f1) / 1e3
+    err = float((imgs[0, 2].double() - out[0]).abs().max()) / clear_field(krn, sc, Nx, Ny)
+    plan.close()
+    del masks, imgs, out
+    rate = n * nf / (ms / 1e3)
+    return {"metric": "4096^2 SOCS images/s (16 clips x 5 focus, K=64)", "value": round(rate, 2),
+            "unit": "images/s", "ms_per_step": round(ms, 3), "clips": n, "focus": nf, "K": nk,
+            "N": (2 * Nx + 1) * (2 * Ny + 1), "engine": "general",
+            "GBps_algorithmic": round(gbs, 1), "frac_of_hbm_peak": round(gbs / peak_gbs, 4),
+            "stage_ms": {"row_and_column_forward": round(st[0], 4), "spectral": round(st[1], 4),
+                         "column_and_row_synthesis": round(st[2], 4)},
+            "synthesis_GBps": round(syn_gbs, 1), "synthesis_frac_of_hbm_peak": round(syn_gbs / peak_gbs, 4),
+            "image_max_err_of_clear_field_vs_fp64": err,
+            "fp64_gpu_images_per_s": round(1.0 / t64, 3), "speedup_vs_fp64_gpu": round(rate * t64, 2),
+            "timing": f"CUDA events over {steps} steps after 3 warm-up steps; stages from per-launch events"}
+
+
+def bench_fwd_adj_4096(args, stream, peak_gbs):
+    """Stress configuration, forward + adjoint: 16 seeded 4096^2 continuous
+    clips (smooth noise through a sigmoid) with binary rectangle targets at 5
+    focus values, K = 64; loss sum over focus of
+    sum (sigmoid(50 (I - 0.225)) - target)^2, gradient dL/dmask summed over
+    focus.  Algorithmic traffic per clip pixel: mask, target read and gradient
+    written (12 B) plus 4 B per image pixel written.  Checked against the plain
+    FP64 GPU path (kl_fp64_socs_vjp, clip 0, the 5 focus values summed)."""
+    import torch
+    import klitho as K
+    import synth
+    L, n, nk = 4096, (args.clips if args.part == "fwd_adj_4096" and args.clips else 16), 64
+    nf = len(FOCUS4096_NM)
+    _, Nx, Ny, sets = quad4096_kernels(nk)
+    plan = K.SocsPlan(L, L, Nx, Ny, nk, nsets=nf, max_clips=n, adjoint=True)
+    for i, (k, sc) in enumerate(sets):
+        plan.set_kernels(i, k, sc)
+    masks = smooth_masks_gpu(L, n, SEED + 44)
+    rng = np.random.default_rng(SEED + 45)
+    tgts = torch.from_numpy(np.stack([synth.rect_mask_fill(L, int(rng.integers(1 << 30)), 0.3)
+                                      for _ in range(n)])).cuda()
+    grad = torch.empty_like(masks)
+    imgs = torch.empty((n, nf, L, L), dtype=torch.float32, device="cuda")
+    loss = torch.empty(n * nf, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        plan.vjp(masks, tgts, grad, loss, imgs, stream=stream)
+    torch.cuda.synchronize()
+    steps = max(3, min(args.steps, 10))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        plan.vjp(masks, tgts, grad, loss, imgs, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    px = L * L
+    bytes_step = 12 * px * n + 4 * px * n * nf
+    gbs = bytes_step / (ms / 1e3) / 1e9
+    # FP64 GPU adjoint of clip 0 for each focus, summed
+    g64 = torch.zeros((1, L, L), dtype=torch.float64, device="cuda")
+    l64 = torch.empty(1, dtype=torch.float64, device="cuda")
+    gk = torch.empty((1, L, L), dtype=torch.float64, device="cuda")
+    t64 = 0.0
+    for i, (krn, sc) in enumerate(sets):
+        kd = torch.from_numpy(np.stack([krn.real, krn.imag], -1).astype(np.float32).copy()).cuda()
+        sd = torch.from_numpy(np.asarray(sc, dtype=np.float32)).cuda()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        K.fp64_socs_vjp(masks[:1], tgts[:1], Nx, Ny, kd, sd, gk, l64)
+        f1.record()
+        torch.cuda.synchronize()
+        t64 += f0.elapsed_time(f1) / 1e3
+        g64 += gk
+    gerr = float((grad[:1].double() - g64).abs().max() / g64.abs().max())
+    plan.close()
+    del masks, tgts, grad, imgs, g64, gk
+    rate = n * nf / (ms / 1e3)
+    fp64_rate = nf / t64
+    return {"metric": "4096^2 fwd+adj (clip, focus) pairs/s (16 clips x 5 focus, K=64)", "value": round(rate, 2),
+            "unit": "pairs/s", "ms_per_step": round(ms, 3), "clips": n, "focus": nf, "K": nk,
+            "GBps_algorithmic": round(gbs, 1), "frac_of_hbm_peak": round(gbs / peak_gbs, 4),
+            "grad_max_err_vs_fp64_rel": gerr, "fp64_gpu_pairs_per_s": round(fp64_rate, 3),
+            "speedup_vs_fp64_gpu": round(rate / fp64_rate, 2),
+            "fp64_sample": "clip 0 at the 5 focus values (kl_fp64_socs_vjp, first calls incl. set-up)",
+            "timing": f"CUDA events over {steps} steps after 3 warm-up steps"}
+
+
+def subspace_report(k_fast, k_ref, ev_ref):
+    """Kernels of two eigensolves compared as subspaces: the largest principal
+    angle (radians) at every cut m < K where the spectrum has a gap
+    ((lambda_m-1 - lambda_m) / lambda_0 > 1e-4; inside near-degenerate
+    clusters the basis is arbitrary), and the weighted projectors
+    sum lambda v v^H (relative Frobenius error)."""
+    A = np.asarray(k_fast, dtype=np.complex128).T
+    B = np.asarray(k_ref, dtype=np.complex128).T
+    ev = np.asarray(ev_ref, dtype=np.float64)
+    qa, _ = np.linalg.qr(A)
+    qb, _ = np.linalg.qr(B)
+    cuts, worst = [], 0.0
+    for m in range(1, A.shape[1]):
+        if (ev[m - 1] - ev[m]) / ev[0] > 1e-4:
+            sv = np.linalg.svd(qa[:, :m].conj().T @ qb[:, :m], compute_uv=False)
+            ang = float(np.arccos(np.clip(sv.min(), -1.0, 1.0)))
+            cuts.append((m, ang))
+            worst = max(worst, ang)
+    # weighted projectors through the K x K Gram products (no N x N matrices)
+    w = np.sqrt(np.maximum(ev, 0))
+    Aw, Bw = A * w[None, :], B * w[None, :]
+    aa, bb, ab = Aw.conj().T @ Aw, Bw.conj().T @ Bw, Aw.conj().T @ Bw
+    diff2 = np.real(np.trace(aa @ aa) + np.trace(bb @ bb) - 2 * np.trace(ab @ ab.conj().T))
+    rel = float(np.sqrt(max(diff2, 0.0)) / np.sqrt(np.real(np.trace(bb @ bb))))
+    return {"max_principal_angle_rad": worst, "gap_cuts": len(cuts),
+            "angles_at_cuts": [[m, a] for m, a in cuts[:64]], "weighted_projector_rel_err": rel}
+
+
 def bench_tcc_eigen(args):
     """TCC + top-K eigen at the larger field: 2048^2, dipole-X (0.7, 0.15) on a
     61^2 grid (98 source points), NA 1.35 water, K = 32, focus -50..50 nm in
@@ -497,7 +782,7 @@ def bench_tcc_eigen(args):
     w = K.TccPlan(src, 1.35, 0.0, L, L, n_medium=synth.N_WATER, precision=K.PREC_FP64)
     w.topk(nk)
     w.close()
-    fast_t, tcc_t, fp64_t, tcc_err, ev_err, its, fast_ev = [], [], [], [], [], [], []
+    fast_t, tcc_t, fp64_t, tcc_err, ev_err, its, fast_ev, subs = [], [], [], [], [], [], [], []
     fast_plan_t, fp64_plan_t = [], []
     for f_nm in focus:
         df = synth.defocus_arg(f_nm)
@@ -519,6 +804,7 @@ def bench_tcc_eigen(args):
         T64 = tq.build()
         tcc_err.append(float(torch.linalg.norm(T.double() - T64) / torch.linalg.norm(T64)))
         ev_err.append(float(np.max(np.abs(ev - ev64)) / np.max(np.abs(ev64))))
+        subs.append(subspace_report(krn, krn64, ev64))
         N = tp.N
         tp.close()
         tq.close()
@@ -543,6 +829,9 @@ def bench_tcc_eigen(args):
             "N": N, "S": int(K.sourcePointCount(src, K.getOuterSigma(src))), "focus_nm": focus,
             "jacobi_sweeps": its, "tcc_rel_frobenius_err_vs_fp64": max(tcc_err),
             "eigenvalue_rel_err_vs_fp64": max(ev_err), "sweep_vs_single_eigenvalue_dev": batch_dev,
+            "max_principal_angle_rad_vs_fp64": max(x["max_principal_angle_rad"] for x in subs),
+            "weighted_projector_rel_err_vs_fp64": max(x["weighted_projector_rel_err"] for x in subs),
+            "gap_cuts_checked": sum(x["gap_cuts"] for x in subs),
             "timing": "wall clock per focus (median of 5) incl. plan (source sampling, pupil factor), "
                       "eigen-solve and kernel download, synchronised; the TCC itself is not needed by "
                       "the fast eigensolve and is timed separately"}
@@ -584,6 +873,8 @@ def bench_tcc_eigen_large(args):
             tp.close()
             return r, N, S
         ((krn, sc, ev, it), N, S), t = timed(fast)
+        if f_nm == focus[2]:
+            fast_k0 = krn
         fast_t.append(t)
         its.append(it)
         evs.append(ev)
@@ -596,11 +887,15 @@ def bench_tcc_eigen_large(args):
         return r
     (k64, s64, ev64, it64), t64 = timed(fp64)
     f = float(np.median(fast_t))
+    sub = subspace_report(fast_k0, k64, ev64)
     return {"metric": "TCC + top-K eigen seconds per focus (4096^2 cross-quadrupole, K=64)",
             "fast_s": round(f, 4), "fast_s_each": [round(x, 4) for x in fast_t],
             "fp64_gpu_s": round(t64, 4), "speedup_vs_fp64_gpu": round(t64 / f, 2),
             "N": N, "S": S, "subspace_iterations": its, "fp64_iterations": it64,
             "eigenvalue_rel_err_vs_fp64": float(np.max(np.abs(evs[2] - ev64)) / np.max(np.abs(ev64))),
+            "max_principal_angle_rad_vs_fp64": sub["max_principal_angle_rad"],
+            "weighted_projector_rel_err_vs_fp64": sub["weighted_projector_rel_err"],
+            "gap_cuts_checked": sub["gap_cuts"],
             "timing": "wall clock per focus incl. plan, eigen-solve and kernel download, after a warm-up "
                       "solve of each path; FP64 at focus 0 only"}
 
@@ -760,6 +1055,10 @@ def run_part(args):
     torch.cuda.set_device(0)
     if args.part == "fwd_adj":
         r = bench_fwd_adj(args, torch.cuda.current_stream(), peaks()[0])
+    elif args.part == "socs_4096":
+        r = bench_socs_4096(args, torch.cuda.current_stream(), peaks()[0])
+    elif args.part == "fwd_adj_4096":
+        r = bench_fwd_adj_4096(args, torch.cuda.current_stream(), peaks()[0])
     elif args.part == "tcc_eigen_large":
         r = bench_tcc_eigen_large(args)
     elif args.part == "tcc_gemm":
@@ -767,6 +1066,25 @@ def run_part(args):
     else:
         r = bench_tcc_eigen(args)
     print(json.dumps(r))
+
+
+def spawn_ranks(args):
+    """`--gpus N` outside a launcher: start N ranks (one process per GPU) with
+    torch.distributed.run on this node, bounded by a timeout; fails loudly when
+    fewer GPUs are visible."""
+    import socket
+    import torch
+    have = torch.cuda.device_count()
+    if have < args.gpus:
+        raise SystemExit(f"bench.py: --gpus {args.gpus} requested but {have} GPU(s) visible")
+    sk = socket.socket()
+    sk.bind(("127.0.0.1", 0))
+    port = sk.getsockname()[1]
+    sk.close()
+    cmd = ["timeout", "-k", "60", "3600", sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={args.gpus}", "--master-addr", "127.0.0.1", f"--master-port={port}",
+           os.path.abspath(__file__)] + sys.argv[1:]
+    raise SystemExit(subprocess.call(cmd))
 
 
 def main():
@@ -786,11 +1104,17 @@ def main():
     ap.add_argument("--clips", type=int, default=0, help="clip count for --only")
     ap.add_argument("--chunks", type=int, default=1,
                     help="plans per size class (>= 1024^2) in the timed graph")
-    ap.add_argument("--part", choices=["all", "fwd_adj", "tcc_eigen", "tcc_eigen_large", "tcc_gemm"], default="all",
+    ap.add_argument("--scaling", choices=["weak", "strong"], default="weak",
+                    help="N > 1: every rank images its own batch (weak) or the batch is split (strong)")
+    ap.add_argument("--part", choices=["all", "fwd_adj", "socs_4096", "fwd_adj_4096", "tcc_eigen",
+                                       "tcc_eigen_large", "tcc_gemm"], default="all",
                     help="run one secondary measurement alone (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        spawn_ranks(args)
+        return
     if args.only:
         n = args.clips or dict(CLASSES).get(args.only, 16)
         CLASSES[:] = [(args.only, n)]

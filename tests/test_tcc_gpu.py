@@ -273,3 +273,51 @@ def test_topk_gram_size_boundaries(cuda, S):
     Pr = weighted_projector(kr[:n], er[:n])
     assert np.linalg.norm(weighted_projector(krn[:n], ev[:n]) - Pr) / np.linalg.norm(Pr) <= 1e-5
     assert 0 < it < 40
+
+
+def principal_angles_at_gaps(kf, kr, ev, rel_gap=1e-4):
+    """Largest principal angle between the spans of the first m kernels of two
+    solves, at every cut m where the reference spectrum has a gap."""
+    qa, _ = np.linalg.qr(np.asarray(kf, np.complex128).T)
+    qb, _ = np.linalg.qr(np.asarray(kr, np.complex128).T)
+    out = []
+    for m in range(1, qa.shape[1]):
+        if (ev[m - 1] - ev[m]) / ev[0] > rel_gap:
+            sv = np.linalg.svd(qa[:, :m].conj().T @ qb[:, :m], compute_uv=False)
+            out.append((m, float(np.arccos(np.clip(sv.min(), -1.0, 1.0)))))
+    return out
+
+
+def test_config4_fast_vs_fp64_gpu_path(cuda):
+    """The stress configuration (4096^2, cross-quadrupole 0.75/0.12 on 81^2,
+    NA 1.35 water: N = 11449, S = 196, K = 64): the fast path's TCC, eigenvalues
+    and kernels against the plain FP64 GPU path, which the tests above pin to
+    zheevr at sizes the CPU oracle handles.  Kernels are compared as weighted
+    projectors and by principal angles at every spectral-gap cut."""
+    import torch
+    src = K.createSource(81, "CrossQuadrupole", radius=0.12, offset=0.75)
+    df = synth.defocus_arg(25.0)
+    tf = K.TccPlan(src, 1.35, df, 4096, 4096, n_medium=1.44)
+    t64 = K.TccPlan(src, 1.35, df, 4096, 4096, n_medium=1.44, precision=K.PREC_FP64)
+    assert (tf.N, tf.S) == (11449, 196)
+    kf, sf, evf, _ = tf.topk(64)
+    k64, s64, ev64, _ = t64.topk(64)
+    assert np.max(np.abs(evf - ev64)) <= 1e-6 * ev64[0]
+    cuts = principal_angles_at_gaps(kf, k64, ev64)
+    assert len(cuts) >= 8
+    assert max(a for _, a in cuts) <= 1e-3, cuts
+    # weighted projectors through K x K Gram products
+    w = np.sqrt(np.maximum(ev64, 0))
+    A = np.asarray(kf, np.complex128).T * w[None, :]
+    B = np.asarray(k64, np.complex128).T * w[None, :]
+    aa, bb, ab = A.conj().T @ A, B.conj().T @ B, A.conj().T @ B
+    d2 = np.real(np.trace(aa @ aa) + np.trace(bb @ bb) - 2 * np.trace(ab @ ab.conj().T))
+    assert np.sqrt(max(d2, 0.0)) <= 1e-5 * np.sqrt(np.real(np.trace(bb @ bb)))
+    # the materialised TCC: tcgen05 BF16x3 against the FP64 accumulation
+    Tf = tf.build()
+    T64 = t64.build()
+    num = torch.linalg.norm(Tf.double() - T64)
+    assert float(num / torch.linalg.norm(T64)) <= 3e-5
+    del Tf, T64
+    tf.close()
+    t64.close()

@@ -81,6 +81,35 @@ def test_vjp_central_differences(cuda):
     assert np.abs(fd - gpu).max() <= 2e-3 * np.abs(fd).max()
 
 
+def test_vjp_central_differences_config3(cuda):
+    """The differentiable-SOCS configuration's clip: 1024^2, K = 24 physical
+    kernels, continuous mask, binary target; central differences of the FP64
+    loss (torch's FP64 FFTs on the GPU) at 64 random pixels where the
+    gradient is not negligible."""
+    L = 1024
+    _, Nx, Ny, krn, sc, _ = kernels(L, 24)
+    mask = synth.smooth_mask(L, seed=31).astype(np.float64)
+    tgt = synth.rect_mask(L, 60, seed=32)
+    _, grad, _, _ = run_vjp(mask[None].astype(np.float32), tgt[None], [(krn, sc)], Nx, Ny, want_image=False)
+    _, g_ref, _, _ = O.socs_vjp_reference_chunked(mask, tgt, krn, sc, Nx, Ny, ALPHA, THR, device="cuda")
+    assert np.abs(grad[0] - g_ref).max() <= 1e-4 * np.abs(g_ref).max()
+    rng = np.random.default_rng(1024)
+    cand = np.argwhere(np.abs(g_ref) >= 0.05 * np.abs(g_ref).max())
+    pix = cand[rng.choice(len(cand), size=64, replace=False)]
+    h = 1e-3
+    fd, gpu = [], []
+    for y, x in pix:
+        mp = mask.copy()
+        mp[y, x] += h
+        mm = mask.copy()
+        mm[y, x] -= h
+        fd.append((O.socs_loss_chunked(mp, tgt, krn, sc, Nx, Ny, ALPHA, THR, device="cuda", chunk=24) -
+                   O.socs_loss_chunked(mm, tgt, krn, sc, Nx, Ny, ALPHA, THR, device="cuda", chunk=24)) / (2 * h))
+        gpu.append(grad[0, y, x])
+    fd, gpu = np.array(fd), np.array(gpu)
+    assert np.abs(fd - gpu).max() <= 2e-3 * np.abs(fd).max()
+
+
 def test_vjp_two_focus_sets_sum(cuda):
     L = 256
     _, Nx, Ny, k0, s0, _ = kernels(L, 10, 0.0)
