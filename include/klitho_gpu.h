@@ -239,7 +239,10 @@ int kl_socs_stage_times(kl_socs_plan plan, double* ms, int* launches);
  * comes from one static 8 MiB device array inside the library (about 38 clips
  * of 1024^2 per call; larger requests return KL_ERR_INVALID with the sizes in
  * kl_last_error).  The first call on each device looks up that array's
- * device address; make it before any stream capture.  Calls share the array,
+ * device address; make it before any stream capture.  The address is looked
+ * up again when the device's primary context has changed since (after a
+ * cudaDeviceReset); make the first call after such a reset outside a capture
+ * as well.  Calls share the array,
  * so calls that overlap on the GPU race and must be serialised by the
  * caller.  Same results as kl_socs_forward with one kernel set. */
 int kl_socs_forward_noalloc(const float* masks_dev, int nclips, int Lx, int Ly, int Nx, int Ny,

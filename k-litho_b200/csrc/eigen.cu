@@ -729,8 +729,9 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
             if (q < B) s_newdiag[lq] = nd;
             s_own[par][j] = make_int4(op, q < B ? oq : -1, lp, lq);
           }
-          for (int c = c0; c < c0 + kCl / 2; ++c)
-            push_rotation(rb, pb, &s_bar[bsel], e * g + j, u, (uint32_t)p | (uint32_t)q << 16, c);
+          if (!*(volatile int*)&s_fail)  // after a timeout no bytes go to barriers that may be unarmed
+            for (int c = c0; c < c0 + kCl / 2; ++c)
+              push_rotation(rb, pb, &s_bar[bsel], e * g + j, u, (uint32_t)p | (uint32_t)q << 16, c);
         }
         __syncwarp();
         if (k + 1 < nk) {
@@ -765,7 +766,9 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
         s_fail = 1;
       // the slot's next use (three steps on) is armed before this CTA's next
       // rotations leave, so no sender can complete bytes of an unarmed phase
-      if (tid == 0) mbar_arm(&s_bar[bsel], cluster_step_bytes(npairs));
+      // (not once this CTA has timed out: the slot's phase may not have completed,
+      // and a second arrival in one phase of a count-1 barrier is undefined)
+      if (tid == 0 && !*(volatile int*)&s_fail) mbar_arm(&s_bar[bsel], cluster_step_bytes(npairs));
       // W <- W U over the own pairs (row r, columns lp and lq; W is kept
       // column-major so that consecutive rows are consecutive words).  The own
       // pairs of a round's first step are written by the rotation warp just
@@ -812,8 +815,9 @@ __global__ void __cluster_dims__(kCl, 1, 1) __launch_bounds__(kClThreads, 1)
           }
           double4* rn = rotx + bnext * npairs;
           uint32_t* pn_ = pqx + bnext * npairs;
-          for (int c = c0; c < c0 + kCl / 2; ++c)
-            push_rotation(rn, pn_, &s_bar[bnext], e * g + j, u, (uint32_t)pn | (uint32_t)qn << 16, c);
+          if (!*(volatile int*)&s_fail)
+            for (int c = c0; c < c0 + kCl / 2; ++c)
+              push_rotation(rn, pn_, &s_bar[bnext], e * g + j, u, (uint32_t)pn | (uint32_t)qn << 16, c);
         }
       } else if (k == 0) {
         update_w();

@@ -21,28 +21,42 @@ namespace kl {
 static thread_local std::string t_err;
 void set_error(const std::string& msg) { t_err = msg; }
 
+// The library's own stream-ordered pool per device (cudaMemPoolCreate), which
+// keeps freed blocks (release threshold at its maximum) so repeated calls
+// neither synchronise nor allocate afresh.  The device's default pool -- the
+// host program's cudaMallocAsync -- is left as the program configured it.
 int scratch_alloc(void** p, size_t bytes, cudaStream_t st, const char* what) {
   static std::mutex mu;
-  static std::vector<int> pooled;  // devices whose default pool keeps freed memory
+  static std::vector<std::pair<int, cudaMemPool_t>> pools;
   int dev = 0;
   cudaGetDevice(&dev);
+  cudaMemPool_t pool = nullptr;
   {
     std::lock_guard<std::mutex> lock(mu);
-    if (std::find(pooled.begin(), pooled.end(), dev) == pooled.end()) {
-      cudaMemPool_t pool;
-      if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    for (auto& e : pools)
+      if (e.first == dev) pool = e.second;
+    if (!pool) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
         uint64_t keep = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools.emplace_back(dev, pool);
+      } else {
+        pool = nullptr;
+        set_error("scratch pool creation failed");
+        return KL_ERR_NOMEM;
       }
-      cudaGetLastError();
-      pooled.push_back(dev);
     }
   }
   *p = nullptr;
-  if (cudaMallocAsync(p, bytes ? bytes : 16, st) != cudaSuccess) {
-    cudaGetLastError();
+  const cudaError_t e = cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st);
+  if (e != cudaSuccess) {
     *p = nullptr;
-    set_error(std::string("device allocation failed (") + what + ", " + std::to_string(bytes) + " bytes)");
+    set_error(std::string("device allocation failed (") + what + ", " + std::to_string(bytes) +
+              " bytes): " + cudaGetErrorString(e));
     return KL_ERR_NOMEM;
   }
   return KL_OK;

@@ -177,8 +177,11 @@ int kl_tcc_build(kl_tcc_plan p, void* tcc_dev, void* stream) {
     kl::scratch_free(X2, st);
     return rc;
   }
-  KL_CUDA_TRY(cudaMemsetAsync(p->err, 0, sizeof(int), st));
-  rc = kl::tcc_split_operands(p->A, N, S, Kp, X1, X2, Y, st);
+  if (cudaMemsetAsync(p->err, 0, sizeof(int), st) != cudaSuccess) {
+    kl::set_error(std::string("kl_tcc_build: ") + cudaGetErrorString(cudaGetLastError()));
+    rc = KL_ERR_CUDA;
+  }
+  if (!rc) rc = kl::tcc_split_operands(p->A, N, S, Kp, X1, X2, Y, st);
   if (!rc) rc = kl::tcc_gemm_tc(X1, X2, Y, N, Kp, (float2*)tcc_dev, p->err, st);
   int herr = 0;
   if (!rc) {

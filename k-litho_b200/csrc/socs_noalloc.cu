@@ -15,6 +15,7 @@
 // (other streams, other host threads) race on it and must be serialised by
 // the caller.  Every scratch element is written before it is read within a
 // call, so no part of it has to start at zero.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -31,10 +32,14 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratch
 
 // Device address of g_noalloc_scratch per device.  In host code the symbol
 // name is only a host-side handle, never a device address, so the address is
-// looked up once per device with that device current.
+// looked up once per device with that device current.  The address belongs
+// to the device's primary context: it is remembered together with that
+// context and looked up again when the context is a new one (after a
+// cudaDeviceReset, for instance).
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
+CUcontext g_ctx[kMaxDevices] = {};
 
 int scratch_address(void** out) {
   int dev = 0;
@@ -44,7 +49,9 @@ int scratch_address(void** out) {
     return KL_ERR_INVALID;
   }
   std::lock_guard<std::mutex> lk(g_mu);
-  if (!g_addr[dev]) {
+  CUcontext ctx = nullptr;
+  cuCtxGetCurrent(&ctx);
+  if (!g_addr[dev] || !ctx || ctx != g_ctx[dev]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || !p) {
@@ -53,6 +60,8 @@ int scratch_address(void** out) {
       return KL_ERR_CUDA;
     }
     g_addr[dev] = p;
+    cuCtxGetCurrent(&ctx);  // the look-up made the primary context current
+    g_ctx[dev] = ctx;
   }
   *out = g_addr[dev];
   return KL_OK;

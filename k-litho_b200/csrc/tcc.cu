@@ -658,13 +658,15 @@ __global__ void k_minmax(const C* __restrict__ m, size_t n, double* __restrict__
 template <typename C>
 int minmax(const C* m, size_t n, double* out4, cudaStream_t st) {
   const int blocks = 296;
-  double* d = nullptr;
-  KL_CUDA_TRY(cudaMalloc(&d, sizeof(double) * 4 * blocks));
-  k_minmax<C><<<blocks, 256, 0, st>>>(m, n, d);
+  void* d = nullptr;
+  int rc = scratch_alloc(&d, sizeof(double) * 4 * blocks, st, "minmax partials");
+  if (rc) return rc;
+  k_minmax<C><<<blocks, 256, 0, st>>>(m, n, static_cast<double*>(d));
   std::vector<double> h(4 * blocks);
-  cudaError_t e = cudaMemcpyAsync(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, st);
+  scratch_free(d, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(d);
   if (e != cudaSuccess) {
     set_error(std::string("minmax: ") + cudaGetErrorString(e));
     return KL_ERR_CUDA;
