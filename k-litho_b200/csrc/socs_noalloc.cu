@@ -41,6 +41,23 @@ std::mutex g_mu;
 void* g_addr[kMaxDevices] = {};
 CUcontext g_ctx[kMaxDevices] = {};
 
+// cuCtxGetCurrent through the runtime's driver entry point (the library does
+// not link the driver library directly)
+CUcontext current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<Fn>(p);
+  }();
+  CUcontext c = nullptr;
+  if (fn) fn(&c);
+  return c;
+}
+
 int scratch_address(void** out) {
   int dev = 0;
   KL_CUDA_TRY(cudaGetDevice(&dev));
@@ -49,8 +66,7 @@ int scratch_address(void** out) {
     return KL_ERR_INVALID;
   }
   std::lock_guard<std::mutex> lk(g_mu);
-  CUcontext ctx = nullptr;
-  cuCtxGetCurrent(&ctx);
+  CUcontext ctx = current_context();
   if (!g_addr[dev] || !ctx || ctx != g_ctx[dev]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
@@ -60,8 +76,7 @@ int scratch_address(void** out) {
       return KL_ERR_CUDA;
     }
     g_addr[dev] = p;
-    cuCtxGetCurrent(&ctx);  // the look-up made the primary context current
-    g_ctx[dev] = ctx;
+    g_ctx[dev] = current_context();  // the look-up made the primary context current
   }
   *out = g_addr[dev];
   return KL_OK;
