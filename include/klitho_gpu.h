@@ -249,6 +249,21 @@ int kl_socs_forward_noalloc(const float* masks_dev, int nclips, int Lx, int Ly, 
                             const float* kernels_dev, const float* scales_dev, int nk,
                             float* images_dev, void* stream);
 
+/* Resist image and printed contour of nimg aerial images (Lx x Ly float32
+ * each, e.g. kl_socs_forward's output).  The reference uses its threshold
+ * TARGET_INTENSITY = 0.225 (K-Litho-TCC/klitho_tcc.cpp:442) only as the top
+ * of image_s.png's colour scale (:547); here it defines, per pixel,
+ *   resist_dev  = 1 / (1 + exp(-alpha (I - threshold)))   (the adjoint's resist model)
+ *   printed_dev = I >= threshold ? 1 : 0                   (bytes)
+ *   edges_dev   = 1 where a printed pixel has a 4-neighbour (periodic over the
+ *                 clip) that does not print: the contour of the pattern
+ * and edge_count_dev[i] the number of contour pixels of image i (unsigned
+ * 64-bit).  Any output may be NULL.  Device memory; stream-ordered; rows up to
+ * 5120 pixels. */
+int kl_resist_contour(const float* images_dev, int nimg, int Lx, int Ly, float alpha, float threshold,
+                      float* resist_dev, unsigned char* printed_dev, unsigned char* edges_dev,
+                      unsigned long long* edge_count_dev, void* stream);
+
 /* The band of FT_r2c (K-Litho-TCC/klitho_tcc.cpp:97-148): centred spectrum
  * scaled by 1/(Lx Ly), cropped to the kernel band; band_dev receives nclips
  * c64 arrays in the kernel layout.  Stream-ordered. */

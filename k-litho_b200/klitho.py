@@ -75,6 +75,8 @@ def lib() -> ctypes.CDLL:
         L.kl_socs_plan_create_ex.argtypes = L.kl_socs_plan_create.argtypes + [ctypes.c_int]
         L.kl_socs_plan_engine.argtypes = [_vp]
         L.kl_socs_plan_destroy.argtypes = [_vp]
+        L.kl_resist_contour.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                        ctypes.c_float, _vp, _vp, _vp, _vp, _vp]
         L.kl_socs_set_kernels.argtypes = [_vp, ctypes.c_int, _c_float_p, _c_float_p, _c_float_p]
         L.kl_socs_forward.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
         L.kl_socs_forward_host.argtypes = [_vp, _c_float_p, ctypes.c_int, _c_float_p, _vp]
@@ -462,6 +464,19 @@ class TccPlan:
         n = masks_dev.shape[0] if nclips is None else nclips
         check(lib().kl_hopkins_image(self._h, _dev_ptr(masks_dev), int(n), _dev_ptr(images_dev),
                                      _stream_ptr(stream)), "kl_hopkins_image")
+
+
+def resist_contour(images_dev, alpha: float = 50.0, threshold: float = 0.225, resist_dev=None,
+                   printed_dev=None, edges_dev=None, edge_count_dev=None, stream=None) -> None:
+    """Resist image, printed pattern and its contour of images (..., Ly, Lx)
+    float32 on the device (kl_resist_contour); outputs are optional tensors of
+    the same shape (float32 / uint8 / uint8) and edge_count_dev int64 per image."""
+    Ly, Lx = images_dev.shape[-2:]
+    n = images_dev.numel() // (Lx * Ly)
+    p = lambda t: _dev_ptr(t) if t is not None else None
+    check(lib().kl_resist_contour(_dev_ptr(images_dev), int(n), int(Lx), int(Ly), float(alpha),
+                                  float(threshold), p(resist_dev), p(printed_dev), p(edges_dev),
+                                  p(edge_count_dev), _stream_ptr(stream)), "kl_resist_contour")
 
 
 def fp64_socs_forward(masks_dev, Nx: int, Ny: int, kernels_dev, scales_dev, images_dev, stream=None) -> None:

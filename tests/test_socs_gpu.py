@@ -150,3 +150,32 @@ def test_socs_engine_choice(cuda):
     assert K.SocsPlan(1024, 1024, 13, 13, 2).engine == "specialised"
     assert K.SocsPlan(300, 300, 3, 3, 2).engine == "general"
     assert K.SocsPlan(1024, 1024, 13, 13, 2, general=True).engine == "general"
+
+
+def test_resist_contour_matches_numpy(cuda):
+    """kl_resist_contour on SOCS images: the sigmoid resist (the adjoint's
+    model), the printed pattern I >= TARGET_INTENSITY (klitho_tcc.cpp:442) and
+    its contour (printed pixels with a non-printing 4-neighbour, periodic)
+    against numpy on the same float32 images."""
+    import torch
+    krn, sc, Nx, Ny = physical_kernels(1024)
+    masks = np.stack([synth.rect_mask_fill(1024, seed=s, density=0.3) for s in (61, 62)])
+    img = gpu_images(masks, [(krn, sc)], Nx, Ny)[:, 0]
+    dev = torch.from_numpy(img.copy()).cuda()
+    res = torch.empty_like(dev)
+    pr = torch.empty(dev.shape, dtype=torch.uint8, device="cuda")
+    ed = torch.empty(dev.shape, dtype=torch.uint8, device="cuda")
+    cnt = torch.empty(2, dtype=torch.int64, device="cuda")
+    K.resist_contour(dev, 50.0, 0.225, res, pr, ed, cnt)
+    torch.cuda.synchronize()
+    want_r = 1.0 / (1.0 + np.exp(-50.0 * (img.astype(np.float64) - 0.225)))
+    assert np.abs(res.cpu().numpy() - want_r).max() <= 2e-6
+    p = img >= np.float32(0.225)
+    assert np.array_equal(pr.cpu().numpy().astype(bool), p)
+    nb = np.zeros_like(p)
+    for ax, sh in ((1, 1), (1, -1), (2, 1), (2, -1)):
+        nb |= ~np.roll(p, sh, axis=ax)
+    e = p & nb
+    assert np.array_equal(ed.cpu().numpy().astype(bool), e)
+    assert list(cnt.cpu().numpy()) == [int(e[i].sum()) for i in range(2)]
+    assert e.sum() > 1000  # the clips do print a pattern
