@@ -211,6 +211,45 @@ __device__ __forceinline__ void re_idft_reg(const float2 (&Z)[P], float (&out)[P
   }
 }
 
+// S[k] = sum_i v[i] e^{-2 pi i k i / P}, k in [0, P/2], any power-of-two P >= 1
+template <int P>
+__device__ __forceinline__ void rdft_any(const float (&v)[P], float2 (&S)[P / 2 + 1]) {
+  if constexpr (P == 1) {
+    S[0] = make_float2(v[0], 0.f);
+  } else {
+    rdft_reg<P>(v, S);
+  }
+}
+
+// out[i] = Re sum_{k=0}^{P/2} Y[k] e^{+2 pi i k i / P}, where Y holds the
+// Hermitian fold of a length-P spectrum Z: Y[0] = Z[0], Y[P/2] = Z[P/2],
+// Y[k] = Z[k] + conj Z[P-k] (so out = Re IDFT_P(Z)).  One P/2-point FFT;
+// accumulating Y instead of Z halves the registers of a row synthesis.
+template <int P>
+__device__ __forceinline__ void c2r_half(const float2 (&Y)[P / 2 + 1], float (&out)[P]) {
+  if constexpr (P == 1) {
+    out[0] = Y[0].x;
+  } else {
+    constexpr int H = P / 2;
+    float2 x[H];
+#pragma unroll
+    for (int k = 0; k < H; ++k) {
+      // F[k] and F[k+H] of the Hermitian spectrum F[k] = Y[k]/2 (0<k<H), F[P-k] = conj F[k]
+      const float2 a = k == 0 ? make_float2(Y[0].x, 0.f) : cscale(Y[k], 0.5f);
+      const float2 b = k == 0 ? make_float2(Y[H].x, 0.f) : cscale(cconj(Y[H - k]), 0.5f);
+      const float2 fe = cadd(a, b);
+      const float2 fo = cmul(csub(a, b), tw_const<P, +1>(k));
+      x[k] = make_float2(fe.x - fo.y, fe.y + fo.x);
+    }
+    fft_reg<H, +1>(x);
+#pragma unroll
+    for (int m = 0; m < H; ++m) {
+      out[2 * m] = x[m].x;
+      out[2 * m + 1] = x[m].y;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Warp FFT of length N = 32*R.  Input: v[j] = x[lane + 32 j].  Output:
 // v[q1] = X[q1 + R * brev5(lane)].  Twiddles are per lane, made once.

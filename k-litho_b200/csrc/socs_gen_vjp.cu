@@ -62,40 +62,6 @@ int check_launch(const char* what) {
 }
 }  // namespace
 
-// S[k] = sum_i v[i] e^{-2 pi i k i / P}, k in [0, P/2]  (as in socs_gen.cu)
-template <int P>
-__device__ __forceinline__ void rdft_any_v(const float (&v)[P], float2 (&S)[P / 2 + 1]) {
-  if constexpr (P == 1) {
-    S[0] = make_float2(v[0], 0.f);
-  } else {
-    rdft_reg<P>(v, S);
-  }
-}
-// out = Re IDFT_P of the Hermitian fold Y (as c2r_half in socs_gen.cu)
-template <int P>
-__device__ __forceinline__ void c2r_half_v(const float2 (&Y)[P / 2 + 1], float (&out)[P]) {
-  if constexpr (P == 1) {
-    out[0] = Y[0].x;
-  } else {
-    constexpr int H = P / 2;
-    float2 x[H];
-#pragma unroll
-    for (int k = 0; k < H; ++k) {
-      const float2 a = k == 0 ? make_float2(Y[0].x, 0.f) : cscale(Y[k], 0.5f);
-      const float2 b = k == 0 ? make_float2(Y[H].x, 0.f) : cscale(cconj(Y[H - k]), 0.5f);
-      const float2 fe = cadd(a, b);
-      const float2 fo = cmul(csub(a, b), tw_const<P, +1>(k));
-      x[k] = make_float2(fe.x - fo.y, fe.y + fo.x);
-    }
-    fft_reg<H, +1>(x);
-#pragma unroll
-    for (int m = 0; m < H; ++m) {
-      out[2 * m] = x[m].x;
-      out[2 * m + 1] = x[m].y;
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // row_vjp: Q rows -> image rows, resist, loss, dL/dI row DFT (written over Q)
 // ---------------------------------------------------------------------------
@@ -153,7 +119,7 @@ __global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const
         }
       }
       float o[PF];
-      c2r_half_v<PF>(Y, o);
+      c2r_half<PF>(Y, o);
       const int lp = lane + 32 * c;
       if (lp < V) {
 #pragma unroll
@@ -170,7 +136,7 @@ __global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const
         for (int i = 0; i < PF; ++i) o[i] = 0.f;
       }
       float2 S[HS];
-      rdft_any_v<PF>(o, S);
+      rdft_any<PF>(o, S);
 #pragma unroll
       for (int k = 0; k < HS; ++k) sb[k * 33 + lane] = S[k];
       __syncwarp();
