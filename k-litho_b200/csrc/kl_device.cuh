@@ -250,6 +250,30 @@ __device__ __forceinline__ void c2r_half(const float2 (&Y)[P / 2 + 1], float (&o
   }
 }
 
+// The columns fx = fxs + 32 t (t < kGenMaxFold, fx <= Nx) of band row r of a
+// kernel (row-major (2Ny+1) x (2Nx+1), 2Nx+1 <= 128), issued as independent
+// loads so that several are in flight at once.
+constexpr int kGenMaxFold = 4;
+__device__ __forceinline__ void gen_load_hrow(const float2* __restrict__ Hk, int r, int nbx, int Nx, int fxs,
+                                              float2 (&h)[kGenMaxFold]) {
+  const float2* hr = Hk + (size_t)r * nbx + Nx;
+#pragma unroll
+  for (int t = 0; t < kGenMaxFold; ++t) {
+    const int fx = fxs + 32 * t;
+    h[t] = fx <= Nx ? __ldg(hr + fx) : make_float2(0.f, 0.f);
+  }
+}
+
+// Coefficients b = lane + 32 t (t < 4, b < nbins <= 128) of one row of a
+// row-coefficient array, as independent loads.
+__device__ __forceinline__ void gen_load_qrow(const float2* __restrict__ qr, int nbins, int lane, float2 (&q)[4]) {
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    const int b = lane + 32 * t;
+    q[t] = b < nbins ? __ldg(qr + b) : make_float2(0.f, 0.f);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Warp FFT of length N = 32*R.  Input: v[j] = x[lane + 32 j].  Output:
 // v[q1] = X[q1 + R * brev5(lane)].  Twiddles are per lane, made once.

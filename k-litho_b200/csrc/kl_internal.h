@@ -112,6 +112,8 @@ struct GenGeom {
 };
 
 constexpr int kGenMaxSplit = 8;
+// the chunk twiddles of the row kernels are staged in shared memory up to 32 KB
+__host__ __device__ inline bool gen_t2_in_smem(const GenGeom& g) { return (size_t)g.nC * g.NBX * 8 <= 32 * 1024; }
 
 int gen_geometry(int Lx, int Ly, int Nx, int Ny, GenGeom* g);
 size_t gen_rowbins_bytes(const GenGeom& g, int nrows_img, int nbins);  // R / Q buffers
@@ -119,7 +121,9 @@ size_t gen_band_bytes(const GenGeom& g, int n, int nparts, int nrows, int ncols)
 size_t gen_T_bytes(const GenGeom& g, int nimg, int nsplit);
 size_t gen_table_elems(const GenGeom& g);  // twb + twl + tw2 + rootLy (float2)
 int gen_build_tables(const GenGeom& g, float2* tables, cudaStream_t st);
-int gen_choose_split(const GenGeom& g, int nimg, int K);
+// kernel slices per image of a spectral launch with `per_sm` resident CTAs per SM
+// (2 for the forward core, 1 for the adjoint's)
+int gen_choose_split(const GenGeom& g, int nimg, int K, int per_sm = 2);
 int gen_choose_parts(const GenGeom& g, int n, int ncols);
 
 // stage launchers (device pointers, stream-ordered)

@@ -167,6 +167,7 @@ int create_gen_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, 
   int tcap = 0, pmax = 0;
   for (int n = 1; n <= max_clips; ++n) {
     tcap = std::max(tcap, n * nsets * kl::gen_choose_split(gg, n * nsets, nk));
+    if (adjoint) tcap = std::max(tcap, n * nsets * kl::gen_choose_split(gg, n * nsets, nk, 1));
     pmax = std::max(pmax, kl::gen_choose_parts(gg, n, gg.nf));
   }
   for (int ns = 1; ns <= kl::kGenMaxSplit; ns *= 2) tcap = std::max(tcap, std::min(ns, nk) * nsets);
@@ -278,6 +279,7 @@ int vjp_gen(kl_socs_plan p, const float* masks, const float* targets, int nclips
   const kl::GenGeom& g = p->gg;
   const int nimg = nclips * p->nsets;
   const int ns = kl::gen_choose_split(g, nimg, p->K);
+  const int ns_adj = kl::gen_choose_split(g, nimg, p->K, 1);
   const int nparts = kl::gen_choose_parts(g, nclips, g.nf);
   const int gparts = kl::gen_choose_parts(g, nimg, g.ntx);
   int rc;
@@ -293,9 +295,9 @@ int vjp_gen(kl_socs_plan p, const float* masks, const float* targets, int nclips
     return rc;
   if ((rc = kl::gen_launch_colfwd(g, p->gtab, p->Q, nimg, g.ntx, 2 * g.Ny, 1.0f, gparts, p->gband, st))) return rc;
   if ((rc = kl::gen_launch_vjp_spectral(g, p->band, nparts, p->gband, gparts, nclips, p->H, p->lam, p->K, p->nsets,
-                                        ns, p->gam, st)))
+                                        ns_adj, p->gam, st)))
     return rc;
-  if ((rc = kl::gen_launch_gradT(g, p->gam, nclips, p->nsets * ns, p->Tg, st))) return rc;
+  if ((rc = kl::gen_launch_gradT(g, p->gam, nclips, p->nsets * ns_adj, p->Tg, st))) return rc;
   if ((rc = kl::gen_launch_colinv(g, p->gtab, p->Tg, nclips, 1, g.Ny, g.nf, p->Q, st))) return rc;
   if ((rc = kl::gen_launch_rowinv(g, p->gtab, p->Q, nclips, g.nf, grad, st))) return rc;
   p->last_vjp_clips = nclips;

@@ -472,24 +472,30 @@ __global__ void __launch_bounds__(kThreads) k_socs_inverse(const float2* __restr
 #pragma unroll 1
       for (int c = 0; c < V / 32; ++c) {
         const int lp = lane + 32 * c;
-        float2 Z[P];
+        // Z[k] = sum over b = k (mod P) of q[b] conj(tw[b]), accumulated as its
+        // Hermitian fold Y[k] = Z[k] + conj Z[P-k] (k <= P/2): half the
+        // registers of Z, and the real output needs nothing more
+        float2 Y[P / 2 + 1];
 #pragma unroll
-        for (int i = 0; i < P; ++i) Z[i] = make_float2(0.f, 0.f);
-        // Z[k] += q[b] * conj(tw[b]) for b = k (mod P), in chunks of P bins so that
-        // only one chunk of coefficients is live in registers
+        for (int i = 0; i <= P / 2; ++i) Y[i] = make_float2(0.f, 0.f);
         constexpr int KB = NBM < P ? NBM : P;
 #pragma unroll 1
         for (int b0 = 0; b0 < NBM; b0 += KB) {
 #pragma unroll
           for (int k = 0; k < KB; ++k) {
             const float2 qb = q[b0 + k], w = twi[(b0 + k) * V + lp];
-            const int kk = k;  // b0 is a multiple of P when NBM > P
-            Z[kk] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Z[kk].x)),
-                                fmaf(qb.y, w.x, fmaf(-qb.x, w.y, Z[kk].y)));
+            // z = qb conj(w); b0 is a multiple of P when NBM > P
+            if (2 * k <= P) {
+              Y[k] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Y[k].x)),
+                                 fmaf(qb.y, w.x, fmaf(-qb.x, w.y, Y[k].y)));
+            } else {
+              Y[P - k] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Y[P - k].x)),
+                                     fmaf(-qb.y, w.x, fmaf(qb.x, w.y, Y[P - k].y)));
+            }
           }
         }
         float o[P];
-        re_idft_reg<P>(Z, o);
+        c2r_half<P>(Y, o);
 #pragma unroll
         for (int i = 0; i < P; ++i) row[lp + V * i] = o[i];
       }

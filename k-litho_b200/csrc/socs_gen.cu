@@ -130,10 +130,20 @@ size_t gen_T_bytes(const GenGeom& g, int nimg, int nsplit) {
 }
 size_t gen_table_elems(const GenGeom& g) { return off_rly(g) + (size_t)g.Ly; }
 
-int gen_choose_split(const GenGeom& g, int nimg, int K) {
-  int ns = 1;
-  while (ns < kGenMaxSplit && g.RG * nimg * ns < 2 * kSMs && K / (2 * ns) >= 3) ns *= 2;
-  return ns;
+int gen_choose_split(const GenGeom& g, int nimg, int K, int per_sm) {
+  // kernel slices per image: the count whose CTAs fill the GPU's resident
+  // slots most evenly (waves x work per CTA), with slices of at least 3 kernels
+  const long long slots = (long long)kSMs * per_sm, ctas = (long long)g.RG * nimg;
+  int best = 1;
+  double best_t = 1e30;
+  for (int ns = 1; ns <= kGenMaxSplit && (ns == 1 || K / ns >= 3); ns *= 2) {
+    const double t = (double)((ctas * ns + slots - 1) / slots) / ns;
+    if (t < best_t * 0.98) {
+      best_t = t;
+      best = ns;
+    }
+  }
+  return best;
 }
 
 int gen_choose_parts(const GenGeom& g, int n, int ncols) {
@@ -291,13 +301,28 @@ __global__ void __launch_bounds__(kT) k_gen_colfwd(const float2* __restrict__ R,
     wf.init(lane);
     const int q = brev5(lane);
     const int fy0 = q - 32 * ((q + Yb) / 32);  // smallest fy >= -Yb with fy = q (mod 32)
+    // the next strip's row bin and phases are loaded while this strip is transformed
+    float2 rn = make_float2(0.f, 0.f), pn[MT];
+    auto fetch = [&](int s) {
+      rn = __ldg(Rn + (size_t)(s + nS * lane) * ncols + fx);
+#pragma unroll
+      for (int t = 0; t < MT; ++t) {
+        const int fy = fy0 + 32 * t;
+        pn[t] = fy <= Yb ? __ldg(rly + mod_pos(fy * s, Ly)) : make_float2(1.f, 0.f);
+      }
+    };
+    if (s0 < s1) fetch(s0);
     for (int s = s0; s < s1; ++s) {
-      float2 v[1] = {__ldg(Rn + (size_t)(s + nS * lane) * ncols + fx)};
+      float2 v[1] = {rn};
+      float2 p[MT];
+#pragma unroll
+      for (int t = 0; t < MT; ++t) p[t] = pn[t];
+      if (s + 1 < s1) fetch(s + 1);
       wf.run(v, lane);
 #pragma unroll
       for (int t = 0; t < MT; ++t) {
         const int fy = fy0 + 32 * t;
-        if (fy <= Yb) acc[t] = cfma(v[0], cconj(__ldg(rly + mod_pos(fy * s, Ly))), acc[t]);
+        if (fy <= Yb) acc[t] = cfma(v[0], cconj(p[t]), acc[t]);
       }
     }
 #pragma unroll
@@ -399,16 +424,29 @@ __global__ void __launch_bounds__(kT, 2) k_gen_spectral(const float2* __restrict
   const size_t nb2 = (size_t)nby * nbx;
   const float2* Hs = H + (size_t)set * K * nb2;
   const int fxs = lane - 32 * ((lane + Nx) / 32);  // smallest fx >= -Nx with fx = lane (mod 32)
+  // the kernel rows come from L2: each warp keeps the loads of its next row in
+  // flight while it folds and transforms the current one (the next kernel's
+  // first row after its last), so their latency overlaps the work
+  float2 hn[kGenMaxFold];
+  if (k0 < k1 && warp < nby) gen_load_hrow(Hs + (size_t)k0 * nb2, warp, nbx, Nx, fxs, hn);
   for (int k = k0; k < k1; ++k) {
     const float2* Hk = Hs + (size_t)k * nb2;
     const float lk = __ldg(lam + set * K + k);
     // stage 1: band rows folded mod 32, then a 32-point inverse FFT over the lanes
     for (int r = warp; r < nby; r += kW) {
+      float2 h[kGenMaxFold];
+#pragma unroll
+      for (int t = 0; t < kGenMaxFold; ++t) h[t] = hn[t];
+      if (r + kW < nby) gen_load_hrow(Hk, r + kW, nbx, Nx, fxs, hn);
+      else if (k + 1 < k1) gen_load_hrow(Hk + nb2, warp, nbx, Nx, fxs, hn);
       float2 v = make_float2(0.f, 0.f);
-      const float2* hr = Hk + (size_t)r * nbx + Nx;
-      for (int fx = fxs; fx <= Nx; fx += 32) {
-        const float2 m = fx >= 0 ? Mh[r * nf + fx] : cconj(Mh[(nby - 1 - r) * nf - fx]);
-        v = cfma(__ldg(hr + fx), m, v);
+#pragma unroll
+      for (int t = 0; t < kGenMaxFold; ++t) {
+        const int fx = fxs + 32 * t;
+        if (fx <= Nx) {
+          const float2 m = fx >= 0 ? Mh[r * nf + fx] : cconj(Mh[(nby - 1 - r) * nf - fx]);
+          v = cfma(h[t], m, v);
+        }
       }
       float2 vv[1] = {v};
       w1.run(vv, lane);
@@ -508,6 +546,7 @@ __global__ void __launch_bounds__(kT) k_gen_colinv(const float2* __restrict__ T,
                                                    float2* __restrict__ Q, int spc) {
   extern __shared__ float4 smem4[];
   float2* Qs = reinterpret_cast<float2*>(smem4);  // [32][nbins + 1]
+  float2* ph = Qs + 32 * (nbins + 1);             // [2A + 1] e^{2 pi i a s / Ly} of the strip
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int lda = 2 * A + 1, qp = nbins + 1, Ly = g.Ly;
   const int img = blockIdx.y;
@@ -521,13 +560,30 @@ __global__ void __launch_bounds__(kT) k_gen_colinv(const float2* __restrict__ T,
   for (int s = s0; s < s1; ++s) {
     int nr = 32;
     if (g.ystrip) {
+      for (int i = threadIdx.x; i < lda; i += kT) ph[i] = __ldg(rly + mod_pos((i - A) * s, Ly));
+      __syncthreads();
+      const int a0 = lane - 32 * ((lane + A) / 32);  // smallest a >= -A with a = lane (mod 32)
       for (int b = warp; b < nbins; b += kW) {
+        // the column's terms a = a0 + 32 t (at most 8: 2A + 1 <= 255), loads issued together
+        float2 tv[8];
+        const float2* tp = Ti + (size_t)b * lda + A;
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const int a = a0 + 32 * t;
+          tv[t] = a <= A ? __ldg(tp + a) : make_float2(0.f, 0.f);
+        }
+        for (int p = 1; p < nsplit; ++p) {
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            const int a = a0 + 32 * t;
+            if (a <= A) tv[t] = cadd(tv[t], __ldg(tp + p * tsz + a));
+          }
+        }
         float2 f = make_float2(0.f, 0.f);
-        for (int a = lane - 32 * ((lane + A) / 32); a <= A; a += 32) {
-          const float2* tp = Ti + (size_t)b * lda + a + A;
-          float2 tv = __ldg(tp);
-          for (int p = 1; p < nsplit; ++p) tv = cadd(tv, __ldg(tp + p * tsz));
-          f = cfma(tv, __ldg(rly + mod_pos(a * s, Ly)), f);
+#pragma unroll
+        for (int t = 0; t < 8; ++t) {
+          const int a = a0 + 32 * t;
+          if (a <= A) f = cfma(tv[t], ph[a + A], f);
         }
         float2 v[1] = {f};
         wf.run(v, lane);
@@ -574,19 +630,34 @@ __global__ void __launch_bounds__(kT) k_gen_rowinv(const float2* __restrict__ Q,
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float2* tb = reinterpret_cast<float2*>(smem4);  // [NBX][32]  e^{+2 pi i b l / Lx}
   float2* qc = tb + g.NBX * 32 + warp * g.NBX;    // [NBX]      this warp's chunk coefficients
-  const float2* tw2 = tables + off_tw2(g);
-  for (int i = threadIdx.x; i < 32 * g.NBX; i += kT) tb[i] = __ldg(tables + i);
-  __syncthreads();
+  float2* t2s = tb + g.NBX * 32 + kW * g.NBX;     // [nC][NBX]  chunk twiddles, when they fit
   const int V = g.V, nch = (V + 31) / 32;
+  const bool t2_shared = gen_t2_in_smem(g);
+  const float2* tw2 = t2_shared ? t2s : tables + off_tw2(g);
+  for (int i = threadIdx.x; i < 32 * g.NBX; i += kT) tb[i] = __ldg(tables + i);
+  if (t2_shared)
+    for (int i = threadIdx.x; i < nch * g.NBX; i += kT) t2s[i] = __ldg(tables + off_tw2(g) + i);
+  __syncthreads();
   const int nbp = (nbins + P - 1) / P * P;
-  for (int row = blockIdx.x * kW + warp; row < nrows; row += gridDim.x * kW) {
-    const float2* qr = Q + (size_t)row * nbins;
+  // each lane holds the coefficients b = lane + 32 t of its warp's row; the
+  // next row's are loaded while the current one is synthesised
+  float2 qn[4];
+  const int row0 = blockIdx.x * kW + warp, rstep = gridDim.x * kW;
+  if (row0 < nrows) gen_load_qrow(Q + (size_t)row0 * nbins, nbins, lane, qn);
+  for (int row = row0; row < nrows; row += rstep) {
+    float2 q[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) q[t] = qn[t];
+    if (row + rstep < nrows) gen_load_qrow(Q + (size_t)(row + rstep) * nbins, nbins, lane, qn);
     float* orow = out + (size_t)row * g.Lx;
 #pragma unroll 1
     for (int c = 0; c < nch; ++c) {
       // q_c[b] = Q[b] e^{2 pi i b 32 c / Lx}: the lane twiddle then only depends on the lane
-      for (int b = lane; b < nbp; b += 32)
-        qc[b] = b < nbins ? cmul(__ldg(qr + b), __ldg(tw2 + (size_t)c * g.NBX + b)) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int b = lane + 32 * t;
+        if (b < nbp) qc[b] = b < nbins ? cmul(q[t], tw2[(size_t)c * g.NBX + b]) : make_float2(0.f, 0.f);
+      }
       __syncwarp();
       float2 Y[HY];
 #pragma unroll
@@ -660,7 +731,8 @@ int launch_rowfwd_t(const GenGeom& g, const float2* tables, const float* src, in
 template <int P>
 int launch_rowinv_t(const GenGeom& g, const float2* tables, const float2* Q, int nrows, int nbins, float* out,
                     cudaStream_t st) {
-  const size_t sm = sizeof(float2) * ((size_t)32 * g.NBX + (size_t)kW * g.NBX);
+  const size_t sm = sizeof(float2) * ((size_t)32 * g.NBX + (size_t)kW * g.NBX +
+                                      (gen_t2_in_smem(g) ? (size_t)g.nC * g.NBX : 0));
   auto kern = k_gen_rowinv<P>;
   int rc = set_smem(kern, sm);
   if (rc) return rc;
@@ -742,7 +814,7 @@ int gen_launch_colinv(const GenGeom& g, const float2* tables, const float2* T, i
   // a few strips per CTA so the image's T is reused from L1, enough CTAs to fill the GPU
   int spc = 1;
   while (spc < 8 && (long long)nimg * ((g.nS + 2 * spc - 1) / (2 * spc)) >= 4 * kSMs) spc *= 2;
-  const size_t sm = sizeof(float2) * (size_t)32 * (nbins + 1);
+  const size_t sm = sizeof(float2) * ((size_t)32 * (nbins + 1) + (size_t)(2 * A + 1));
   int rc = set_smem(k_gen_colinv, sm);
   if (rc) return rc;
   dim3 grid((g.nS + spc - 1) / spc, nimg);

@@ -79,17 +79,30 @@ __global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const
   float2* tl = tb + NBX * 32;                      // [32][NBX] the same, transposed
   float2* qc = tl + NBX * 32 + warp * NBX;         // [NBX]
   float2* sb = tl + NBX * 32 + kW * NBX + warp * HS * 33;  // [HS][33]
-  const float2* tw2 = tables + off_tw2(g);
+  float2* t2s = tl + NBX * 32 + kW * NBX + kW * HS * 33;   // [nC][NBX] chunk twiddles, when they fit
+  const int Lx = g.Lx, Ly = g.Ly, V = g.Vf, nch = (V + 31) / 32;
+  const bool t2_shared = gen_t2_in_smem(g);
+  const float2* tw2 = t2_shared ? t2s : tables + off_tw2(g);
   for (int i = threadIdx.x; i < 64 * NBX; i += kT) tb[i] = __ldg(tables + i);
+  if (t2_shared)
+    for (int i = threadIdx.x; i < nch * NBX; i += kT) t2s[i] = __ldg(tables + off_tw2(g) + i);
   __syncthreads();
   const int img = blockIdx.y, clip = img / nsets;
-  const int Lx = g.Lx, Ly = g.Ly, V = g.Vf, nch = (V + 31) / 32;
   const int nbp = (ntx + PF - 1) / PF * PF;
   const int nt = (ntx + 31) / 32;
   double lsum = 0.0;
-  for (int y = blockIdx.x * kW + warp; y < Ly; y += gridDim.x * kW) {
+  // each lane holds the coefficients b = lane + 32 t of its warp's row (the
+  // next row's are loaded while the current one is worked on)
+  const int y0 = blockIdx.x * kW + warp, ystep = gridDim.x * kW;
+  float2 qn[4];
+  if (y0 < Ly) gen_load_qrow(Q + ((size_t)img * Ly + y0) * ntx, ntx, lane, qn);
+  for (int y = y0; y < Ly; y += ystep) {
     const size_t row = (size_t)img * Ly + y;
     float2* qr = Q + row * ntx;
+    float2 q[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) q[t] = qn[t];
+    if (y + ystep < Ly) gen_load_qrow(Q + (row + ystep) * ntx, ntx, lane, qn);
     float* orow = images ? images + row * Lx : nullptr;
     const float* trow = targets + ((size_t)clip * Ly + y) * Lx;
     float2 acc[4];
@@ -98,8 +111,11 @@ __global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const
     float rsum = 0.f;
 #pragma unroll 1
     for (int c = 0; c < nch; ++c) {
-      for (int b = lane; b < nbp; b += 32)
-        qc[b] = b < ntx ? cmul(qr[b], __ldg(tw2 + (size_t)c * NBX + b)) : make_float2(0.f, 0.f);
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int b = lane + 32 * t;
+        if (b < nbp) qc[b] = b < ntx ? cmul(q[t], tw2[(size_t)c * NBX + b]) : make_float2(0.f, 0.f);
+      }
       __syncwarp();
       float2 Y[HS];
 #pragma unroll
@@ -157,7 +173,7 @@ __global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const
             s.x = fmaf(sv.x, w.x, fmaf(svy, w.y, s.x));
             s.y = fmaf(svy, w.x, fmaf(-sv.x, w.y, s.y));
           }
-          acc[t] = cfma(s, cconj(__ldg(tw2 + (size_t)c * NBX + gx)), acc[t]);
+          acc[t] = cfma(s, cconj(tw2[(size_t)c * NBX + gx]), acc[t]);
         }
       }
       __syncwarp();
@@ -254,18 +270,30 @@ __device__ void gv_make_gamma(const float2* __restrict__ gband, int gparts, cons
 }
 
 // stage 1 of a field: band rows of Hk . M' folded mod 32, inverse 32-point FFT
-// over the lanes -> E1[r][j]
-__device__ __forceinline__ void gv_field_rows(const GenGeom& g, const float2* __restrict__ Hk, const float2* Mh,
-                                              float2* E1, const WarpFFT<1, +1>& w1, int lane, int warp) {
+// over the lanes -> E1[r][j].  hn holds the loads of the warp's first row of
+// Hk on entry and, on exit, those of the first row of Hnext (when not NULL):
+// each row's successor is in flight while the row is worked on.
+__device__ __forceinline__ void gv_field_rows(const GenGeom& g, const float2* __restrict__ Hk,
+                                              const float2* __restrict__ Hnext, const float2* Mh, float2* E1,
+                                              const WarpFFT<1, +1>& w1, int lane, int warp,
+                                              float2 (&hn)[kGenMaxFold]) {
   const int nf = g.nf, nby = g.nby, nbx = g.nbx, Nx = g.Nx;
   const int fxs = lane - 32 * ((lane + Nx) / 32);
   const int br = brev5(lane);
   for (int r = warp; r < nby; r += kW) {
+    float2 h[kGenMaxFold];
+#pragma unroll
+    for (int t = 0; t < kGenMaxFold; ++t) h[t] = hn[t];
+    if (r + kW < nby) gen_load_hrow(Hk, r + kW, nbx, Nx, fxs, hn);
+    else if (Hnext) gen_load_hrow(Hnext, warp, nbx, Nx, fxs, hn);
     float2 v = make_float2(0.f, 0.f);
-    const float2* hr = Hk + (size_t)r * nbx + Nx;
-    for (int fx = fxs; fx <= Nx; fx += 32) {
-      const float2 m = fx >= 0 ? Mh[r * nf + fx] : cconj(Mh[(nby - 1 - r) * nf - fx]);
-      v = cfma(__ldg(hr + fx), m, v);
+#pragma unroll
+    for (int t = 0; t < kGenMaxFold; ++t) {
+      const int fx = fxs + 32 * t;
+      if (fx <= Nx) {
+        const float2 m = fx >= 0 ? Mh[r * nf + fx] : cconj(Mh[(nby - 1 - r) * nf - fx]);
+        v = cfma(h[t], m, v);
+      }
     }
     float2 vv[1] = {v};
     w1.run(vv, lane);
@@ -335,10 +363,13 @@ __global__ void __launch_bounds__(kT, 1) k_gen_vjp_spectral(const float2* __rest
   const size_t nb2 = (size_t)nby * nbx;
   const float2* Hs = H + (size_t)set * K * nb2;
   const int fxm = br - 32 * ((br + Nx) / 32);  // smallest fx >= -Nx with fx = brev5(lane) (mod 32)
+  const int fxs = lane - 32 * ((lane + Nx) / 32);
+  float2 hn[kGenMaxFold];
+  if (k0 < k1 && warp < nby) gen_load_hrow(Hs + (size_t)k0 * nb2, warp, nbx, Nx, fxs, hn);
   for (int k = k0; k < k1; ++k) {
     const float2* Hk = Hs + (size_t)k * nb2;
     const float lk = __ldg(lam + set * K + k) * invg2;
-    gv_field_rows(g, Hk, Mh, E1, w1, lane, warp);
+    gv_field_rows(g, Hk, k + 1 < k1 ? Hk + nb2 : nullptr, Mh, E1, w1, lane, warp, hn);
     __syncthreads();
     // per column: field e(p), w = conj(e) gam lk, then W1[fy] = sum_p w e^{+2 pi i fy p/G}
 #pragma unroll
@@ -359,12 +390,18 @@ __global__ void __launch_bounds__(kT, 1) k_gen_vjp_spectral(const float2* __rest
     __syncthreads();
     // rows fy: F[m] = sum_j W1[fy][j] e^{+2 pi i m j / 32}; Acc[fy][fx] += H_k F[fx mod 32]
     for (int r = warp; r < nby; r += kW) {
+      // the row's kernel values are loaded before the FFT so the loads overlap it
+      float2 hh[kGenMaxFold];
+      gen_load_hrow(Hk, r, nbx, Nx, fxm, hh);
       float2 vv[1] = {Ws[r * 33 + lane]};
       w1.run(vv, lane);
       // lane holds F[m], m = brev5(lane): the bins fx = m (mod 32)
-      const float2* hr = Hk + (size_t)r * nbx + Nx;
       float2* ar = Acc + (size_t)r * nbx + Nx;
-      for (int fx = fxm; fx <= Nx; fx += 32) ar[fx] = cfma(__ldg(hr + fx), vv[0], ar[fx]);
+#pragma unroll
+      for (int t = 0; t < kGenMaxFold; ++t) {
+        const int fx = fxm + 32 * t;
+        if (fx <= Nx) ar[fx] = cfma(hh[t], vv[0], ar[fx]);
+      }
     }
     __syncthreads();
   }
@@ -447,8 +484,12 @@ __global__ void __launch_bounds__(kT) k_gen_vjp_source(const float2* __restrict_
   wi.init(lane);
   const float invg2 = 1.0f / ((float)G * (float)G);
   const size_t nb2 = (size_t)nby * g.nbx;
+  const int fxs = lane - 32 * ((lane + g.Nx) / 32);
+  float2 hn[kGenMaxFold];
+  if (s0 < s1 && warp < nby) gen_load_hrow(Hs + (size_t)s0 * nb2, warp, g.nbx, g.Nx, fxs, hn);
   for (int s = s0; s < s1; ++s) {
-    gv_field_rows(g, Hs + (size_t)s * nb2, Mh, E1, w1, lane, warp);
+    gv_field_rows(g, Hs + (size_t)s * nb2, s + 1 < s1 ? Hs + (size_t)(s + 1) * nb2 : nullptr, Mh, E1, w1, lane, warp,
+                  hn);
     __syncthreads();
     float part = 0.f;
 #pragma unroll
@@ -477,7 +518,8 @@ namespace {
 template <int PF>
 int launch_rowvjp_t(const GenGeom& g, const float2* tables, float2* Q, int nimg, int nsets, const float* targets,
                     float alpha, float thr, float* images, double* loss, cudaStream_t st) {
-  const size_t sm = sizeof(float2) * ((size_t)64 * g.NBX + (size_t)kW * g.NBX + (size_t)kW * (PF / 2 + 1) * 33);
+  const size_t sm = sizeof(float2) * ((size_t)64 * g.NBX + (size_t)kW * g.NBX + (size_t)kW * (PF / 2 + 1) * 33 +
+                                      (gen_t2_in_smem(g) ? (size_t)g.nC * g.NBX : 0));
   auto kern = k_gen_rowvjp<PF>;
   int rc = set_smem(kern, sm);
   if (rc) return rc;
