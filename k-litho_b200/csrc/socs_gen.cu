@@ -572,13 +572,6 @@ __global__ void __launch_bounds__(kT) k_gen_colinv(const float2* __restrict__ T,
           const int a = a0 + 32 * t;
           tv[t] = a <= A ? __ldg(tp + a) : make_float2(0.f, 0.f);
         }
-        for (int p = 1; p < nsplit; ++p) {
-#pragma unroll
-          for (int t = 0; t < 8; ++t) {
-            const int a = a0 + 32 * t;
-            if (a <= A) tv[t] = cadd(tv[t], __ldg(tp + p * tsz + a));
-          }
-        }
         float2 f = make_float2(0.f, 0.f);
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
@@ -598,9 +591,7 @@ __global__ void __launch_bounds__(kT) k_gen_colinv(const float2* __restrict__ T,
           int m = mod_pos(-A * y, Ly);
           const float2* tp = Ti + (size_t)b * lda;
           for (int a = 0; a < lda; ++a) {
-            float2 tv = __ldg(tp + a);
-            for (int p = 1; p < nsplit; ++p) tv = cadd(tv, __ldg(tp + p * tsz + a));
-            f = cfma(tv, __ldg(rly + m), f);
+            f = cfma(__ldg(tp + a), __ldg(rly + m), f);
             m += y;
             if (m >= Ly) m -= Ly;
           }
@@ -685,6 +676,17 @@ __global__ void __launch_bounds__(kT) k_gen_rowinv(const float2* __restrict__ Q,
       }
       __syncwarp();
     }
+  }
+}
+
+// slice partials of T summed into slice 0 (one pass over L2-resident data), so
+// that the column synthesis reads one spectrum per image
+__global__ void k_gen_sumT(float2* __restrict__ T, size_t tsz, int nsplit) {
+  float2* Ti = T + (size_t)blockIdx.y * nsplit * tsz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tsz; i += (size_t)gridDim.x * blockDim.x) {
+    float2 v = Ti[i];
+    for (int p = 1; p < nsplit; ++p) v = cadd(v, Ti[p * tsz + i]);
+    Ti[i] = v;
   }
 }
 
@@ -811,6 +813,14 @@ int gen_launch_spectral(const GenGeom& g, const float2* band, int nparts, int nc
 int gen_launch_colinv(const GenGeom& g, const float2* tables, const float2* T, int nimg, int nsplit, int A,
                       int nbins, float2* Q, cudaStream_t st) {
   if (nimg <= 0) return KL_OK;
+  if (nsplit > 1) {
+    // fold the slices into slice 0 first (T is the caller's spectra buffer)
+    const size_t tsz = (size_t)nbins * (2 * A + 1);
+    const int bx = (int)std::min<size_t>((tsz + 255) / 256, 64);
+    k_gen_sumT<<<dim3(bx, nimg), 256, 0, st>>>(const_cast<float2*>(T), tsz, nsplit);
+    int rc = check_launch("k_gen_sumT");
+    if (rc) return rc;
+  }
   // a few strips per CTA so the image's T is reused from L1, enough CTAs to fill the GPU
   int spc = 1;
   while (spc < 8 && (long long)nimg * ((g.nS + 2 * spc - 1) / (2 * spc)) >= 4 * kSMs) spc *= 2;
@@ -818,7 +828,7 @@ int gen_launch_colinv(const GenGeom& g, const float2* tables, const float2* T, i
   int rc = set_smem(k_gen_colinv, sm);
   if (rc) return rc;
   dim3 grid((g.nS + spc - 1) / spc, nimg);
-  k_gen_colinv<<<grid, kT, sm, st>>>(T, nsplit, A, nbins, g, tables + off_rly(g), Q, spc);
+  k_gen_colinv<<<grid, kT, sm, st>>>(T, nsplit, A, nbins, g, tables + off_rly(g), Q, spc);  // reads slice 0
   return check_launch("k_gen_colinv");
 }
 

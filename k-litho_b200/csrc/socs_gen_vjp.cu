@@ -66,7 +66,7 @@ int check_launch(const char* what) {
 // row_vjp: Q rows -> image rows, resist, loss, dL/dI row DFT (written over Q)
 // ---------------------------------------------------------------------------
 template <int PF>
-__global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const GenGeom g,
+__global__ void __launch_bounds__(kT, 2) k_gen_rowvjp(float2* __restrict__ Q, const GenGeom g,
                                                    const float2* __restrict__ tables, int nsets,
                                                    const float* __restrict__ targets, float alpha, float thr,
                                                    float* __restrict__ images, double* __restrict__ loss) {
@@ -111,6 +111,11 @@ __global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const
     float rsum = 0.f;
 #pragma unroll 1
     for (int c = 0; c < nch; ++c) {
+      const int lp = lane + 32 * c;
+      // the chunk's targets are loaded first, so that they arrive during the synthesis
+      float tg[PF];
+#pragma unroll
+      for (int i = 0; i < PF; ++i) tg[i] = lp < V ? __ldcs(trow + lp + V * i) : 0.f;
 #pragma unroll
       for (int t = 0; t < 4; ++t) {
         const int b = lane + 32 * t;
@@ -136,14 +141,13 @@ __global__ void __launch_bounds__(kT) k_gen_rowvjp(float2* __restrict__ Q, const
       }
       float o[PF];
       c2r_half<PF>(Y, o);
-      const int lp = lane + 32 * c;
       if (lp < V) {
 #pragma unroll
         for (int i = 0; i < PF; ++i) {
           const int x = lp + V * i;
           if (orow) __stcs(orow + x, o[i]);
           const float sg = __frcp_rn(1.0f + __expf(-alpha * (o[i] - thr)));
-          const float d = sg - __ldcs(trow + x);
+          const float d = sg - tg[i];
           rsum = fmaf(d, d, rsum);
           o[i] = 2.0f * d * sg * (1.0f - sg) * alpha;
         }

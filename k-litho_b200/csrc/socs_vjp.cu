@@ -125,17 +125,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_vjp_inverse(const float2* __res
       const int lp = lane + 32 * c;
       float o[P];
       {
-        float2 Z[P];
+        // the Hermitian fold of the lane's sub-bins, accumulated in the order of
+        // k_socs_inverse so that the image equals the forward pass's bit for bit
+        float2 Y[P / 2 + 1];
 #pragma unroll
-        for (int i = 0; i < P; ++i) Z[i] = make_float2(0.f, 0.f);
+        for (int i = 0; i <= P / 2; ++i) Y[i] = make_float2(0.f, 0.f);
 #pragma unroll
         for (int b = 0; b < NBM; ++b) {
           const float2 qb = q[b], w = tw[b * V + lp];
           const int k = b % P;
-          Z[k] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Z[k].x)),
-                             fmaf(qb.y, w.x, fmaf(-qb.x, w.y, Z[k].y)));
+          if (2 * k <= P) {
+            Y[k] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Y[k].x)),
+                               fmaf(qb.y, w.x, fmaf(-qb.x, w.y, Y[k].y)));
+          } else {
+            Y[P - k] = make_float2(fmaf(qb.x, w.x, fmaf(qb.y, w.y, Y[P - k].x)),
+                                   fmaf(-qb.y, w.x, fmaf(qb.x, w.y, Y[P - k].y)));
+          }
         }
-        re_idft_reg<P>(Z, o);
+        c2r_half<P>(Y, o);
       }
       // resist model, loss and dL/dI on the lane's pixels
       __pipeline_wait_prior(0);
