@@ -135,6 +135,26 @@ int kl_socs_plan_create_ex(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, i
 /* 0 if the plan runs on the specialised kernels, 1 on the general pipeline. */
 int kl_socs_plan_engine(kl_socs_plan plan);
 
+/* Engine of the image synthesis (the FI step) on the specialised kernels:
+ * KL_SYNTH_CUDA_CORES, a per-lane DFT of each row's coefficients;
+ * KL_SYNTH_TENSOR_CORES, the same sum as an FP16x3 split matrix product on
+ * the tensor cores (periods with Lx, Ly multiples of 128 and 2(2Nx+1) <= 128;
+ * image error of the same order as the CUDA-core engine's); KL_SYNTH_AUTO
+ * (the default), the engine kl_socs_autotune picked, else the CUDA cores.
+ * Returns KL_ERR_UNSUPPORTED for the tensor-core engine on other geometries
+ * and on general-pipeline plans.  No counterpart in the reference. */
+#define KL_SYNTH_AUTO 0
+#define KL_SYNTH_CUDA_CORES 1
+#define KL_SYNTH_TENSOR_CORES 2
+int kl_socs_set_synthesis(kl_socs_plan plan, int mode);
+/* The engine the next kl_socs_forward of nclips clips uses (KL_SYNTH_CUDA_CORES
+ * or KL_SYNTH_TENSOR_CORES; KL_SYNTH_CUDA_CORES on the general pipeline). */
+int kl_socs_synthesis(kl_socs_plan plan, int nclips);
+/* Synchronises the device and returns KL_OK, or KL_ERR_CUDA (with a message)
+ * if a tensor-core pipeline wait of the plan's kernels has timed out since
+ * the last call (the affected images are incomplete); clears the status. */
+int kl_socs_plan_status(kl_socs_plan plan);
+
 /* Upload kernel set `set`: nk planes of the kernel layout, real and imaginary
  * parts separately (as krn_<i>_r.bin / krn_<i>_i.bin hold them), and nk
  * eigenvalues (kernel_info.txt).  Host pointers; synchronous. */
@@ -159,10 +179,11 @@ int kl_socs_forward_host(kl_socs_plan plan, const float* masks_host, int nclips,
 
 /* Times the plan's launch shapes for batches of nclips clips (kernel slices of
  * the spectral stage: 1, 2, 4, 8; image strips per CTA of the synthesis stage:
- * 1 .. 16) with CUDA events on `stream` and keeps the fastest; later calls of
- * kl_socs_forward with nclips clips use it.  Writes images_dev (the images of
- * the chosen shape).  Synchronous.  The chosen shape is returned in
- * *nsplit / *spc when those are not NULL. */
+ * 1 .. 16; the tensor-core synthesis where the geometry allows it) with CUDA
+ * events on `stream` and keeps the fastest; later calls of kl_socs_forward
+ * with nclips clips use it.  Writes images_dev (the images of the chosen
+ * shape).  Synchronous.  The chosen shape is returned in *nsplit / *spc when
+ * those are not NULL (*spc = -1: the tensor-core synthesis). */
 int kl_socs_autotune(kl_socs_plan plan, const float* masks_dev, int nclips, float* images_dev,
                      void* stream, int* nsplit, int* spc);
 

@@ -84,6 +84,16 @@ int socs_launch_spectral(const SocsGeom& g, const float2* partial, int nclips, c
 // spc: strips per CTA of the inverse kernel (0 = chosen from the batch size)
 int socs_launch_inverse(const SocsGeom& g, const float2* tx, const float2* ty, const float2* T,
                         int nclips, int nsets, int nsplit, float* images, cudaStream_t st, int spc = 0);
+// Image synthesis on the tensor cores (socs_synth_tc.cu): the inverse stage as
+// an FP16x3 split GEMM of the row coefficients against a cos/sin basis.
+bool synth_tc_supported(const SocsGeom& g);
+int synth_tc_kp(const SocsGeom& g);  // padded K (64 or 128) of the basis rows
+bool synth_tc_aligned(const float* images);  // TMA stores need 16-byte aligned images
+// basis [Lx][Kp] as FP16 hi and lo halves (each Lx * Kp * 2 bytes)
+int synth_tc_build_basis(const SocsGeom& g, void* bhi, void* blo, cudaStream_t st);
+// err: device status word, set to a nonzero code if a pipeline wait times out
+int synth_tc_launch(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi,
+                    const void* blo, int nimg, float* images, int* err, cudaStream_t st);
 // centred band of FT_r2c (DC at the band centre), complex64 nby x nbx per clip
 int socs_launch_band(const SocsGeom& g, const float2* partial, int nclips, float2* band,
                      cudaStream_t st);

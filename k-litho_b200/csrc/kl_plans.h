@@ -35,7 +35,13 @@ struct kl_socs_plan_s {
   std::vector<cudaEvent_t> events;
   // launch shape chosen by kl_socs_autotune for batches of tune_clips clips
   int tcap = 0;  // clip x kernel-slice products the spectra buffer holds
-  int tune_clips = 0, tune_nsplit = 0, tune_spc = 0;
+  int tune_clips = 0, tune_nsplit = 0, tune_spc = 0;  // tune_spc < 0: tensor-core synthesis
+  // synthesis engine of the specialised pipeline (KL_SYNTH_*), the tensor-core
+  // basis (FP16 hi / lo halves, [Lx][Kp]) and its pipeline status word
+  int synth = 0;
+  void* bhi = nullptr;
+  void* blo = nullptr;
+  int* status = nullptr;
   // general-geometry pipeline (socs_gen.cu): any period, bands up to 4N+1 <= 256.
   // Used when the specialised kernels above do not cover the geometry (or on
   // request); `g` then only carries the sizes.

@@ -43,6 +43,9 @@ void free_plan(kl_socs_plan p) {
   cudaFree(p->band);
   cudaFree(p->Q);
   cudaFree(p->gband);
+  cudaFree(p->bhi);
+  cudaFree(p->blo);
+  cudaFree(p->status);
   delete p;
 }
 
@@ -112,6 +115,15 @@ int run_forward_gen(kl_socs_plan p, const float* masks, int nclips, float* image
   return stage_mark(p, st, ev4, 3);
 }
 
+// synthesis on the tensor cores for a batch of nclips clips: when requested,
+// or when the autotuner picked it for this batch size
+bool use_tc_synthesis(kl_socs_plan p, int nclips) {
+  if (p->gen || !p->bhi) return false;
+  if (p->synth == KL_SYNTH_TENSOR_CORES) return true;
+  if (p->synth == KL_SYNTH_CUDA_CORES) return false;
+  return p->tune_clips == nclips && p->tune_nsplit > 0 && p->tune_spc < 0;
+}
+
 int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st,
                 const cudaEvent_t* ev4 = nullptr) {
   if (p->gen) return run_forward_gen(p, masks, nclips, images, st, ev4);
@@ -119,13 +131,16 @@ int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, c
   if ((rc = stage_mark(p, st, ev4, 0))) return rc;
   int nsplit, spc;
   launch_shape(p, nclips, &nsplit, &spc);
+  const bool tc = use_tc_synthesis(p, nclips) && kl::synth_tc_aligned(images);
+  spc = spc > 0 ? spc : 0;
   if ((rc = kl::socs_launch_forward(p->g, p->tx, p->ty, masks, nclips, p->partial, st))) return rc;
   if ((rc = stage_mark(p, st, ev4, 1))) return rc;
   rc = kl::socs_launch_spectral(p->g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, nsplit,
                                 p->T, st);
   if (rc) return rc;
   if ((rc = stage_mark(p, st, ev4, 2))) return rc;
-  rc = kl::socs_launch_inverse(p->g, p->tx, p->ty, p->T, nclips, p->nsets, nsplit, images, st, spc);
+  rc = tc ? kl::synth_tc_launch(p->g, p->T, p->ty, nsplit, p->bhi, p->blo, nclips * p->nsets, images, p->status, st)
+          : kl::socs_launch_inverse(p->g, p->tx, p->ty, p->T, nclips, p->nsets, nsplit, images, st, spc);
   if (rc) return rc;
   return stage_mark(p, st, ev4, 3);
 }
@@ -250,6 +265,16 @@ int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int 
     free_plan(p);
     return rc;
   }
+  if (kl::synth_tc_supported(g)) {
+    const size_t bb = (size_t)g.Lx * kl::synth_tc_kp(g) * 2;
+    if ((rc = alloc(&p->bhi, bb, "synthesis basis")) || (rc = alloc(&p->blo, bb, "synthesis basis")) ||
+        (rc = alloc((void**)&p->status, sizeof(int), "status word")) ||
+        (rc = kl::synth_tc_build_basis(g, p->bhi, p->blo, nullptr))) {
+      free_plan(p);
+      return rc;
+    }
+    cudaMemset(p->status, 0, sizeof(int));
+  }
   if (adjoint) {
     const size_t nb2s = (size_t)g.nby * g.nbx;
     if ((rc = alloc((void**)&p->gpart, kl::vjp_gpart_bytes(g, max_clips * nsets), "dL/dI partials")) ||
@@ -362,6 +387,37 @@ int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nc
   return KL_OK;
 }
 
+int kl_socs_set_synthesis(kl_socs_plan p, int mode) {
+  KL_CHECK_ARG(p != nullptr, "kl_socs_set_synthesis: plan is NULL");
+  KL_CHECK_ARG(mode == KL_SYNTH_AUTO || mode == KL_SYNTH_CUDA_CORES || mode == KL_SYNTH_TENSOR_CORES,
+               "kl_socs_set_synthesis: mode must be KL_SYNTH_AUTO, KL_SYNTH_CUDA_CORES or KL_SYNTH_TENSOR_CORES");
+  if (mode == KL_SYNTH_TENSOR_CORES && !p->bhi) {
+    kl::set_error(p->gen ? "kl_socs_set_synthesis: the general pipeline has no tensor-core synthesis"
+                         : "kl_socs_set_synthesis: the tensor-core synthesis needs Lx, Ly multiples of 128 and "
+                           "2(2Nx+1) <= 128");
+    return KL_ERR_UNSUPPORTED;
+  }
+  p->synth = mode;
+  return KL_OK;
+}
+
+int kl_socs_synthesis(kl_socs_plan p, int nclips) {
+  if (!p) return KL_ERR_INVALID;
+  return use_tc_synthesis(p, nclips) ? KL_SYNTH_TENSOR_CORES : KL_SYNTH_CUDA_CORES;
+}
+
+int kl_socs_plan_status(kl_socs_plan p) {
+  KL_CHECK_ARG(p != nullptr, "kl_socs_plan_status: plan is NULL");
+  KL_CUDA_TRY(cudaDeviceSynchronize());
+  if (!p->status) return KL_OK;
+  int code = 0;
+  KL_CUDA_TRY(cudaMemcpy(&code, p->status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (!code) return KL_OK;
+  KL_CUDA_TRY(cudaMemset(p->status, 0, sizeof(int)));
+  kl::set_error("tensor-core synthesis: pipeline wait timed out (code " + std::to_string(code) + ")");
+  return KL_ERR_CUDA;
+}
+
 int kl_socs_plan_destroy(kl_socs_plan plan) {
   free_plan(plan);
   return KL_OK;
@@ -448,7 +504,7 @@ int kl_socs_forward_host(kl_socs_plan p, const float* masks_host, int nclips, fl
   KL_CUDA_TRY(cudaEventRecord(p->hev[0], sout));
   KL_CUDA_TRY(cudaStreamWaitEvent(st, p->hev[0], 0));
   KL_CUDA_TRY(cudaStreamSynchronize(st));
-  return KL_OK;
+  return p->status ? kl_socs_plan_status(p) : KL_OK;
 }
 
 int kl_socs_enable_timing(kl_socs_plan p, int enable) {

@@ -117,7 +117,8 @@ int kl_socs_autotune(kl_socs_plan p, const float* masks, int nclips, float* imag
       best_ns = ns;
     }
   }
-  // ... then strips per CTA of the inverse stage
+  // ... then strips per CTA of the inverse stage, and the tensor-core synthesis
+  if (!p->gen && p->bhi && p->synth == KL_SYNTH_AUTO) spcs.push_back(-1);
   for (size_t i = 0; i < spcs.size() && !rc; ++i) {
     if ((rc = time_shape(best_ns, spcs[i], &t))) break;
     if (t < best) {
@@ -125,6 +126,7 @@ int kl_socs_autotune(kl_socs_plan p, const float* masks, int nclips, float* imag
       best_spc = spcs[i];
     }
   }
+  if (!rc && p->status) rc = kl_socs_plan_status(p);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   p->timing = timing;

@@ -1,0 +1,574 @@
+// socs_synth_tc.cu -- the image synthesis of the specialised SOCS pipeline on
+// the 5th-generation tensor cores (sm_100a).
+//
+// k_socs_inverse (socs_fast.cu) synthesises each image row from its 2Nx+1
+// row coefficients Q[b] (the FI step of K-Litho-SOCS/klitho_socs.cpp:158-194
+// restricted to the band) with a per-lane DFT on the CUDA cores.  The same
+// step is a real matrix product per tile of 128 rows:
+//     image[y][x] = sum_b Re(Q[y][b] e^{2 pi i b x / Lx})
+//                 = sum_k A[y][k] B[k][x],  A = [Re Q, -Im Q],  B = [cos; sin],
+// with K = 2(2Nx+1) <= 128.  It runs as tcgen05.mma kind::f16 on a 3-term FP16
+// split, A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32 in TMEM: each
+// split operand keeps 22 significant bits and the dropped A_lo B_lo term is
+// 2^-22 of a product, far below the 1e-5-of-clear-field bar.  A is scaled per
+// image by a power of two so that FP16's range holds it (the bound
+// |Q[b]| <= w_b sum_a |T[a][b]| fixes the exponent); the epilogue undoes it.
+//
+// One persistent CTA per SM handles a contiguous run of 128-row tiles (rows
+// of 128/J strips, y = s + nS j as in k_socs_inverse), with four roles:
+//   warps 0-3  coefficient warps: load the image's band-limited intensity
+//              spectrum T into shared memory (when the image changes), build
+//              the tile's A with J-point warp FFTs along y, two columns at a
+//              time, and write the FP16 halves straight into the
+//              128-byte-swizzled K-major layout (A double-buffered when
+//              shared memory allows, so the next tile's A is built while the
+//              tensor cores work on this one);
+//   warps 4-7  epilogue warps: TMEM accumulator tiles -> registers -> (scale)
+//              -> a swizzled 32 x 32 staging tile per warp -> TMA bulk store of
+//              32 image rows (the HBM-bound part: whole 128-byte lines, no
+//              load/store-unit traffic per row);
+//   warp 8     TMA producer of the basis tiles B (plan-time, L2-resident);
+//   warp 9     MMA issuer, into a ring of TMEM accumulators (512 columns).
+// Every wait is bounded; a timeout sets the plan's status word and stops
+// every role.
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <climits>
+
+#include "kl_device.cuh"
+#include "kl_internal.h"
+#include "kl_tc.cuh"
+
+namespace kl {
+namespace {
+constexpr int kRows = 128;       // tile rows (MMA M, TMEM lanes)
+constexpr int kCW = 4;           // coefficient warps
+constexpr int kEW = 4;           // epilogue warps
+constexpr int kSThreads = 32 * (kCW + kEW + 2);
+constexpr int kProdWarp = kCW + kEW, kMmaWarp = kCW + kEW + 1;
+constexpr int kStages = 4;       // basis tile stages (16 KB each)
+constexpr int kStageBufs = 2;    // staging tiles per epilogue warp
+constexpr int kAtomBytes = kRows * 128;  // one 64-wide K atom of A (128 rows x 128 B)
+constexpr int kTmemCols = 512;
+constexpr int kScaleRing = 8;
+constexpr int kMaxSets = 16;     // TMEM accumulator ring slots
+
+// N tile: 64 columns for one K atom, 32 for two (16 KB basis stages)
+__host__ __device__ constexpr int synth_nt(int KA) { return KA == 1 ? 64 : 32; }
+// columns b of the row coefficients come in groups of 8: K index of column b,
+// part 0 (Re, against cos) or 1 (-Im, against sin) is 16 (b / 8) + 8 part + b % 8
+__host__ __device__ constexpr int synth_ntx8(int ntx) { return (ntx + 7) & ~7; }
+// row stride of the staged spectrum (float2): 8-column groups stay 16-byte
+// aligned and consecutive rows fall on different banks
+__host__ __device__ constexpr int synth_tstride(int ntx) { return synth_ntx8(ntx) + 2; }
+
+struct SynthSmem {
+  size_t a, b, stg, ts, ph, bars, total;
+  int nA;  // A buffers (2 = the next tile's A is built during this tile's MMAs)
+};
+__host__ __device__ inline SynthSmem synth_smem(int KA, int nty, int ntx, int nst, int nA) {
+  SynthSmem s{};
+  const int NT = synth_nt(KA);
+  s.nA = nA;
+  const size_t abuf = 2 * (size_t)KA * kAtomBytes;           // [hi atoms][lo atoms]
+  s.a = 0;
+  s.b = s.a + nA * abuf;                                       // stages of [hi atoms][lo atoms]
+  const size_t stage = 2 * (size_t)KA * NT * 128;
+  s.stg = s.b + kStages * stage;                               // [kEW][kStageBufs] 4 KB tiles
+  s.ts = s.stg + (size_t)kEW * kStageBufs * 4096;              // T [nty][tstride] float2
+  s.ph = s.ts + sizeof(float2) * (size_t)nty * synth_tstride(ntx);  // phases [nst][nty] float2
+  s.bars = (s.ph + sizeof(float2) * (size_t)nst * nty + 15) & ~(size_t)15;
+  s.total = s.bars + 8 * (2 * kStages + 4 + 2 * kMaxSets + 1) + 64;
+  return s;
+}
+constexpr size_t kSmemMax = 227 * 1024 - 1024;  // dynamic bytes usable after the 1 KB alignment pad
+}  // namespace
+
+// plan-time basis: B[x][k] = cos(2 pi b x / Lx) for K index k of (b, part 0),
+// sin(2 pi b x / Lx) for (b, part 1), 0 for b >= ntx and the padding; FP16 hi
+// and lo halves, [Lx][Kp]
+__global__ void k_synth_basis(int Lx, int ntx, int Kp, __half* __restrict__ bhi, __half* __restrict__ blo) {
+  const size_t n = (size_t)Lx * Kp;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i / Kp), k = (int)(i % Kp);
+    const int b = 8 * (k >> 4) + (k & 7), part = (k >> 3) & 1;
+    float v = 0.f;
+    if (b < ntx) {
+      const float2 e = expi2pi_frac((long long)b * x, Lx);
+      v = part ? e.y : e.x;
+    }
+    const __half h = __float2half_rn(v);
+    bhi[i] = h;
+    blo[i] = __float2half_rn(v - __half2float(h));
+  }
+}
+
+template <int RJ, int KA, int NA>
+__global__ void __launch_bounds__(kSThreads, 1)
+    k_socs_synth_tc(const float2* __restrict__ T, const SocsGeom g, const float2* __restrict__ ty, int nsplit,
+                    const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+                    const __grid_constant__ CUtensorMap tm_img, int nimg, int nset, int* __restrict__ err) {
+  constexpr int J = 32 * RJ;
+  constexpr int NST = kRows / J;  // strips per tile
+  constexpr int NT = synth_nt(KA);
+  constexpr int NBYTES_B = NT * 128;  // one atom of a basis tile
+  constexpr int ABUF = 2 * KA * kAtomBytes;
+  constexpr int PHR = 2;              // strip phases per coefficient thread (nst * nty <= 256)
+  constexpr uint32_t IDESC = tc::idesc_f16(kRows, NT, false);
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const SynthSmem L = synth_smem(KA, g.nty, g.ntx, NST, NA);
+  uint8_t* abase = smem + L.a;
+  uint8_t* bst = smem + L.b;
+  uint8_t* stg = smem + L.stg;
+  float2* Ts = reinterpret_cast<float2*>(smem + L.ts);
+  float2* ph = reinterpret_cast<float2*>(smem + L.ph);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);  // basis stage loaded
+  uint64_t* empty = full + kStages;                              // basis stage consumed
+  uint64_t* afull = empty + kStages;                             // A buffer built
+  uint64_t* aempty = afull + 2;                                  // A buffer consumed
+  uint64_t* tfull = aempty + 2;                                  // accumulator ready (ring of nset <= 16)
+  uint64_t* tempty = tfull + kMaxSets;                           // accumulator drained
+  uint64_t* drain = tempty + kMaxSets;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  __shared__ int s_abort;
+  __shared__ float s_scale[2];          // scale of A and its inverse for the current image
+  __shared__ float s_inv[kScaleRing];   // inverse scale per tile, read by the epilogue
+  __shared__ volatile int s_seq[kScaleRing];  // tile number whose scale a slot holds
+  __shared__ unsigned s_bound;
+  volatile int* abort = &s_abort;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
+  const int ntx = g.ntx, nty = g.nty, A2 = 2 * g.Ny;
+  const int tiles_img = g.Ly / kRows, ntile = g.Lx / NT;
+  const int total = nimg * tiles_img;
+  const int per = (total + gridDim.x - 1) / gridDim.x;
+  const int t0 = blockIdx.x * per, t1 = min(total, t0 + per);
+  const size_t tsz = (size_t)nty * ntx;
+
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      tc::mbar_init(tc::smem_u32(&full[s]), 1);
+      tc::mbar_init(tc::smem_u32(&empty[s]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(tc::smem_u32(&afull[b]), 1);
+      tc::mbar_init(tc::smem_u32(&aempty[b]), 1);
+    }
+    for (int a = 0; a < kMaxSets; ++a) {
+      tc::mbar_init(tc::smem_u32(&tfull[a]), 1);
+      tc::mbar_init(tc::smem_u32(&tempty[a]), kEW);
+    }
+    tc::mbar_init(tc::smem_u32(drain), 1);
+    for (int i = 0; i < kScaleRing; ++i) s_seq[i] = -1;
+    s_abort = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(tmem_slot)),
+                 "r"(nset * NT)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // the K padding of A (k >= 2 ntx8) is zero once and never written again
+  for (int i = tid; i < NA * kRows * KA * 64; i += kSThreads) {
+    const int buf = i / (kRows * KA * 64), rem = i - buf * (kRows * KA * 64);
+    const int r = rem / (KA * 64), k = rem - r * (KA * 64);
+    if (k >= 2 * synth_ntx8(ntx)) {
+      const uint32_t off = (uint32_t)(buf * ABUF + (k >> 6) * kAtomBytes) + tc::sw128_offset(r, k & 63);
+      *reinterpret_cast<__half*>(abase + off) = __float2half_rn(0.f);
+      *reinterpret_cast<__half*>(abase + off + KA * kAtomBytes) = __float2half_rn(0.f);
+    }
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // zeros visible to the MMA
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == kProdWarp) {
+    // TMA producer (one lane): the basis tiles of every N tile, tile after tile
+    if (lane == 0) {
+      int it = 0, armed[kStages];
+      for (int s = 0; s < kStages; ++s) armed[s] = -1;
+      bool ok = true;
+      for (int t = t0; t < t1 && ok; ++t)
+        for (int n = 0; n < ntile; ++n, ++it) {
+          const int s = it % kStages, use = it / kStages;
+          if (use > 0 && !(ok = tc::mbar_wait_ab(tc::smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 11, abort)))
+            break;
+          const uint32_t bar = tc::smem_u32(&full[s]);
+          tc::mbar_expect_tx(bar, 2 * KA * NBYTES_B);
+          uint8_t* st = bst + (size_t)s * 2 * KA * NBYTES_B;
+#pragma unroll
+          for (int a = 0; a < KA; ++a) {
+            tc::tma_load_2d(tc::smem_u32(st + a * NBYTES_B), &tm_hi, 64 * a, n * NT, bar);
+            tc::tma_load_2d(tc::smem_u32(st + (KA + a) * NBYTES_B), &tm_lo, 64 * a, n * NT, bar);
+          }
+          armed[s] = use;
+        }
+      // no copy may still be writing shared memory when the CTA exits
+      for (int s = 0; s < kStages; ++s)
+        if (armed[s] >= 0) tc::mbar_wait(tc::smem_u32(&full[s]), (uint32_t)(armed[s] & 1), err, 14);
+    }
+    __syncwarp();
+  } else if (warp == kMmaWarp) {
+    // MMA issuer (one lane): N tile number `it` of the run accumulates into
+    // ring slot it % nset; the A buffer is released after the tile's last MMA
+    if (lane == 0) {
+      int it = 0, ti = 0;
+      bool ok = true;
+      for (int t = t0; t < t1 && ok; ++t, ++ti) {
+        const int buf = ti % NA, ause = ti / NA;
+        if (!(ok = tc::mbar_wait_ab(tc::smem_u32(&afull[buf]), (uint32_t)(ause & 1), err, 12, abort))) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t ah = tc::smem_u32(abase + buf * ABUF), al = ah + KA * kAtomBytes;
+        for (int n = 0; n < ntile && ok; ++n, ++it) {
+          const int a = it % nset, tuse = it / nset, s = it % kStages, use = it / kStages;
+          if (tuse > 0 && !(ok = tc::mbar_wait_ab(tc::smem_u32(&tempty[a]), (uint32_t)((tuse - 1) & 1), err, 13, abort)))
+            break;
+          if (!(ok = tc::mbar_wait_ab(tc::smem_u32(&full[s]), (uint32_t)(use & 1), err, 15, abort))) break;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t acc = tmem + (uint32_t)(a * NT);
+          const uint32_t bh = tc::smem_u32(bst + (size_t)s * 2 * KA * NBYTES_B), bl = bh + KA * NBYTES_B;
+#pragma unroll
+          for (int at = 0; at < KA; ++at)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const uint32_t oa = (uint32_t)(at * kAtomBytes + k * 32), ob = (uint32_t)(at * NBYTES_B + k * 32);
+              tc::mma_f16(acc, tc::smem_desc(ah + oa), tc::smem_desc(bh + ob), IDESC, (at | k) ? 1u : 0u);
+              tc::mma_f16(acc, tc::smem_desc(ah + oa), tc::smem_desc(bl + ob), IDESC, 1u);
+              tc::mma_f16(acc, tc::smem_desc(al + oa), tc::smem_desc(bh + ob), IDESC, 1u);
+            }
+          tc::mma_commit(tc::smem_u32(&empty[s]));
+          tc::mma_commit(tc::smem_u32(&tfull[a]));
+        }
+        if (ok) tc::mma_commit(tc::smem_u32(&aempty[buf]));
+      }
+      tc::mma_commit(tc::smem_u32(drain));
+      tc::mbar_wait(tc::smem_u32(drain), 0u, err, 16);
+    }
+    __syncwarp();
+  } else if (warp >= kCW) {
+    // epilogue warps: TMEM lanes 32 ew .. 32 ew + 31 are rows of one strip,
+    // j = j0 .. j0 + 31 (y = s + nS j), written as 32 x 32 boxes by TMA
+    const int ew = warp & 3;
+    const int r0 = 32 * ew, st = r0 / J, j0 = r0 - st * J;
+    uint8_t* mystg = stg + (size_t)ew * kStageBufs * 4096;
+    const uint64_t policy = tc::policy_evict_first();
+    int it = 0, ti = 0, sb = 0;
+    bool ok = true;
+    for (int t = t0; t < t1 && ok; ++t, ++ti) {
+      const int img = t / tiles_img, s0 = (t - img * tiles_img) * NST;
+      // the tile's inverse scale, published with its tile number
+      const int slot = ti % kScaleRing;
+      bool seen = true;
+      if (lane == 0 && s_seq[slot] != ti) {
+        const unsigned long long w0 = tc::now_ns();
+        while (s_seq[slot] != ti) {
+          if (*abort) {
+            seen = false;
+            break;
+          }
+          if (tc::now_ns() - w0 > tc::kWaitNs) {
+            atomicExch(err, 18);
+            *abort = 1;
+            seen = false;
+            break;
+          }
+          __nanosleep(64);
+        }
+      }
+      if (!__shfl_sync(0xffffffffu, seen, 0)) break;
+      __threadfence_block();
+      const float inv = s_inv[slot];
+      for (int n = 0; n < ntile; ++n, ++it) {
+        const int a = it % nset, tuse = it / nset;
+        const bool ready = tc::mbar_wait_ab(tc::smem_u32(&tfull[a]), (uint32_t)(tuse & 1), err, 17, abort);
+        if (!__all_sync(0xffffffffu, ready)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t base = tmem + ((uint32_t)r0 << 16) + (uint32_t)(a * NT);
+#pragma unroll 1
+        for (int c0 = 0; c0 < NT; c0 += 32) {
+          uint32_t v[32];
+          tc::tmem_ld32(base + (uint32_t)c0, v);
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          if (c0 + 32 == NT) {
+            // the accumulator is in registers: hand it back to the MMA
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(tc::smem_u32(&tempty[a]));
+          }
+          // staging tile sb is free once its previous store has read it
+          if (lane == 0) tc::bulk_wait_read<kStageBufs - 1>();
+          __syncwarp();
+          uint8_t* tile = mystg + sb * 4096;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) {
+            const float4 o = make_float4(__uint_as_float(v[4 * q]) * inv, __uint_as_float(v[4 * q + 1]) * inv,
+                                         __uint_as_float(v[4 * q + 2]) * inv, __uint_as_float(v[4 * q + 3]) * inv);
+            *reinterpret_cast<float4*>(tile + lane * 128 + ((q ^ (lane & 7)) << 4)) = o;
+          }
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if (lane == 0) {
+            tc::tma_store_4d(&tm_img, tc::smem_u32(tile), n * NT + c0, s0 + st, j0, img, policy);
+            tc::bulk_commit();
+          }
+          sb = sb + 1 == kStageBufs ? 0 : sb + 1;
+        }
+      }
+    }
+    if (lane == 0) tc::bulk_wait_all();
+    __syncwarp();
+  } else {
+    // coefficient warps
+    int cur_img = -1, ti = 0;
+    const int br = (int)(__brev((unsigned)lane) >> 27);
+    const int nph = NST * nty;
+    const int ng = synth_ntx8(ntx) / 8;  // 8-column groups
+    const int tstr = synth_tstride(ntx);
+    WarpFFT<RJ, +1> wf;
+    wf.init(lane);
+    // phases e^{2 pi i a s / Ly} of the next tile's strips, held in registers
+    float2 phn[PHR];
+    auto load_ph = [&](int t) {
+      const int img = t / tiles_img, s0 = (t - img * tiles_img) * NST;
+#pragma unroll
+      for (int k = 0; k < PHR; ++k) {
+        const int i = tid + 32 * kCW * k;
+        if (i < nph) {
+          const int st = i / nty;
+          phn[k] = __ldg(ty + (size_t)(s0 + st) * nty + (i - st * nty));
+        }
+      }
+    };
+    if (t0 < t1) load_ph(t0);
+    for (int t = t0; t < t1; ++t, ++ti) {
+      const int img = t / tiles_img;
+      const int buf = ti % NA, ause = ti / NA;
+      bool ok = true;
+      if (ause > 0) ok = tc::mbar_wait_ab(tc::smem_u32(&aempty[buf]), (uint32_t)((ause - 1) & 1), err, 19, abort);
+      // the four warps go on or leave together (a named-barrier OR)
+      int stop;
+      asm volatile(
+          "{\n\t.reg .pred p, q;\n\t"
+          "setp.ne.s32 p, %1, 0;\n\t"
+          "bar.red.or.pred q, 1, %2, p;\n\t"
+          "selp.s32 %0, 1, 0, q;\n\t}"
+          : "=r"(stop)
+          : "r"((!ok || *abort) ? 1 : 0), "r"(32 * kCW)
+          : "memory");
+      if (stop) break;
+      // the image's spectrum (slices summed, rows padded with zeros) and the
+      // power-of-two scale of A
+      if (img != cur_img) {
+        cur_img = img;
+        if (tid == 0) s_bound = 0u;
+        const float2* Ti = T + (size_t)img * nsplit * tsz;
+        for (int i = tid; i < nty * tstr; i += 32 * kCW) {
+          const int ar = i / tstr, b = i - ar * tstr;
+          float2 v = make_float2(0.f, 0.f);
+          if (b < ntx) {
+            const size_t o = (size_t)ar * ntx + b;
+            v = __ldg(Ti + o);
+            for (int p = 1; p < nsplit; ++p) v = cadd(v, __ldg(Ti + p * tsz + o));
+          }
+          Ts[i] = v;
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(32 * kCW) : "memory");
+        // |Q[y][b]| <= w_b sum_a |T[a][b]|: the largest bound fixes the exponent
+        for (int b = tid; b < ntx; b += 32 * kCW) {
+          float sum = 0.f;
+          for (int ar = 0; ar < nty; ++ar) sum += fabsf(Ts[ar * tstr + b].x) + fabsf(Ts[ar * tstr + b].y);
+          atomicMax(&s_bound, __float_as_uint(sum * (b == 0 ? 1.f : 2.f)));
+        }
+        asm volatile("bar.sync 1, %0;" ::"r"(32 * kCW) : "memory");
+        if (tid == 0) {
+          const float bnd = __uint_as_float(s_bound);
+          int e = 0;
+          if (bnd > 0.f) {
+            int x;
+            frexpf(bnd, &x);  // bnd < 2^x
+            e = min(max(14 - x, -100), 100);
+          }
+          s_scale[0] = ldexpf(1.f, e);
+          s_scale[1] = ldexpf(1.f, -e);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < PHR; ++k) {
+        const int i = tid + 32 * kCW * k;
+        if (i < nph) ph[i] = phn[k];
+      }
+      if (t + 1 < t1) load_ph(t + 1);
+      asm volatile("bar.sync 1, %0;" ::"r"(32 * kCW) : "memory");
+      const float sc = s_scale[0];
+      if (tid == 0) {
+        s_inv[ti % kScaleRing] = s_scale[1];
+        __threadfence_block();
+        s_seq[ti % kScaleRing] = ti;
+      }
+      uint8_t* ahi = abase + buf * ABUF;
+      uint8_t* alo = ahi + KA * kAtomBytes;
+      // A of the tile: a warp task is one strip and one group of 8 columns,
+      // eight independent J-point FFTs along y; each lane then holds 8
+      // consecutive K entries of its rows, stored as 16-byte swizzled chunks
+      const int ntask = NST * ng;
+      for (int task = warp; task < ntask; task += kCW) {
+        const int st = task / ng, g8 = task - st * ng;
+        const float2* phs = ph + st * nty;
+        float2 v[8][RJ];
+#pragma unroll
+        for (int j = 0; j < RJ; ++j) {
+          const int n = lane + 32 * j;
+#pragma unroll
+          for (int i = 0; i < 8; ++i) v[i][j] = make_float2(0.f, 0.f);
+          for (int ar = n - J * ((n + A2) / J); ar <= A2; ar += J) {
+            const float2 p = phs[ar + A2];
+            const float4* trow = reinterpret_cast<const float4*>(Ts + (ar + A2) * tstr + 8 * g8);
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+              const float4 tt = trow[h];
+              v[2 * h][j] = cfma(make_float2(tt.x, tt.y), p, v[2 * h][j]);
+              v[2 * h + 1][j] = cfma(make_float2(tt.z, tt.w), p, v[2 * h + 1][j]);
+            }
+          }
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) wf.run(v[i], lane);
+#pragma unroll
+        for (int q1 = 0; q1 < RJ; ++q1) {
+          const int r = st * J + q1 + RJ * br;
+#pragma unroll
+          for (int part = 0; part < 2; ++part) {
+            uint32_t hi[4], lo[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              // weight 2 folds the conjugate half plane in, except at b = 0
+              const float w0 = (g8 == 0 && i == 0 ? 1.f : 2.f) * sc, w1 = 2.f * sc;
+              const float x0 = part ? -v[2 * i][q1].y * w0 : v[2 * i][q1].x * w0;
+              const float x1 = part ? -v[2 * i + 1][q1].y * w1 : v[2 * i + 1][q1].x * w1;
+              const __half2 h2 = __floats2half2_rn(x0, x1);
+              const float2 hf = __half22float2(h2);
+              const __half2 l2 = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+              hi[i] = *reinterpret_cast<const uint32_t*>(&h2);
+              lo[i] = *reinterpret_cast<const uint32_t*>(&l2);
+            }
+            const int c = 2 * g8 + part;  // 16-byte chunk of the row
+            const uint32_t off = (uint32_t)((c >> 3) * kAtomBytes + r * 128 + (((c & 7) ^ (r & 7)) << 4));
+            *reinterpret_cast<uint4*>(ahi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4*>(alo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          }
+        }
+      }
+      // the generic-proxy writes of A become visible to the tensor cores
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("bar.sync 1, %0;" ::"r"(32 * kCW) : "memory");
+      if (tid == 0) tc::mbar_arrive(tc::smem_u32(&afull[buf]));
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(nset * NT) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+int synth_ka(const SocsGeom& g) { return 2 * synth_ntx8(g.ntx) <= 64 ? 1 : 2; }
+// A double-buffered when shared memory holds two
+int synth_na(const SocsGeom& g) {
+  const int nst = kRows / g.J;
+  return synth_smem(synth_ka(g), g.nty, g.ntx, nst, 2).total <= kSmemMax ? 2 : 1;
+}
+}  // namespace
+
+bool synth_tc_supported(const SocsGeom& g) {
+  if (g.Ly % kRows != 0 || g.Lx % 128 != 0 || 2 * synth_ntx8(g.ntx) > 128) return false;
+  if (g.J != 32 && g.J != 64 && g.J != 128) return false;
+  const int nst = kRows / g.J;
+  if (nst * g.nty > 2 * 32 * kCW) return false;  // strip phases held two per coefficient thread
+  return synth_smem(synth_ka(g), g.nty, g.ntx, nst, 1).total <= kSmemMax;
+}
+
+int synth_tc_kp(const SocsGeom& g) { return 64 * synth_ka(g); }
+
+int synth_tc_build_basis(const SocsGeom& g, void* bhi, void* blo, cudaStream_t st) {
+  const int Kp = synth_tc_kp(g);
+  const size_t n = (size_t)g.Lx * Kp;
+  k_synth_basis<<<(int)std::min<size_t>((n + 255) / 256, 4096), 256, 0, st>>>(
+      g.Lx, g.ntx, Kp, static_cast<__half*>(bhi), static_cast<__half*>(blo));
+  KL_CUDA_TRY(cudaGetLastError());
+  return KL_OK;
+}
+
+namespace {
+template <int RJ, int KA, int NA>
+int launch_synth(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi, const void* blo,
+                 int nimg, float* images, int* err, cudaStream_t st) {
+  constexpr int NT = synth_nt(KA);
+  const int Kp = 64 * KA;
+  CUtensorMap mh, ml, mi;
+  // images as [nimg][J][nS][Lx]: row y = s + nS j of image i
+  const unsigned long long dims[4] = {(unsigned long long)g.Lx, (unsigned long long)g.nS, (unsigned long long)g.J,
+                                      (unsigned long long)nimg};
+  const unsigned long long strides[3] = {4ull * g.Lx, 4ull * g.Lx * g.nS, 4ull * g.Lx * g.Ly};
+  int rc;
+  if ((rc = tc::make_map_2b(&mh, bhi, g.Lx, Kp, 64, NT, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)) ||
+      (rc = tc::make_map_2b(&ml, blo, g.Lx, Kp, 64, NT, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)) ||
+      (rc = tc::make_map_f32_rows(&mi, images, dims, strides)))
+    return rc;
+  const SynthSmem L = synth_smem(KA, g.nty, g.ntx, kRows / (32 * RJ), NA);
+  // one CTA per SM (the TMEM ring takes up to all 512 columns)
+  const size_t sm = std::max<size_t>(L.total, 120 * 1024) + 1024;
+  auto kern = k_socs_synth_tc<RJ, KA, NA>;
+  KL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  int dev = 0, sms = 148;
+  KL_CUDA_TRY(cudaGetDevice(&dev));
+  KL_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // runs of equal length: every CTA but possibly the last takes `per` tiles
+  const int tiles = nimg * (g.Ly / kRows);
+  const int per = (tiles + sms - 1) / sms;
+  const int grid = (tiles + per - 1) / per;
+  const int nset = std::min(std::min(kTmemCols / NT, g.Lx / NT), kMaxSets);
+  kern<<<grid, kSThreads, sm, st>>>(T, g, ty, nsplit, mh, ml, mi, nimg, nset, err);
+  KL_CUDA_TRY(cudaGetLastError());
+  return KL_OK;
+}
+
+template <int RJ, int KA>
+int launch_na(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi, const void* blo,
+              int nimg, float* images, int* err, cudaStream_t st) {
+  return synth_na(g) == 2 ? launch_synth<RJ, KA, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st)
+                          : launch_synth<RJ, KA, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+}
+}  // namespace
+
+bool synth_tc_aligned(const float* images) { return (reinterpret_cast<uintptr_t>(images) & 15) == 0; }
+
+int synth_tc_launch(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi,
+                    const void* blo, int nimg, float* images, int* err, cudaStream_t st) {
+  if (nimg <= 0) return KL_OK;
+  if (!synth_tc_supported(g) || !synth_tc_aligned(images)) {
+    set_error("synth_tc_launch: geometry or image alignment outside the tensor-core synthesis");
+    return KL_ERR_UNSUPPORTED;
+  }
+  const int RJ = g.J / 32, KA = synth_ka(g);
+  if (RJ == 1 && KA == 1) return launch_na<1, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 1 && KA == 2) return launch_na<1, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 2 && KA == 1) return launch_na<2, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 2 && KA == 2) return launch_na<2, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 4 && KA == 1) return launch_na<4, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  return launch_na<4, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+}
+
+}  // namespace kl
+

@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "kl_internal.h"
+#include "kl_tc.cuh"
 #include "kl_tcc.h"
 
 namespace kl {
@@ -181,88 +182,21 @@ namespace {
 constexpr int TM = 128, TN = 128, TK = 64;
 constexpr int TILE_BYTES = TM * TK * 2;         // 16 KB, one 128 x 64 bf16 tile
 constexpr int STAGE_BYTES = 3 * TILE_BYTES;     // X1, X2, Y
-constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s bound on any pipeline wait
-
 // instruction descriptor: dense, f32 accumulate, bf16 A/B, both K-major, M=128, N=128
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
-                           ((uint32_t)(TM >> 4) << 24);
+constexpr uint32_t IDESC = tc::idesc_f16(TM, TN, true);
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ unsigned long long now_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// bounded wait; returns false (and records `code`) if the phase never completes
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int* err, int code) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = now_ns();
-  while (true) {
-    if (mbar_try(bar, parity)) return true;
-    if (now_ns() - t0 > WAIT_NS) {
-      atomicExch(err, code);
-      return false;
-    }
-    __nanosleep(128);
-  }
-}
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                            uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-          "r"(dst),
-      "l"(map), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-// K-major, 128-byte swizzle, 8-row core groups 1024 B apart
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
+using tc::mbar_arrive;
+using tc::mbar_expect_tx;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::mbar_wait_ab;
+using tc::mma_commit;
+using tc::smem_desc;
+using tc::smem_u32;
+using tc::tma_load_2d;
+using tc::tmem_ld32;
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accum) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(IDESC), "r"(accum), "r"(0), "r"(0), "r"(0), "r"(0));
-}
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-               : "memory");
-}
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
-        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
-        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
+  tc::mma_f16(tmem_d, da, db, IDESC, accum);
 }
 }  // namespace
 
@@ -281,23 +215,6 @@ constexpr int kGemmThreads = 32 * (2 + kEpiWarps);
 constexpr int EPI_BYTES = kEpiWarps * 32 * 33 * 8;  // per epilogue warp a 32 x 33 float2 tile
 constexpr int PSMEM_BYTES = kStages * STAGE_BYTES + EPI_BYTES + 1024 + 256;
 constexpr uint32_t PTMEM_COLS = 512;  // two accumulator sets of (re 128 | im 128)
-
-// bounded wait that also gives up when another role has aborted
-__device__ __forceinline__ bool mbar_wait_ab(uint32_t bar, uint32_t parity, int* err, int code,
-                                             volatile int* abort) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = now_ns();
-  while (true) {
-    if (mbar_try(bar, parity)) return true;
-    if (*abort) return false;
-    if (now_ns() - t0 > WAIT_NS) {
-      atomicExch(err, code);
-      *abort = 1;
-      return false;
-    }
-    __nanosleep(64);
-  }
-}
 
 __device__ __forceinline__ void upper_tile(int t, int nt, int& ib, int& jb) {
   int rowlen = nt;
@@ -471,41 +388,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 }
 
 namespace {
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-  static EncodeTiledFn fn = nullptr;
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)p;
-  }
-  return fn;
-}
-
 int make_map(CUtensorMap* m, const void* base, int rows, int Kp) {
-  EncodeTiledFn enc = encode_fn();
-  if (!enc) {
-    set_error("cuTensorMapEncodeTiled is unavailable");
-    return KL_ERR_CUDA;
-  }
-  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)Kp * 2};
-  const cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)TM};
-  const cuuint32_t estr[2] = {1, 1};
-  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
-                   estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
-    return KL_ERR_CUDA;
-  }
-  return KL_OK;
+  return tc::make_map_2b(m, base, rows, Kp, TK, TM, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16);
 }
 }  // namespace
 

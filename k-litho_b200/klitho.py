@@ -27,6 +27,9 @@ KL_ERR_NOT_CONVERGED = 5
 KL_ERR_IO = 6
 KL_SOCS_ADJOINT = 1
 KL_SOCS_GENERAL = 2
+KL_SYNTH_AUTO = 0
+KL_SYNTH_CUDA_CORES = 1
+KL_SYNTH_TENSOR_CORES = 2
 
 _c_int_p = ctypes.POINTER(ctypes.c_int)
 _c_float_p = ctypes.POINTER(ctypes.c_float)
@@ -74,6 +77,9 @@ def lib() -> ctypes.CDLL:
                                           ctypes.c_int]
         L.kl_socs_plan_create_ex.argtypes = L.kl_socs_plan_create.argtypes + [ctypes.c_int]
         L.kl_socs_plan_engine.argtypes = [_vp]
+        L.kl_socs_set_synthesis.argtypes = [_vp, ctypes.c_int]
+        L.kl_socs_synthesis.argtypes = [_vp, ctypes.c_int]
+        L.kl_socs_plan_status.argtypes = [_vp]
         L.kl_socs_plan_destroy.argtypes = [_vp]
         L.kl_resist_contour.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                                         ctypes.c_float, _vp, _vp, _vp, _vp, _vp]
@@ -247,6 +253,20 @@ class SocsPlan:
     def engine(self) -> str:
         """'specialised' or 'general' (kl_socs_plan_engine)."""
         return "general" if lib().kl_socs_plan_engine(self._h) == 1 else "specialised"
+
+    def set_synthesis(self, mode: str) -> None:
+        """'auto', 'cuda' or 'tensor' engine of the image synthesis
+        (kl_socs_set_synthesis)."""
+        m = {"auto": KL_SYNTH_AUTO, "cuda": KL_SYNTH_CUDA_CORES, "tensor": KL_SYNTH_TENSOR_CORES}[mode]
+        check(lib().kl_socs_set_synthesis(self._h, m), "kl_socs_set_synthesis")
+
+    def synthesis(self, nclips: int) -> str:
+        """'cuda' or 'tensor': the engine a forward of nclips clips uses."""
+        return "tensor" if lib().kl_socs_synthesis(self._h, int(nclips)) == KL_SYNTH_TENSOR_CORES else "cuda"
+
+    def status(self) -> None:
+        """Raise if a tensor-core pipeline wait timed out (kl_socs_plan_status)."""
+        check(lib().kl_socs_plan_status(self._h), "kl_socs_plan_status")
 
     def close(self) -> None:
         if getattr(self, "_h", None):
