@@ -47,15 +47,19 @@ constexpr int kCW = 4;           // coefficient warps
 constexpr int kEW = 4;           // epilogue warps
 constexpr int kSThreads = 32 * (kCW + kEW + 2);
 constexpr int kProdWarp = kCW + kEW, kMmaWarp = kCW + kEW + 1;
-constexpr int kStages = 4;       // basis tile stages (16 KB each)
+constexpr int kMaxStages = 4;    // basis unit stages
 constexpr int kStageBufs = 2;    // staging tiles per epilogue warp
 constexpr int kAtomBytes = kRows * 128;  // one 64-wide K atom of A (128 rows x 128 B)
 constexpr int kTmemCols = 512;
 constexpr int kScaleRing = 8;
 constexpr int kMaxSets = 16;     // TMEM accumulator ring slots
 
-// N tile: 64 columns for one K atom, 32 for two (16 KB basis stages)
-__host__ __device__ constexpr int synth_nt(int KA) { return KA == 1 ? 64 : 32; }
+// N tile: 256 columns for one K atom, 128 for two.  Each MMA reads its A
+// slice from shared memory once for the whole N tile, so wide tiles keep the
+// operand traffic per output byte low.  The basis streams in units of one K
+// atom of one half (hi or lo): NT rows x 128 bytes.
+__host__ __device__ constexpr int synth_nt(int KA) { return KA == 1 ? 256 : 128; }
+__host__ __device__ constexpr int synth_stages(int KA) { return KA == 1 ? 3 : 4; }
 // columns b of the row coefficients come in groups of 8: K index of column b,
 // part 0 (Re, against cos) or 1 (-Im, against sin) is 16 (b / 8) + 8 part + b % 8
 __host__ __device__ constexpr int synth_ntx8(int ntx) { return (ntx + 7) & ~7; }
@@ -74,12 +78,12 @@ __host__ __device__ inline SynthSmem synth_smem(int KA, int nty, int ntx, int ns
   const size_t abuf = 2 * (size_t)KA * kAtomBytes;           // [hi atoms][lo atoms]
   s.a = 0;
   s.b = s.a + nA * abuf;                                       // stages of [hi atoms][lo atoms]
-  const size_t stage = 2 * (size_t)KA * NT * 128;
-  s.stg = s.b + kStages * stage;                               // [kEW][kStageBufs] 4 KB tiles
+  const size_t unit = (size_t)NT * 128;
+  s.stg = s.b + synth_stages(KA) * unit;                       // [kEW][kStageBufs] 4 KB tiles
   s.ts = s.stg + (size_t)kEW * kStageBufs * 4096;              // T [nty][tstride] float2
   s.ph = s.ts + sizeof(float2) * (size_t)nty * synth_tstride(ntx);  // phases [nst][nty] float2
   s.bars = (s.ph + sizeof(float2) * (size_t)nst * nty + 15) & ~(size_t)15;
-  s.total = s.bars + 8 * (2 * kStages + 4 + 2 * kMaxSets + 1) + 64;
+  s.total = s.bars + 8 * (2 * kMaxStages + 4 + 2 * kMaxSets + 1) + 64;
   return s;
 }
 constexpr size_t kSmemMax = 227 * 1024 - 1024;  // dynamic bytes usable after the 1 KB alignment pad
@@ -112,7 +116,8 @@ __global__ void __launch_bounds__(kSThreads, 1)
   constexpr int J = 32 * RJ;
   constexpr int NST = kRows / J;  // strips per tile
   constexpr int NT = synth_nt(KA);
-  constexpr int NBYTES_B = NT * 128;  // one atom of a basis tile
+  constexpr int UNIT = NT * 128;     // one K atom of one half of a basis tile
+  constexpr int STAGES = synth_stages(KA);
   constexpr int ABUF = 2 * KA * kAtomBytes;
   constexpr int PHR = 2;              // strip phases per coefficient thread (nst * nty <= 256)
   constexpr uint32_t IDESC = tc::idesc_f16(kRows, NT, false);
@@ -124,9 +129,9 @@ __global__ void __launch_bounds__(kSThreads, 1)
   uint8_t* stg = smem + L.stg;
   float2* Ts = reinterpret_cast<float2*>(smem + L.ts);
   float2* ph = reinterpret_cast<float2*>(smem + L.ph);
-  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);  // basis stage loaded
-  uint64_t* empty = full + kStages;                              // basis stage consumed
-  uint64_t* afull = empty + kStages;                             // A buffer built
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);  // basis unit loaded
+  uint64_t* empty = full + kMaxStages;                           // basis unit consumed
+  uint64_t* afull = empty + kMaxStages;                          // A buffer built
   uint64_t* aempty = afull + 2;                                  // A buffer consumed
   uint64_t* tfull = aempty + 2;                                  // accumulator ready (ring of nset <= 16)
   uint64_t* tempty = tfull + kMaxSets;                           // accumulator drained
@@ -147,7 +152,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
   const size_t tsz = (size_t)nty * ntx;
 
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
+    for (int s = 0; s < kMaxStages; ++s) {
       tc::mbar_init(tc::smem_u32(&full[s]), 1);
       tc::mbar_init(tc::smem_u32(&empty[s]), 1);
     }
@@ -187,36 +192,37 @@ __global__ void __launch_bounds__(kSThreads, 1)
   const uint32_t tmem = *tmem_slot;
 
   if (warp == kProdWarp) {
-    // TMA producer (one lane): the basis tiles of every N tile, tile after tile
+    // TMA producer (one lane): per N tile, for each K atom the hi unit then
+    // the lo unit of the basis, tile after tile
     if (lane == 0) {
-      int it = 0, armed[kStages];
-      for (int s = 0; s < kStages; ++s) armed[s] = -1;
+      int u = 0, armed[kMaxStages];
+      for (int s = 0; s < kMaxStages; ++s) armed[s] = -1;
       bool ok = true;
       for (int t = t0; t < t1 && ok; ++t)
-        for (int n = 0; n < ntile; ++n, ++it) {
-          const int s = it % kStages, use = it / kStages;
-          if (use > 0 && !(ok = tc::mbar_wait_ab(tc::smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 11, abort)))
-            break;
-          const uint32_t bar = tc::smem_u32(&full[s]);
-          tc::mbar_expect_tx(bar, 2 * KA * NBYTES_B);
-          uint8_t* st = bst + (size_t)s * 2 * KA * NBYTES_B;
-#pragma unroll
-          for (int a = 0; a < KA; ++a) {
-            tc::tma_load_2d(tc::smem_u32(st + a * NBYTES_B), &tm_hi, 64 * a, n * NT, bar);
-            tc::tma_load_2d(tc::smem_u32(st + (KA + a) * NBYTES_B), &tm_lo, 64 * a, n * NT, bar);
+        for (int n = 0; n < ntile && ok; ++n)
+          for (int h = 0; h < 2 * KA; ++h, ++u) {
+            const int s = u % STAGES, use = u / STAGES;
+            if (use > 0 &&
+                !(ok = tc::mbar_wait_ab(tc::smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 11, abort)))
+              break;
+            const uint32_t bar = tc::smem_u32(&full[s]);
+            tc::mbar_expect_tx(bar, UNIT);
+            tc::tma_load_2d(tc::smem_u32(bst + (size_t)s * UNIT), (h & 1) ? &tm_lo : &tm_hi, 64 * (h >> 1), n * NT,
+                            bar);
+            armed[s] = use;
           }
-          armed[s] = use;
-        }
       // no copy may still be writing shared memory when the CTA exits
-      for (int s = 0; s < kStages; ++s)
+      for (int s = 0; s < STAGES; ++s)
         if (armed[s] >= 0) tc::mbar_wait(tc::smem_u32(&full[s]), (uint32_t)(armed[s] & 1), err, 14);
     }
     __syncwarp();
   } else if (warp == kMmaWarp) {
     // MMA issuer (one lane): N tile number `it` of the run accumulates into
-    // ring slot it % nset; the A buffer is released after the tile's last MMA
+    // ring slot it % nset; per K atom, the hi unit of the basis serves
+    // A_hi B_hi and A_lo B_hi, the lo unit A_hi B_lo.  The A buffer is released
+    // after the tile's last MMA.
     if (lane == 0) {
-      int it = 0, ti = 0;
+      int it = 0, ti = 0, u = 0;
       bool ok = true;
       for (int t = t0; t < t1 && ok; ++t, ++ti) {
         const int buf = ti % NA, ause = ti / NA;
@@ -224,24 +230,30 @@ __global__ void __launch_bounds__(kSThreads, 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t ah = tc::smem_u32(abase + buf * ABUF), al = ah + KA * kAtomBytes;
         for (int n = 0; n < ntile && ok; ++n, ++it) {
-          const int a = it % nset, tuse = it / nset, s = it % kStages, use = it / kStages;
+          const int a = it % nset, tuse = it / nset;
           if (tuse > 0 && !(ok = tc::mbar_wait_ab(tc::smem_u32(&tempty[a]), (uint32_t)((tuse - 1) & 1), err, 13, abort)))
             break;
-          if (!(ok = tc::mbar_wait_ab(tc::smem_u32(&full[s]), (uint32_t)(use & 1), err, 15, abort))) break;
-          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t acc = tmem + (uint32_t)(a * NT);
-          const uint32_t bh = tc::smem_u32(bst + (size_t)s * 2 * KA * NBYTES_B), bl = bh + KA * NBYTES_B;
-#pragma unroll
-          for (int at = 0; at < KA; ++at)
+          for (int h = 0; h < 2 * KA && ok; ++h, ++u) {
+            const int s = u % STAGES, use = u / STAGES;
+            if (!(ok = tc::mbar_wait_ab(tc::smem_u32(&full[s]), (uint32_t)(use & 1), err, 15, abort))) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t bb = tc::smem_u32(bst + (size_t)s * UNIT);
+            const uint32_t oa0 = (uint32_t)((h >> 1) * kAtomBytes);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-              const uint32_t oa = (uint32_t)(at * kAtomBytes + k * 32), ob = (uint32_t)(at * NBYTES_B + k * 32);
-              tc::mma_f16(acc, tc::smem_desc(ah + oa), tc::smem_desc(bh + ob), IDESC, (at | k) ? 1u : 0u);
-              tc::mma_f16(acc, tc::smem_desc(ah + oa), tc::smem_desc(bl + ob), IDESC, 1u);
-              tc::mma_f16(acc, tc::smem_desc(al + oa), tc::smem_desc(bh + ob), IDESC, 1u);
+              const uint64_t db = tc::smem_desc(bb + k * 32);
+              const uint32_t oa = oa0 + k * 32;
+              if ((h & 1) == 0) {
+                tc::mma_f16(acc, tc::smem_desc(ah + oa), db, IDESC, (h | k) ? 1u : 0u);
+                tc::mma_f16(acc, tc::smem_desc(al + oa), db, IDESC, 1u);
+              } else {
+                tc::mma_f16(acc, tc::smem_desc(ah + oa), db, IDESC, 1u);
+              }
             }
-          tc::mma_commit(tc::smem_u32(&empty[s]));
-          tc::mma_commit(tc::smem_u32(&tfull[a]));
+            tc::mma_commit(tc::smem_u32(&empty[s]));
+          }
+          if (ok) tc::mma_commit(tc::smem_u32(&tfull[a]));
         }
         if (ok) tc::mma_commit(tc::smem_u32(&aempty[buf]));
       }
@@ -494,6 +506,7 @@ int synth_na(const SocsGeom& g) {
 bool synth_tc_supported(const SocsGeom& g) {
   if (g.Ly % kRows != 0 || g.Lx % 128 != 0 || 2 * synth_ntx8(g.ntx) > 128) return false;
   if (g.J != 32 && g.J != 64 && g.J != 128) return false;
+  if (g.Lx % synth_nt(synth_ka(g)) != 0) return false;
   const int nst = kRows / g.J;
   if (nst * g.nty > 2 * 32 * kCW) return false;  // strip phases held two per coefficient thread
   return synth_smem(synth_ka(g), g.nty, g.ntx, nst, 1).total <= kSmemMax;
