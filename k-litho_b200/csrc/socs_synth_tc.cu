@@ -7,28 +7,32 @@
 // step is a real matrix product per tile of 128 rows:
 //     image[y][x] = sum_b Re(Q[y][b] e^{2 pi i b x / Lx})
 //                 = sum_k A[y][k] B[k][x],  A = [Re Q, -Im Q],  B = [cos; sin],
-// with K = 2(2Nx+1) <= 128.  It runs as tcgen05.mma kind::f16 on a 3-term FP16
-// split, A_hi B_hi + A_hi B_lo + A_lo B_hi, accumulated in FP32 in TMEM: each
-// split operand keeps 22 significant bits and the dropped A_lo B_lo term is
-// 2^-22 of a product, far below the 1e-5-of-clear-field bar.  A is scaled per
-// image by a power of two so that FP16's range holds it (the bound
-// |Q[b]| <= w_b sum_a |T[a][b]| fixes the exponent); the epilogue undoes it.
+// with K = 2 ntx8 <= 128 (ntx = 2Nx+1 columns rounded up to groups of 8).  It
+// runs as tcgen05.mma kind::f16 on a 3-term FP16 split, A_hi B_hi + A_lo B_hi
+// + A_hi B_lo, accumulated in FP32 in TMEM: each split operand keeps 22
+// significant bits and the dropped A_lo B_lo term is 2^-22 of a product, far
+// below the 1e-5-of-clear-field bar.  A is scaled per image by a power of two
+// so that FP16's range holds it (the bound |Q[b]| <= w_b sum_a |T[a][b]| fixes
+// the exponent); the epilogue undoes it.
 //
-// One persistent CTA per SM handles a contiguous run of 128-row tiles (rows
-// of 128/J strips, y = s + nS j as in k_socs_inverse), with four roles:
-//   warps 0-3  coefficient warps: load the image's band-limited intensity
-//              spectrum T into shared memory (when the image changes), build
-//              the tile's A with J-point warp FFTs along y, two columns at a
-//              time, and write the FP16 halves straight into the
-//              128-byte-swizzled K-major layout (A double-buffered when
-//              shared memory allows, so the next tile's A is built while the
-//              tensor cores work on this one);
+// The kernel is bound by shared-memory bandwidth long before the tensor
+// cores are busy, so A lives in TMEM (the MMA reads it from there, not from
+// shared memory) and shared memory carries only the basis tiles and the
+// output staging.  One persistent CTA per SM handles a contiguous run of
+// 128-row tiles (rows of 128/J strips, y = s + nS j as in k_socs_inverse):
+//   warps 0-3  coefficient warps: warp w owns TMEM lanes 32w..32w+31, i.e.
+//              rows 32w.. of the tile (strip 32w/J).  It loads the image's
+//              band-limited intensity spectrum T into shared memory (when the
+//              image changes, shared by the four warps), runs J-point warp
+//              FFTs along y for 8 columns at a time, moves each row's values
+//              to its lane and writes the FP16 halves of A into TMEM
+//              (double-buffered: the next tile's A is built while the tensor
+//              cores work on this one);
 //   warps 4-7  epilogue warps: TMEM accumulator tiles -> registers -> (scale)
 //              -> a swizzled 32 x 32 staging tile per warp -> TMA bulk store of
-//              32 image rows (the HBM-bound part: whole 128-byte lines, no
-//              load/store-unit traffic per row);
-//   warp 8     TMA producer of the basis tiles B (plan-time, L2-resident);
-//   warp 9     MMA issuer, into a ring of TMEM accumulators (512 columns).
+//              32 image rows (whole 128-byte lines);
+//   warp 8     TMA producer of the basis units (plan-time, L2-resident);
+//   warp 9     MMA issuer, into a ring of TMEM accumulators.
 // Every wait is bounded; a timeout sets the plan's status word and stops
 // every role.
 #include <cuda_fp16.h>
@@ -47,43 +51,34 @@ constexpr int kCW = 4;           // coefficient warps
 constexpr int kEW = 4;           // epilogue warps
 constexpr int kSThreads = 32 * (kCW + kEW + 2);
 constexpr int kProdWarp = kCW + kEW, kMmaWarp = kCW + kEW + 1;
-constexpr int kMaxStages = 4;    // basis unit stages
+constexpr int kStages = 6;       // basis unit stages (16 KB each)
 constexpr int kStageBufs = 2;    // staging tiles per epilogue warp
-constexpr int kAtomBytes = kRows * 128;  // one 64-wide K atom of A (128 rows x 128 B)
 constexpr int kTmemCols = 512;
 constexpr int kScaleRing = 8;
-constexpr int kMaxSets = 16;     // TMEM accumulator ring slots
+constexpr int kMaxSets = 4;      // TMEM accumulator ring slots
+constexpr int kNT = 128;         // N tile (MMA N): accumulator columns per slot
 
-// N tile: 256 columns for one K atom, 128 for two.  Each MMA reads its A
-// slice from shared memory once for the whole N tile, so wide tiles keep the
-// operand traffic per output byte low.  The basis streams in units of one K
-// atom of one half (hi or lo): NT rows x 128 bytes.
-__host__ __device__ constexpr int synth_nt(int KA) { return KA == 1 ? 256 : 128; }
-__host__ __device__ constexpr int synth_stages(int KA) { return KA == 1 ? 3 : 4; }
 // columns b of the row coefficients come in groups of 8: K index of column b,
 // part 0 (Re, against cos) or 1 (-Im, against sin) is 16 (b / 8) + 8 part + b % 8
 __host__ __device__ constexpr int synth_ntx8(int ntx) { return (ntx + 7) & ~7; }
 // row stride of the staged spectrum (float2): 8-column groups stay 16-byte
 // aligned and consecutive rows fall on different banks
 __host__ __device__ constexpr int synth_tstride(int ntx) { return synth_ntx8(ntx) + 2; }
+// TMEM columns: accumulator slots first, then two A buffers of K columns each
+// (hi halves in the first K/2, lo halves in the next K/2)
+__host__ __device__ constexpr int synth_nset(int KA) { return (kTmemCols - 2 * 64 * KA) / kNT; }
 
 struct SynthSmem {
-  size_t a, b, stg, ts, ph, bars, total;
-  int nA;  // A buffers (2 = the next tile's A is built during this tile's MMAs)
+  size_t b, stg, ts, ph, bars, total;
 };
-__host__ __device__ inline SynthSmem synth_smem(int KA, int nty, int ntx, int nst, int nA) {
+__host__ __device__ inline SynthSmem synth_smem(int nty, int ntx, int nst) {
   SynthSmem s{};
-  const int NT = synth_nt(KA);
-  s.nA = nA;
-  const size_t abuf = 2 * (size_t)KA * kAtomBytes;           // [hi atoms][lo atoms]
-  s.a = 0;
-  s.b = s.a + nA * abuf;                                       // stages of [hi atoms][lo atoms]
-  const size_t unit = (size_t)NT * 128;
-  s.stg = s.b + synth_stages(KA) * unit;                       // [kEW][kStageBufs] 4 KB tiles
+  s.b = 0;                                                     // [kStages] units of kNT x 128 B
+  s.stg = s.b + (size_t)kStages * kNT * 128;                   // [kEW][kStageBufs] 4 KB tiles
   s.ts = s.stg + (size_t)kEW * kStageBufs * 4096;              // T [nty][tstride] float2
   s.ph = s.ts + sizeof(float2) * (size_t)nty * synth_tstride(ntx);  // phases [nst][nty] float2
   s.bars = (s.ph + sizeof(float2) * (size_t)nst * nty + 15) & ~(size_t)15;
-  s.total = s.bars + 8 * (2 * kMaxStages + 4 + 2 * kMaxSets + 1) + 64;
+  s.total = s.bars + 8 * (2 * kStages + 4 + 2 * kMaxSets + 1) + 64;
   return s;
 }
 constexpr size_t kSmemMax = 227 * 1024 - 1024;  // dynamic bytes usable after the 1 KB alignment pad
@@ -108,51 +103,50 @@ __global__ void k_synth_basis(int Lx, int ntx, int Kp, __half* __restrict__ bhi,
   }
 }
 
-template <int RJ, int KA, int NA>
+template <int RJ, int KA>
 __global__ void __launch_bounds__(kSThreads, 1)
     k_socs_synth_tc(const float2* __restrict__ T, const SocsGeom g, const float2* __restrict__ ty, int nsplit,
                     const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
-                    const __grid_constant__ CUtensorMap tm_img, int nimg, int nset, int* __restrict__ err) {
+                    const __grid_constant__ CUtensorMap tm_img, int nimg, int* __restrict__ err) {
   constexpr int J = 32 * RJ;
-  constexpr int NST = kRows / J;  // strips per tile
-  constexpr int NT = synth_nt(KA);
-  constexpr int UNIT = NT * 128;     // one K atom of one half of a basis tile
-  constexpr int STAGES = synth_stages(KA);
-  constexpr int ABUF = 2 * KA * kAtomBytes;
-  constexpr int PHR = 2;              // strip phases per coefficient thread (nst * nty <= 256)
-  constexpr uint32_t IDESC = tc::idesc_f16(kRows, NT, false);
+  constexpr int NST = kRows / J;       // strips per tile
+  constexpr int UNIT = kNT * 128;      // one K atom of one half of a basis tile
+  constexpr int KC = 32 * KA;          // TMEM columns of one half of A
+  constexpr int NSET = synth_nset(KA);
+  constexpr int ACOL = NSET * kNT;     // first A column
+  constexpr int PHR = 2;               // strip phases per coefficient thread (nst * nty <= 256)
+  constexpr uint32_t IDESC = tc::idesc_f16(kRows, kNT, false);
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-  const SynthSmem L = synth_smem(KA, g.nty, g.ntx, NST, NA);
-  uint8_t* abase = smem + L.a;
+  const SynthSmem L = synth_smem(g.nty, g.ntx, NST);
   uint8_t* bst = smem + L.b;
   uint8_t* stg = smem + L.stg;
   float2* Ts = reinterpret_cast<float2*>(smem + L.ts);
   float2* ph = reinterpret_cast<float2*>(smem + L.ph);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L.bars);  // basis unit loaded
-  uint64_t* empty = full + kMaxStages;                           // basis unit consumed
-  uint64_t* afull = empty + kMaxStages;                          // A buffer built
+  uint64_t* empty = full + kStages;                              // basis unit consumed
+  uint64_t* afull = empty + kStages;                             // A buffer written
   uint64_t* aempty = afull + 2;                                  // A buffer consumed
-  uint64_t* tfull = aempty + 2;                                  // accumulator ready (ring of nset <= 16)
+  uint64_t* tfull = aempty + 2;                                  // accumulator ready
   uint64_t* tempty = tfull + kMaxSets;                           // accumulator drained
   uint64_t* drain = tempty + kMaxSets;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
   __shared__ int s_abort;
-  __shared__ float s_scale[2];          // scale of A and its inverse for the current image
-  __shared__ float s_inv[kScaleRing];   // inverse scale per tile, read by the epilogue
+  __shared__ float s_scale[2];                // scale of A and its inverse for the current image
+  __shared__ float s_inv[kScaleRing];         // inverse scale per tile, read by the epilogue
   __shared__ volatile int s_seq[kScaleRing];  // tile number whose scale a slot holds
   __shared__ unsigned s_bound;
   volatile int* abort = &s_abort;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tid = threadIdx.x;
   const int ntx = g.ntx, nty = g.nty, A2 = 2 * g.Ny;
-  const int tiles_img = g.Ly / kRows, ntile = g.Lx / NT;
+  const int tiles_img = g.Ly / kRows, ntile = g.Lx / kNT;
   const int total = nimg * tiles_img;
   const int per = (total + gridDim.x - 1) / gridDim.x;
   const int t0 = blockIdx.x * per, t1 = min(total, t0 + per);
   const size_t tsz = (size_t)nty * ntx;
 
   if (tid == 0) {
-    for (int s = 0; s < kMaxStages; ++s) {
+    for (int s = 0; s < kStages; ++s) {
       tc::mbar_init(tc::smem_u32(&full[s]), 1);
       tc::mbar_init(tc::smem_u32(&empty[s]), 1);
     }
@@ -171,21 +165,10 @@ __global__ void __launch_bounds__(kSThreads, 1)
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(tmem_slot)),
-                 "r"(nset * NT)
+                 "r"(kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  // the K padding of A (k >= 2 ntx8) is zero once and never written again
-  for (int i = tid; i < NA * kRows * KA * 64; i += kSThreads) {
-    const int buf = i / (kRows * KA * 64), rem = i - buf * (kRows * KA * 64);
-    const int r = rem / (KA * 64), k = rem - r * (KA * 64);
-    if (k >= 2 * synth_ntx8(ntx)) {
-      const uint32_t off = (uint32_t)(buf * ABUF + (k >> 6) * kAtomBytes) + tc::sw128_offset(r, k & 63);
-      *reinterpret_cast<__half*>(abase + off) = __float2half_rn(0.f);
-      *reinterpret_cast<__half*>(abase + off + KA * kAtomBytes) = __float2half_rn(0.f);
-    }
-  }
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // zeros visible to the MMA
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -195,60 +178,60 @@ __global__ void __launch_bounds__(kSThreads, 1)
     // TMA producer (one lane): per N tile, for each K atom the hi unit then
     // the lo unit of the basis, tile after tile
     if (lane == 0) {
-      int u = 0, armed[kMaxStages];
-      for (int s = 0; s < kMaxStages; ++s) armed[s] = -1;
+      int u = 0, armed[kStages];
+      for (int s = 0; s < kStages; ++s) armed[s] = -1;
       bool ok = true;
       for (int t = t0; t < t1 && ok; ++t)
         for (int n = 0; n < ntile && ok; ++n)
           for (int h = 0; h < 2 * KA; ++h, ++u) {
-            const int s = u % STAGES, use = u / STAGES;
+            const int s = u % kStages, use = u / kStages;
             if (use > 0 &&
                 !(ok = tc::mbar_wait_ab(tc::smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 11, abort)))
               break;
             const uint32_t bar = tc::smem_u32(&full[s]);
             tc::mbar_expect_tx(bar, UNIT);
-            tc::tma_load_2d(tc::smem_u32(bst + (size_t)s * UNIT), (h & 1) ? &tm_lo : &tm_hi, 64 * (h >> 1), n * NT,
+            tc::tma_load_2d(tc::smem_u32(bst + (size_t)s * UNIT), (h & 1) ? &tm_lo : &tm_hi, 64 * (h >> 1), n * kNT,
                             bar);
             armed[s] = use;
           }
       // no copy may still be writing shared memory when the CTA exits
-      for (int s = 0; s < STAGES; ++s)
+      for (int s = 0; s < kStages; ++s)
         if (armed[s] >= 0) tc::mbar_wait(tc::smem_u32(&full[s]), (uint32_t)(armed[s] & 1), err, 14);
     }
     __syncwarp();
   } else if (warp == kMmaWarp) {
     // MMA issuer (one lane): N tile number `it` of the run accumulates into
-    // ring slot it % nset; per K atom, the hi unit of the basis serves
-    // A_hi B_hi and A_lo B_hi, the lo unit A_hi B_lo.  The A buffer is released
-    // after the tile's last MMA.
+    // ring slot it % NSET; per K atom, the hi unit of the basis serves
+    // A_hi B_hi and A_lo B_hi, the lo unit A_hi B_lo (A from TMEM).  The A
+    // buffer is released after the tile's last MMA.
     if (lane == 0) {
       int it = 0, ti = 0, u = 0;
       bool ok = true;
       for (int t = t0; t < t1 && ok; ++t, ++ti) {
-        const int buf = ti % NA, ause = ti / NA;
+        const int buf = ti & 1, ause = ti >> 1;
         if (!(ok = tc::mbar_wait_ab(tc::smem_u32(&afull[buf]), (uint32_t)(ause & 1), err, 12, abort))) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t ah = tc::smem_u32(abase + buf * ABUF), al = ah + KA * kAtomBytes;
+        const uint32_t ah = tmem + (uint32_t)(ACOL + buf * 2 * KC), al = ah + KC;
         for (int n = 0; n < ntile && ok; ++n, ++it) {
-          const int a = it % nset, tuse = it / nset;
+          const int a = it % NSET, tuse = it / NSET;
           if (tuse > 0 && !(ok = tc::mbar_wait_ab(tc::smem_u32(&tempty[a]), (uint32_t)((tuse - 1) & 1), err, 13, abort)))
             break;
-          const uint32_t acc = tmem + (uint32_t)(a * NT);
+          const uint32_t acc = tmem + (uint32_t)(a * kNT);
           for (int h = 0; h < 2 * KA && ok; ++h, ++u) {
-            const int s = u % STAGES, use = u / STAGES;
+            const int s = u % kStages, use = u / kStages;
             if (!(ok = tc::mbar_wait_ab(tc::smem_u32(&full[s]), (uint32_t)(use & 1), err, 15, abort))) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t bb = tc::smem_u32(bst + (size_t)s * UNIT);
-            const uint32_t oa0 = (uint32_t)((h >> 1) * kAtomBytes);
+            const uint32_t ac0 = (uint32_t)(32 * (h >> 1));  // A column of the atom's first k step
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
               const uint64_t db = tc::smem_desc(bb + k * 32);
-              const uint32_t oa = oa0 + k * 32;
+              const uint32_t ac = ac0 + 8 * k;  // 16 K elements = 8 columns
               if ((h & 1) == 0) {
-                tc::mma_f16(acc, tc::smem_desc(ah + oa), db, IDESC, (h | k) ? 1u : 0u);
-                tc::mma_f16(acc, tc::smem_desc(al + oa), db, IDESC, 1u);
+                tc::mma_f16_ts(acc, ah + ac, db, IDESC, (h | k) ? 1u : 0u);
+                tc::mma_f16_ts(acc, al + ac, db, IDESC, 1u);
               } else {
-                tc::mma_f16(acc, tc::smem_desc(ah + oa), db, IDESC, 1u);
+                tc::mma_f16_ts(acc, ah + ac, db, IDESC, 1u);
               }
             }
             tc::mma_commit(tc::smem_u32(&empty[s]));
@@ -295,20 +278,20 @@ __global__ void __launch_bounds__(kSThreads, 1)
       __threadfence_block();
       const float inv = s_inv[slot];
       for (int n = 0; n < ntile; ++n, ++it) {
-        const int a = it % nset, tuse = it / nset;
+        const int a = it % NSET, tuse = it / NSET;
         const bool ready = tc::mbar_wait_ab(tc::smem_u32(&tfull[a]), (uint32_t)(tuse & 1), err, 17, abort);
         if (!__all_sync(0xffffffffu, ready)) {
           ok = false;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t base = tmem + ((uint32_t)r0 << 16) + (uint32_t)(a * NT);
+        const uint32_t base = tmem + ((uint32_t)r0 << 16) + (uint32_t)(a * kNT);
 #pragma unroll 1
-        for (int c0 = 0; c0 < NT; c0 += 32) {
+        for (int c0 = 0; c0 < kNT; c0 += 32) {
           uint32_t v[32];
           tc::tmem_ld32(base + (uint32_t)c0, v);
           asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-          if (c0 + 32 == NT) {
+          if (c0 + 32 == kNT) {
             // the accumulator is in registers: hand it back to the MMA
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
@@ -327,7 +310,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
           asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
           __syncwarp();
           if (lane == 0) {
-            tc::tma_store_4d(&tm_img, tc::smem_u32(tile), n * NT + c0, s0 + st, j0, img, policy);
+            tc::tma_store_4d(&tm_img, tc::smem_u32(tile), n * kNT + c0, s0 + st, j0, img, policy);
             tc::bulk_commit();
           }
           sb = sb + 1 == kStageBufs ? 0 : sb + 1;
@@ -337,14 +320,25 @@ __global__ void __launch_bounds__(kSThreads, 1)
     if (lane == 0) tc::bulk_wait_all();
     __syncwarp();
   } else {
-    // coefficient warps
-    int cur_img = -1, ti = 0;
-    const int br = (int)(__brev((unsigned)lane) >> 27);
+    // coefficient warps: warp w writes TMEM lanes 32w .. 32w + 31, rows
+    // jw .. jw + 31 of strip sw of the tile (all 8-column groups)
+    const int sw = (32 * warp) / J, jw = 32 * warp - sw * J;
+    // lane of the FFT output that holds row jw + lane, and its register
+    const int R = jw + lane, qsel = R % RJ, src = (int)(__brev((unsigned)(R / RJ)) >> 27);
+    const uint32_t lanebase = tmem + ((uint32_t)(32 * warp) << 16);
     const int nph = NST * nty;
     const int ng = synth_ntx8(ntx) / 8;  // 8-column groups
     const int tstr = synth_tstride(ntx);
+    int cur_img = -1, ti = 0;
     WarpFFT<RJ, +1> wf;
     wf.init(lane);
+    // the K padding (columns 8 ng .. KC of each half) is zero once for both buffers
+    {
+      uint32_t z[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      for (int c = 8 * ng; c < KC; c += 8)
+        for (int hb = 0; hb < 4; ++hb) tc::tmem_st8(lanebase + (uint32_t)(ACOL + hb * KC + c), z);
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+    }
     // phases e^{2 pi i a s / Ly} of the next tile's strips, held in registers
     float2 phn[PHR];
     auto load_ph = [&](int t) {
@@ -361,7 +355,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
     if (t0 < t1) load_ph(t0);
     for (int t = t0; t < t1; ++t, ++ti) {
       const int img = t / tiles_img;
-      const int buf = ti % NA, ause = ti / NA;
+      const int buf = ti & 1, ause = ti >> 1;
       bool ok = true;
       if (ause > 0) ok = tc::mbar_wait_ab(tc::smem_u32(&aempty[buf]), (uint32_t)((ause - 1) & 1), err, 19, abort);
       // the four warps go on or leave together (a named-barrier OR)
@@ -375,6 +369,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
           : "r"((!ok || *abort) ? 1 : 0), "r"(32 * kCW)
           : "memory");
       if (stop) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       // the image's spectrum (slices summed, rows padded with zeros) and the
       // power-of-two scale of A
       if (img != cur_img) {
@@ -424,15 +419,12 @@ __global__ void __launch_bounds__(kSThreads, 1)
         __threadfence_block();
         s_seq[ti % kScaleRing] = ti;
       }
-      uint8_t* ahi = abase + buf * ABUF;
-      uint8_t* alo = ahi + KA * kAtomBytes;
-      // A of the tile: a warp task is one strip and one group of 8 columns,
-      // eight independent J-point FFTs along y; each lane then holds 8
-      // consecutive K entries of its rows, stored as 16-byte swizzled chunks
-      const int ntask = NST * ng;
-      for (int task = warp; task < ntask; task += kCW) {
-        const int st = task / ng, g8 = task - st * ng;
-        const float2* phs = ph + st * nty;
+      const uint32_t ahi = lanebase + (uint32_t)(ACOL + buf * 2 * KC), alo = ahi + KC;
+      const float2* phs = ph + sw * nty;
+      // per group of 8 columns: eight independent J-point FFTs along y, each
+      // lane then fetches the values of its own row and writes 8 columns of
+      // A_hi and A_lo (16 K entries) to TMEM
+      for (int g8 = 0; g8 < ng; ++g8) {
         float2 v[8][RJ];
 #pragma unroll
         for (int j = 0; j < RJ; ++j) {
@@ -452,33 +444,37 @@ __global__ void __launch_bounds__(kSThreads, 1)
         }
 #pragma unroll
         for (int i = 0; i < 8; ++i) wf.run(v[i], lane);
+        uint32_t hi[8], lo[8];
 #pragma unroll
-        for (int q1 = 0; q1 < RJ; ++q1) {
-          const int r = st * J + q1 + RJ * br;
+        for (int i = 0; i < 8; i += 2) {
+          float2 s0v = make_float2(0.f, 0.f), s1v = make_float2(0.f, 0.f);
 #pragma unroll
-          for (int part = 0; part < 2; ++part) {
-            uint32_t hi[4], lo[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              // weight 2 folds the conjugate half plane in, except at b = 0
-              const float w0 = (g8 == 0 && i == 0 ? 1.f : 2.f) * sc, w1 = 2.f * sc;
-              const float x0 = part ? -v[2 * i][q1].y * w0 : v[2 * i][q1].x * w0;
-              const float x1 = part ? -v[2 * i + 1][q1].y * w1 : v[2 * i + 1][q1].x * w1;
-              const __half2 h2 = __floats2half2_rn(x0, x1);
-              const float2 hf = __half22float2(h2);
-              const __half2 l2 = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
-              hi[i] = *reinterpret_cast<const uint32_t*>(&h2);
-              lo[i] = *reinterpret_cast<const uint32_t*>(&l2);
+          for (int q = 0; q < RJ; ++q) {
+            const float ax = __shfl_sync(0xffffffffu, v[i][q].x, src), ay = __shfl_sync(0xffffffffu, v[i][q].y, src);
+            const float bx = __shfl_sync(0xffffffffu, v[i + 1][q].x, src);
+            const float by = __shfl_sync(0xffffffffu, v[i + 1][q].y, src);
+            if (q == qsel) {
+              s0v = make_float2(ax, ay);
+              s1v = make_float2(bx, by);
             }
-            const int c = 2 * g8 + part;  // 16-byte chunk of the row
-            const uint32_t off = (uint32_t)((c >> 3) * kAtomBytes + r * 128 + (((c & 7) ^ (r & 7)) << 4));
-            *reinterpret_cast<uint4*>(ahi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<uint4*>(alo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
           }
+          // weight 2 folds the conjugate half plane in, except at b = 0
+          const float w0 = (g8 == 0 && i == 0 ? 1.f : 2.f) * sc, w1 = 2.f * sc;
+          const float re0 = s0v.x * w0, re1 = s1v.x * w1, im0 = -s0v.y * w0, im1 = -s1v.y * w1;
+          const __half2 hr = __floats2half2_rn(re0, re1), hm = __floats2half2_rn(im0, im1);
+          const float2 fr = __half22float2(hr), fm = __half22float2(hm);
+          const __half2 lr = __floats2half2_rn(re0 - fr.x, re1 - fr.y), lm = __floats2half2_rn(im0 - fm.x, im1 - fm.y);
+          hi[i / 2] = *reinterpret_cast<const uint32_t*>(&hr);
+          hi[4 + i / 2] = *reinterpret_cast<const uint32_t*>(&hm);
+          lo[i / 2] = *reinterpret_cast<const uint32_t*>(&lr);
+          lo[4 + i / 2] = *reinterpret_cast<const uint32_t*>(&lm);
         }
+        tc::tmem_st8(ahi + (uint32_t)(8 * g8), hi);
+        tc::tmem_st8(alo + (uint32_t)(8 * g8), lo);
       }
-      // the generic-proxy writes of A become visible to the tensor cores
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      // A complete in TMEM before the MMA issuer is told
+      asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       asm volatile("bar.sync 1, %0;" ::"r"(32 * kCW) : "memory");
       if (tid == 0) tc::mbar_arrive(tc::smem_u32(&afull[buf]));
     }
@@ -487,7 +483,7 @@ __global__ void __launch_bounds__(kSThreads, 1)
   __syncthreads();
   if (warp == 0) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(nset * NT) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
   }
 }
 
@@ -496,20 +492,14 @@ __global__ void __launch_bounds__(kSThreads, 1)
 // ---------------------------------------------------------------------------
 namespace {
 int synth_ka(const SocsGeom& g) { return 2 * synth_ntx8(g.ntx) <= 64 ? 1 : 2; }
-// A double-buffered when shared memory holds two
-int synth_na(const SocsGeom& g) {
-  const int nst = kRows / g.J;
-  return synth_smem(synth_ka(g), g.nty, g.ntx, nst, 2).total <= kSmemMax ? 2 : 1;
-}
 }  // namespace
 
 bool synth_tc_supported(const SocsGeom& g) {
-  if (g.Ly % kRows != 0 || g.Lx % 128 != 0 || 2 * synth_ntx8(g.ntx) > 128) return false;
+  if (g.Ly % kRows != 0 || g.Lx % kNT != 0 || 2 * synth_ntx8(g.ntx) > 128) return false;
   if (g.J != 32 && g.J != 64 && g.J != 128) return false;
-  if (g.Lx % synth_nt(synth_ka(g)) != 0) return false;
   const int nst = kRows / g.J;
   if (nst * g.nty > 2 * 32 * kCW) return false;  // strip phases held two per coefficient thread
-  return synth_smem(synth_ka(g), g.nty, g.ntx, nst, 1).total <= kSmemMax;
+  return synth_smem(g.nty, g.ntx, nst).total <= kSmemMax;
 }
 
 int synth_tc_kp(const SocsGeom& g) { return 64 * synth_ka(g); }
@@ -524,10 +514,9 @@ int synth_tc_build_basis(const SocsGeom& g, void* bhi, void* blo, cudaStream_t s
 }
 
 namespace {
-template <int RJ, int KA, int NA>
+template <int RJ, int KA>
 int launch_synth(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi, const void* blo,
                  int nimg, float* images, int* err, cudaStream_t st) {
-  constexpr int NT = synth_nt(KA);
   const int Kp = 64 * KA;
   CUtensorMap mh, ml, mi;
   // images as [nimg][J][nS][Lx]: row y = s + nS j of image i
@@ -535,14 +524,15 @@ int launch_synth(const SocsGeom& g, const float2* T, const float2* ty, int nspli
                                       (unsigned long long)nimg};
   const unsigned long long strides[3] = {4ull * g.Lx, 4ull * g.Lx * g.nS, 4ull * g.Lx * g.Ly};
   int rc;
-  if ((rc = tc::make_map_2b(&mh, bhi, g.Lx, Kp, 64, NT, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)) ||
-      (rc = tc::make_map_2b(&ml, blo, g.Lx, Kp, 64, NT, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)) ||
+  if ((rc = tc::make_map_2b(&mh, bhi, g.Lx, Kp, 64, kNT, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)) ||
+      (rc = tc::make_map_2b(&ml, blo, g.Lx, Kp, 64, kNT, CU_TENSOR_MAP_DATA_TYPE_FLOAT16)) ||
       (rc = tc::make_map_f32_rows(&mi, images, dims, strides)))
     return rc;
-  const SynthSmem L = synth_smem(KA, g.nty, g.ntx, kRows / (32 * RJ), NA);
-  // one CTA per SM (the TMEM ring takes up to all 512 columns)
+  const SynthSmem L = synth_smem(g.nty, g.ntx, kRows / (32 * RJ));
+  // one CTA per SM: the kernel allocates all 512 TMEM columns, and the shared
+  // memory request keeps a second CTA off the SM
   const size_t sm = std::max<size_t>(L.total, 120 * 1024) + 1024;
-  auto kern = k_socs_synth_tc<RJ, KA, NA>;
+  auto kern = k_socs_synth_tc<RJ, KA>;
   KL_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   int dev = 0, sms = 148;
   KL_CUDA_TRY(cudaGetDevice(&dev));
@@ -551,17 +541,9 @@ int launch_synth(const SocsGeom& g, const float2* T, const float2* ty, int nspli
   const int tiles = nimg * (g.Ly / kRows);
   const int per = (tiles + sms - 1) / sms;
   const int grid = (tiles + per - 1) / per;
-  const int nset = std::min(std::min(kTmemCols / NT, g.Lx / NT), kMaxSets);
-  kern<<<grid, kSThreads, sm, st>>>(T, g, ty, nsplit, mh, ml, mi, nimg, nset, err);
+  kern<<<grid, kSThreads, sm, st>>>(T, g, ty, nsplit, mh, ml, mi, nimg, err);
   KL_CUDA_TRY(cudaGetLastError());
   return KL_OK;
-}
-
-template <int RJ, int KA>
-int launch_na(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi, const void* blo,
-              int nimg, float* images, int* err, cudaStream_t st) {
-  return synth_na(g) == 2 ? launch_synth<RJ, KA, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st)
-                          : launch_synth<RJ, KA, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
 }
 }  // namespace
 
@@ -575,13 +557,12 @@ int synth_tc_launch(const SocsGeom& g, const float2* T, const float2* ty, int ns
     return KL_ERR_UNSUPPORTED;
   }
   const int RJ = g.J / 32, KA = synth_ka(g);
-  if (RJ == 1 && KA == 1) return launch_na<1, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
-  if (RJ == 1 && KA == 2) return launch_na<1, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
-  if (RJ == 2 && KA == 1) return launch_na<2, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
-  if (RJ == 2 && KA == 2) return launch_na<2, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
-  if (RJ == 4 && KA == 1) return launch_na<4, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
-  return launch_na<4, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 1 && KA == 1) return launch_synth<1, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 1 && KA == 2) return launch_synth<1, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 2 && KA == 1) return launch_synth<2, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 2 && KA == 2) return launch_synth<2, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  if (RJ == 4 && KA == 1) return launch_synth<4, 1>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
+  return launch_synth<4, 2>(g, T, ty, nsplit, bhi, blo, nimg, images, err, st);
 }
 
 }  // namespace kl
-
