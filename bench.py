@@ -301,8 +301,8 @@ def run_ours(args):
         stage_ms += np.array(t)
         stage_n += np.array(c)
         per_class.append({"L": L, "clips": n, "fwd_ms": t[0] / max(c[0], 1), "spectral_ms": t[1] / max(c[1], 1),
-                          "inverse_ms": t[2] / max(c[2], 1), "tuned_kernel_slices": ns,
-                          "tuned_strips_per_cta": spc})
+                          "synthesis_ms": t[2] / max(c[2], 1), "tuned_kernel_slices": ns,
+                          "tuned_strips_per_cta": spc, "synthesis": p.synthesis(n)})
         p.enable_timing(False)
     # ... and their spans inside the graph, where the size classes overlap
     # (stage events captured into a separate graph)
@@ -325,7 +325,7 @@ def run_ours(args):
     value = total_equiv / (ms_per_step / 1e3)
 
     # roofline of the dominant kernel (largest share of device time)
-    names = ["socs_forward", "socs_spectral", "socs_inverse"]
+    names = ["socs_forward", "socs_spectral", "socs_synthesis"]
     dom = int(np.argmax(stage_ms))
     bytes_per_step = [sum(4 * L * L * n for L, n in CLASSES),
                       0,
@@ -341,8 +341,10 @@ def run_ours(args):
                 "frac": round(achieved / peak, 4),
                 "traffic": (int(TRAFFIC_PER_ALGORITHMIC_BYTE[names[dom]] * bytes_per_step[dom] / launches_per_step)
                             if names[dom] in TRAFFIC_PER_ALGORITHMIC_BYTE else None),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the 2048^2 and "
-                                  "1024^2 captures (profiles/socs_inverse_full.md), scaled by pixels",
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_socs_synth_tc "
+                                  "captures at 2048^2 and 1024^2 (profiles/socs_synth_tc_full.md), scaled by pixels",
+                "kernels": sorted({("k_socs_synth_tc" if c["synthesis"] == "tensor" else "k_socs_inverse")
+                                   for c in per_class}),
                 "algorithmic_bytes_per_launch": int(bytes_per_step[dom] / launches_per_step)}
     else:
         roof = {"kernel": names[dom], "bound": "compute", "achieved": None, "peak": None,
@@ -424,10 +426,10 @@ def run_ours(args):
 
 
 # DRAM bytes per algorithmic byte measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum): synthesis on 48 x 2048^2 + 144 x 1024^2 images, forward
-# on 48 clips of 1024^2; both kernels stream their clip data once, so traffic
-# scales with the pixels of a launch.
-TRAFFIC_PER_ALGORITHMIC_BYTE = {"socs_inverse": (3.376 + 544.117 + 4.802 + 749.687) / (603.98 + 805.31),
+# dram__bytes_write.sum): tensor-core synthesis on 48 x 2048^2 + 144 x 1024^2
+# images, forward on 48 clips of 1024^2; both kernels stream their clip data
+# once, so traffic scales with the pixels of a launch.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {"socs_synthesis": (5.847 + 746.890 + 3.649 + 546.218) / (805.31 + 603.98),
                                 "socs_forward": (201.372 + 4.389) / 201.33}
 
 

@@ -141,6 +141,8 @@ int kl_socs_plan_engine(kl_socs_plan plan);
  * the tensor cores (periods with Lx, Ly multiples of 128 and 2(2Nx+1) <= 128;
  * image error of the same order as the CUDA-core engine's); KL_SYNTH_AUTO
  * (the default), the engine kl_socs_autotune picked, else the CUDA cores.
+ * The gradient synthesis of kl_socs_vjp runs on the tensor cores wherever
+ * the geometry allows, unless KL_SYNTH_CUDA_CORES is set.
  * Returns KL_ERR_UNSUPPORTED for the tensor-core engine on other geometries
  * and on general-pipeline plans.  No counterpart in the reference. */
 #define KL_SYNTH_AUTO 0

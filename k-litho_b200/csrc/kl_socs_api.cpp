@@ -382,7 +382,12 @@ int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nc
                                     ns2, p->gam, st)))
     return rc;
   if ((rc = kl::vjp_launch_gradT(g, p->gam, nclips, p->nsets * ns2, p->Tg, st))) return rc;
-  if ((rc = kl::socs_launch_inverse(g, p->tx, p->ty, p->Tg, nclips, 1, 1, grad, st))) return rc;
+  // the gradient is a band-limited synthesis like the image: on the tensor
+  // cores unless the plan asks for the CUDA-core engine
+  const bool tcg = p->bhi && p->synth != KL_SYNTH_CUDA_CORES && kl::synth_tc_aligned(grad);
+  rc = tcg ? kl::synth_tc_launch(g, p->Tg, p->ty, 1, p->bhi, p->blo, nclips, grad, p->status, st)
+           : kl::socs_launch_inverse(g, p->tx, p->ty, p->Tg, nclips, 1, 1, grad, st);
+  if (rc) return rc;
   p->last_vjp_clips = nclips;
   return KL_OK;
 }

@@ -31,11 +31,12 @@ def kernels(L, nk, defocus_nm=0.0):
     return src, Nx, Ny, krn.astype(np.complex64), sc, df
 
 
-def run_vjp(masks, targets, sets, Nx, Ny, want_image=True):
+def run_vjp(masks, targets, sets, Nx, Ny, want_image=True, synthesis="auto"):
     import torch
     n, Ly, Lx = masks.shape
     nk = sets[0][0].shape[0]
     plan = K.SocsPlan(Lx, Ly, Nx, Ny, nk, nsets=len(sets), max_clips=n, adjoint=True)
+    plan.set_synthesis(synthesis)
     for i, (k, s) in enumerate(sets):
         plan.set_kernels(i, k, s)
     md = torch.from_numpy(np.ascontiguousarray(masks, dtype=np.float32)).cuda()
@@ -191,3 +192,16 @@ def test_vjp_image_equals_forward(cuda):
     plan.forward(md, out)
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), img)
+
+
+@pytest.mark.parametrize("L", [512, 1024])
+def test_vjp_gradient_synthesis_engines_agree(cuda, L):
+    # the gradient's band-limited synthesis on the tensor cores (default) and
+    # on the CUDA cores: same gradient within the FP32 tolerance
+    _, Nx, Ny, krn, sc, _ = kernels(L, 24)
+    masks = np.stack([synth.smooth_mask(L, seed=s) for s in (31, 32)])
+    tgts = np.stack([synth.rect_mask(L, 20, seed=s) for s in (33, 34)])
+    _, g_tc, loss_tc, _ = run_vjp(masks, tgts, [(krn, sc)], Nx, Ny, want_image=False)
+    _, g_cu, loss_cu, _ = run_vjp(masks, tgts, [(krn, sc)], Nx, Ny, want_image=False, synthesis="cuda")
+    assert np.array_equal(loss_tc, loss_cu)
+    assert np.abs(g_tc - g_cu).max() <= 1e-5 * np.abs(g_cu).max()
