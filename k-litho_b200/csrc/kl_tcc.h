@@ -39,17 +39,16 @@ void tcc_pupil_host(const std::vector<SrcPoint>& pts, const PupilParams& pp, dou
 // Device: A[f][s] = sqrt(J_s) P(f, s) in FP32 (N x S complex64, row-major).
 int tcc_build_A(const SrcPoint* pts_dev, const PupilParams& pp, float2* A, cudaStream_t st);
 
-// Device: bf16 split operands for TCC = A A^H on the tensor cores.
-// X1, X2, Y are N x Kp bf16, Kp = round_up(6 S, 64).
-int tcc_split_operands(const float2* A, int N, int S, int Kp, void* X1, void* X2, void* Y,
-                       cudaStream_t st);
+// Device: bf16 split operands for TCC = A A^H on the tensor cores: four
+// planes X1h, X2h, X1l, X2l of N x K2p bf16 in one buffer (4 N K2p elements),
+// K2p = round_up(2 S, 64) = tcc_kp(S).
+int tcc_split_operands(const float2* A, int N, int S, int K2p, void* ops, cudaStream_t st);
 int tcc_kp(int S);
 
-// Device: Hermitian TCC (N x N complex64) = X1 Y^T + i X2 Y^T by tcgen05 MMA,
-// upper tiles computed, lower tiles mirrored.  err_dev receives a nonzero code
-// if a pipeline wait gave up.
-int tcc_gemm_tc(const void* X1, const void* X2, const void* Y, int N, int Kp, float2* tcc,
-                int* err_dev, cudaStream_t st);
+// Device: Hermitian TCC (N x N complex64) = X1 Y^T + i X2 Y^T (Y = X1, three
+// split terms) by tcgen05 MMA, upper tiles computed, lower tiles mirrored.
+// err_dev receives a nonzero code if a pipeline wait gave up.
+int tcc_gemm_tc(const void* ops, int N, int K2p, float2* tcc, int* err_dev, cudaStream_t st);
 
 // Device: FP64 TCC by direct accumulation over source points (the plain FP64
 // path): tcc[i][j] = sum_s J_s P[i][s] conj(P[j][s]).  P is N x S complex128.

@@ -167,22 +167,16 @@ int kl_tcc_build(kl_tcc_plan p, void* tcc_dev, void* stream) {
     if (rc) return rc;
     return KL_OK;
   }
-  const int Kp = kl::tcc_kp(S);
-  void *X1 = nullptr, *X2 = nullptr, *Y = nullptr;
-  const size_t ob = sizeof(uint16_t) * (size_t)N * Kp;
+  const int K2p = kl::tcc_kp(S);
+  void* ops = nullptr;
   int rc;
-  if ((rc = kl::scratch_alloc(&X1, ob, st, "split operand")) || (rc = kl::scratch_alloc(&X2, ob, st, "split operand")) ||
-      (rc = kl::scratch_alloc(&Y, ob, st, "split operand"))) {
-    kl::scratch_free(X1, st);
-    kl::scratch_free(X2, st);
-    return rc;
-  }
+  if ((rc = kl::scratch_alloc(&ops, sizeof(uint16_t) * 4 * (size_t)N * K2p, st, "split operands"))) return rc;
   if (cudaMemsetAsync(p->err, 0, sizeof(int), st) != cudaSuccess) {
     kl::set_error(std::string("kl_tcc_build: ") + cudaGetErrorString(cudaGetLastError()));
     rc = KL_ERR_CUDA;
   }
-  if (!rc) rc = kl::tcc_split_operands(p->A, N, S, Kp, X1, X2, Y, st);
-  if (!rc) rc = kl::tcc_gemm_tc(X1, X2, Y, N, Kp, (float2*)tcc_dev, p->err, st);
+  if (!rc) rc = kl::tcc_split_operands(p->A, N, S, K2p, ops, st);
+  if (!rc) rc = kl::tcc_gemm_tc(ops, N, K2p, (float2*)tcc_dev, p->err, st);
   int herr = 0;
   if (!rc) {
     cudaMemcpyAsync(&herr, p->err, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -194,9 +188,7 @@ int kl_tcc_build(kl_tcc_plan p, void* tcc_dev, void* stream) {
       rc = KL_ERR_CUDA;
     }
   }
-  kl::scratch_free(X1, st);
-  kl::scratch_free(X2, st);
-  kl::scratch_free(Y, st);
+  kl::scratch_free(ops, st);
   return rc;
 }
 

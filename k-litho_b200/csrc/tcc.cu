@@ -134,43 +134,45 @@ int tcc_build_A(const SrcPoint* pts_dev, const PupilParams& pp, float2* A, cudaS
 // ---------------------------------------------------------------------------
 // bf16 split operands
 // ---------------------------------------------------------------------------
-int tcc_kp(int S) { return ((6 * S + 63) / 64) * 64; }
+// Four planes of N x K2p bf16, K2p = round_up(2 S, 64), one after another in
+// one buffer: X1h, X2h, X1l, X2l.  With a = A[f][s] split as
+// a = ah + al (ah = bf16(a), al = bf16(a - ah)), the K index k < S holds the
+// real part of source point s = k, S <= k < 2S the imaginary part of s = k - S:
+//   X1 = (ar, ai), X2 = (ai, -ar), each as hi and lo planes, and Y = X1, so
+//   Re TCC = X1h Yh^T + X1h Yl^T + X1l Yh^T, Im TCC = the same with X2
+// (the three split terms; the lo x lo term is dropped), Y's tiles being X1's
+// rows of the other tile index.  Each hi tile is loaded once per k block and
+// used by two MMAs.
+int tcc_kp(int S) { return ((2 * S + 63) / 64) * 64; }
 
-__global__ void k_tcc_split(const float2* __restrict__ A, int N, int S, int Kp,
-                            __nv_bfloat16* __restrict__ X1, __nv_bfloat16* __restrict__ X2,
-                            __nv_bfloat16* __restrict__ Y) {
-  const size_t n = (size_t)N * Kp;
+__global__ void k_tcc_split(const float2* __restrict__ A, int N, int S, int K2p, __nv_bfloat16* __restrict__ ops) {
+  const size_t n = (size_t)N * K2p, plane = n;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int f = (int)(i / Kp), k = (int)(i % Kp);
-    float x1 = 0.f, x2 = 0.f, y = 0.f;
-    if (k < 6 * S) {
-      const int seg = k / S, s = k - seg * S;
+    const int f = (int)(i / K2p), k = (int)(i % K2p);
+    float x1h = 0.f, x2h = 0.f, x1l = 0.f, x2l = 0.f;
+    if (k < 2 * S) {
+      const int s = k < S ? k : k - S;
       const float2 a = A[(size_t)f * S + s];
-      const __nv_bfloat16 rh = __float2bfloat16_rn(a.x), ih = __float2bfloat16_rn(a.y);
-      const float rhf = __bfloat162float(rh), ihf = __bfloat162float(ih);
-      const float rl = __bfloat162float(__float2bfloat16_rn(a.x - rhf));
-      const float il = __bfloat162float(__float2bfloat16_rn(a.y - ihf));
-      switch (seg) {
-        case 0: x1 = rhf; x2 = ihf; y = rhf; break;
-        case 1: x1 = ihf; x2 = -rhf; y = ihf; break;
-        case 2: x1 = rhf; x2 = ihf; y = rl; break;
-        case 3: x1 = ihf; x2 = -rhf; y = il; break;
-        case 4: x1 = rl; x2 = il; y = rhf; break;
-        default: x1 = il; x2 = -rl; y = ihf; break;
+      const float rh = __bfloat162float(__float2bfloat16_rn(a.x)), ih = __bfloat162float(__float2bfloat16_rn(a.y));
+      const float rl = __bfloat162float(__float2bfloat16_rn(a.x - rh));
+      const float il = __bfloat162float(__float2bfloat16_rn(a.y - ih));
+      if (k < S) {
+        x1h = rh; x2h = ih; x1l = rl; x2l = il;
+      } else {
+        x1h = ih; x2h = -rh; x1l = il; x2l = -rl;
       }
     }
-    X1[i] = __float2bfloat16_rn(x1);
-    X2[i] = __float2bfloat16_rn(x2);
-    Y[i] = __float2bfloat16_rn(y);
+    ops[i] = __float2bfloat16_rn(x1h);              // X1h
+    ops[plane + i] = __float2bfloat16_rn(x2h);      // X2h
+    ops[2 * plane + i] = __float2bfloat16_rn(x1l);  // X1l
+    ops[3 * plane + i] = __float2bfloat16_rn(x2l);  // X2l
   }
 }
 
-int tcc_split_operands(const float2* A, int N, int S, int Kp, void* X1, void* X2, void* Y,
-                       cudaStream_t st) {
-  const size_t n = (size_t)N * Kp;
+int tcc_split_operands(const float2* A, int N, int S, int K2p, void* ops, cudaStream_t st) {
+  const size_t n = (size_t)N * K2p;
   const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
-  k_tcc_split<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(A, N, S, Kp, (__nv_bfloat16*)X1,
-                                                       (__nv_bfloat16*)X2, (__nv_bfloat16*)Y);
+  k_tcc_split<<<blocks > 0 ? blocks : 1, 256, 0, st>>>(A, N, S, K2p, (__nv_bfloat16*)ops);
   KL_CUDA_TRY(cudaGetLastError());
   return KL_OK;
 }
@@ -181,9 +183,13 @@ int tcc_split_operands(const float2* A, int N, int S, int Kp, void* X1, void* X2
 namespace {
 constexpr int TM = 128, TN = 128, TK = 64;
 constexpr int TILE_BYTES = TM * TK * 2;         // 16 KB, one 128 x 64 bf16 tile
-constexpr int STAGE_BYTES = 3 * TILE_BYTES;     // X1, X2, Y
-// instruction descriptor: dense, f32 accumulate, bf16 A/B, both K-major, M=128, N=128
-constexpr uint32_t IDESC = tc::idesc_f16(TM, TN, true);
+constexpr int STAGE_BYTES = 6 * TILE_BYTES;     // X1h X2h | X1l X2l | Yh | Yl
+// One MMA computes re and im of a tile: A = the Y tile (128 rows j), B = the X1
+// and X2 tiles stacked (256 rows: X1 then X2, adjacent in shared memory), so
+// the accumulator holds re[i][j] in columns i and im[i][j] in columns 128 + i
+// of lane j, and each k step reads Y once instead of twice.
+// Instruction descriptor: dense, f32 accumulate, bf16 A/B, both K-major, M=128, N=256.
+constexpr uint32_t IDESC = tc::idesc_f16(TM, 2 * TN, true);
 
 using tc::mbar_arrive;
 using tc::mbar_expect_tx;
@@ -209,11 +215,11 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t 
 // loads, MMAs and stores of consecutive tiles overlap.  Every wait is bounded:
 // a timeout records `err`, raises the CTA's abort flag and every role stops.
 namespace {
-constexpr int kStages = 4;
+constexpr int kStages = 2;
 constexpr int kEpiWarps = 4;
 constexpr int kGemmThreads = 32 * (2 + kEpiWarps);
 constexpr int EPI_BYTES = kEpiWarps * 32 * 33 * 8;  // per epilogue warp a 32 x 33 float2 tile
-constexpr int PSMEM_BYTES = kStages * STAGE_BYTES + EPI_BYTES + 1024 + 256;
+constexpr int PSMEM_BYTES = kStages * STAGE_BYTES + EPI_BYTES + 1024 + 128;
 constexpr uint32_t PTMEM_COLS = 512;  // two accumulator sets of (re 128 | im 128)
 
 __device__ __forceinline__ void upper_tile(int t, int nt, int& ib, int& jb) {
@@ -229,9 +235,8 @@ __device__ __forceinline__ void upper_tile(int t, int nt, int& ib, int& jb) {
 }  // namespace
 
 __global__ void __launch_bounds__(kGemmThreads, 1)
-    k_tcc_gemm(const __grid_constant__ CUtensorMap tmX1, const __grid_constant__ CUtensorMap tmX2,
-               const __grid_constant__ CUtensorMap tmY, int N, int nkb, int nt,
-               float2* __restrict__ tcc, int* __restrict__ err) {
+    k_tcc_gemm(const __grid_constant__ CUtensorMap tmO, int N, int nkb, int nt, float2* __restrict__ tcc,
+               int* __restrict__ err) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
   float2* epi = reinterpret_cast<float2*>(smem + kStages * STAGE_BYTES);
@@ -284,10 +289,15 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         if (use > 0 && !(ok = mbar_wait_ab(smem_u32(&empty[s]), (uint32_t)((use - 1) & 1), err, 1, abort))) break;
         const uint32_t bar = smem_u32(&full[s]);
         mbar_expect_tx(bar, STAGE_BYTES);
+        // planes of the operand buffer: X1h rows 0.., X2h rows N.., X1l rows
+        // 2N.., X2l rows 3N..; Y's tiles are X1's rows of tile jb
         uint8_t* st = smem + s * STAGE_BYTES;
-        tma_load_2d(smem_u32(st), &tmX1, kb * TK, ib * TM, bar);
-        tma_load_2d(smem_u32(st + TILE_BYTES), &tmX2, kb * TK, ib * TM, bar);
-        tma_load_2d(smem_u32(st + 2 * TILE_BYTES), &tmY, kb * TK, jb * TN, bar);
+        tma_load_2d(smem_u32(st), &tmO, kb * TK, ib * TM, bar);
+        tma_load_2d(smem_u32(st + TILE_BYTES), &tmO, kb * TK, N + ib * TM, bar);
+        tma_load_2d(smem_u32(st + 2 * TILE_BYTES), &tmO, kb * TK, 2 * N + ib * TM, bar);
+        tma_load_2d(smem_u32(st + 3 * TILE_BYTES), &tmO, kb * TK, 3 * N + ib * TM, bar);
+        tma_load_2d(smem_u32(st + 4 * TILE_BYTES), &tmO, kb * TK, jb * TN, bar);
+        tma_load_2d(smem_u32(st + 5 * TILE_BYTES), &tmO, kb * TK, 2 * N + jb * TN, bar);
         armed[s] = use;
       }
     }
@@ -307,14 +317,15 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         const int s = it % kStages, use = it / kStages;
         if (!(ok = mbar_wait_ab(smem_u32(&full[s]), (uint32_t)(use & 1), err, 2, abort))) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t a1 = smem_u32(smem + s * STAGE_BYTES);
-        const uint32_t a2 = a1 + TILE_BYTES, b = a1 + 2 * TILE_BYTES;
+        const uint32_t xh = smem_u32(smem + s * STAGE_BYTES), xl = xh + 2 * TILE_BYTES;
+        const uint32_t yh = xh + 4 * TILE_BYTES, yl = xh + 5 * TILE_BYTES;
 #pragma unroll
         for (int k = 0; k < TK / 16; ++k) {
           const uint32_t accum = (kb > 0 || k > 0) ? 1u : 0u;
           const uint32_t off = (uint32_t)(k * 32);  // 16 bf16 along K inside the swizzle atom
-          mma_bf16(acc, smem_desc(a1 + off), smem_desc(b + off), accum);
-          mma_bf16(acc + 128, smem_desc(a2 + off), smem_desc(b + off), accum);
+          mma_bf16(acc, smem_desc(yh + off), smem_desc(xh + off), accum);
+          mma_bf16(acc, smem_desc(yl + off), smem_desc(xh + off), 1u);
+          mma_bf16(acc, smem_desc(yh + off), smem_desc(xl + off), 1u);
         }
         mma_commit(smem_u32(&empty[s]));
       }
@@ -324,7 +335,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     mma_commit(smem_u32(drain));
     mbar_wait(smem_u32(drain), 0u, err, 6);
   } else if (warp >= 2) {
-    // epilogue: warp w drains TMEM lanes (tile rows) 32 (w % 4) .. + 31
+    // epilogue: warp w drains TMEM lanes 32 (w % 4) .. + 31, i.e. tile columns
+    // j = jb TN + 32 (w % 4) + lane; each lane holds re and im of TCC[i][j] for
+    // the tile's i in its TMEM columns
     const int q = warp & 3;
     float2* stage = epi + (warp - 2) * 32 * 33;
     int tl = 0;
@@ -336,41 +349,41 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       int ib, jb;
       upper_tile(t, nt, ib, jb);
-      const int r = q * 32 + lane;
-      const int i = ib * TM + r;
+      const int r = q * 32 + lane;  // tile column of this lane
+      const int j = jb * TN + r;
       const bool diag = ib == jb;
       const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * 256);
 #pragma unroll 1
-      for (int c0 = 0; c0 < TN; c0 += 32) {
+      for (int c0 = 0; c0 < TM; c0 += 32) {
         uint32_t re[32], im[32];
         tmem_ld32(base + (uint32_t)c0, re);
         tmem_ld32(base + 128u + (uint32_t)c0, im);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        // the warp's 32 x 32 block goes through its staging buffer so that each
-        // store writes 32 consecutive columns of one row
+        // TCC[i][j] (i <= j): consecutive lanes write consecutive j
 #pragma unroll
-        for (int c = 0; c < 32; ++c) stage[lane * 33 + c] = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
+        for (int c = 0; c < 32; ++c) {
+          const int i = ib * TM + c0 + c;
+          if (i < N && j < N && (!diag || r >= c0 + c)) {
+            float2 v = make_float2(__uint_as_float(re[c]), __uint_as_float(im[c]));
+            if (diag && r == c0 + c) v.y = 0.f;
+            tcc[(size_t)i * N + j] = v;
+          }
+        }
+        // TCC[j][i] = conj TCC[i][j] (i < j, the lower triangle of a diagonal
+        // tile): the warp's 32 x 32 block goes through its staging buffer so
+        // that each store writes 32 consecutive i of one row j
+#pragma unroll
+        for (int c = 0; c < 32; ++c) stage[lane * 33 + c] = make_float2(__uint_as_float(re[c]), -__uint_as_float(im[c]));
         __syncwarp();
         {
-          const int j = jb * TN + c0 + lane;
+          const int i = ib * TM + c0 + lane;
 #pragma unroll 4
           for (int rr = 0; rr < 32; ++rr) {
-            const int row = q * 32 + rr, ii = ib * TM + row;
-            if (ii < N && j < N && (!diag || c0 + lane >= row)) {
-              float2 v = stage[rr * 33 + lane];
-              if (diag && c0 + lane == row) v.y = 0.f;
-              tcc[(size_t)ii * N + j] = v;
-            }
+            const int col = q * 32 + rr, jj = jb * TN + col;
+            if (jj < N && i < N && (!diag || c0 + lane < col)) tcc[(size_t)jj * N + i] = stage[rr * 33 + lane];
           }
         }
         __syncwarp();
-        // conjugate transpose: tcc[j][i], consecutive lanes write consecutive i
-#pragma unroll
-        for (int c = 0; c < 32; ++c) {
-          const int j = jb * TN + c0 + c;
-          if (j < N && i < N && (!diag || c0 + c > r))
-            tcc[(size_t)j * N + i] = make_float2(__uint_as_float(re[c]), -__uint_as_float(im[c]));
-        }
       }
       // this set's TMEM is read: the MMAs of tile tl + 2 may overwrite it
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -393,21 +406,19 @@ int make_map(CUtensorMap* m, const void* base, int rows, int Kp) {
 }
 }  // namespace
 
-int tcc_gemm_tc(const void* X1, const void* X2, const void* Y, int N, int Kp, float2* tcc,
-                int* err_dev, cudaStream_t st) {
-  KL_CHECK_ARG(N > 0 && Kp > 0 && Kp % TK == 0, "tcc_gemm_tc: bad sizes");
-  KL_CHECK_ARG(((uintptr_t)X1 | (uintptr_t)X2 | (uintptr_t)Y) % 16 == 0, "tcc_gemm_tc: operands must be 16-byte aligned");
-  CUtensorMap m1, m2, my;
+int tcc_gemm_tc(const void* ops, int N, int K2p, float2* tcc, int* err_dev, cudaStream_t st) {
+  KL_CHECK_ARG(N > 0 && K2p > 0 && K2p % TK == 0, "tcc_gemm_tc: bad sizes");
+  KL_CHECK_ARG((uintptr_t)ops % 16 == 0, "tcc_gemm_tc: operands must be 16-byte aligned");
+  CUtensorMap mo;
   int rc;
-  if ((rc = make_map(&m1, X1, N, Kp)) || (rc = make_map(&m2, X2, N, Kp)) || (rc = make_map(&my, Y, N, Kp))) return rc;
+  if ((rc = make_map(&mo, ops, 4 * N, K2p))) return rc;
   const int nt = (N + TM - 1) / TM;
   const int tiles = nt * (nt + 1) / 2;
   int dev = 0, sms = 0;
   KL_CUDA_TRY(cudaGetDevice(&dev));
   KL_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   KL_CUDA_TRY(cudaFuncSetAttribute(k_tcc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, PSMEM_BYTES));
-  k_tcc_gemm<<<std::min(tiles, std::max(1, sms)), kGemmThreads, PSMEM_BYTES, st>>>(m1, m2, my, N, Kp / TK, nt, tcc,
-                                                                                    err_dev);
+  k_tcc_gemm<<<std::min(tiles, std::max(1, sms)), kGemmThreads, PSMEM_BYTES, st>>>(mo, N, K2p / TK, nt, tcc, err_dev);
   KL_CUDA_TRY(cudaGetLastError());
   return KL_OK;
 }
