@@ -94,6 +94,16 @@ int synth_tc_build_basis(const SocsGeom& g, void* bhi, void* blo, cudaStream_t s
 // err: device status word, set to a nonzero code if a pipeline wait times out
 int synth_tc_launch(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi,
                     const void* blo, int nimg, float* images, int* err, cudaStream_t st);
+// The adjoint's image + resist + loss + row DFT of dL/dI on the tensor cores
+// (socs_vjp_tc.cu), in place of vjp_launch_inverse: same outputs (images,
+// loss, strip partials of the spectrum of dL/dI).
+bool vjp_tc_supported(const SocsGeom& g);
+// transposed row-DFT basis [64][Lx] as FP16 hi and lo halves (each 64 * Lx * 2 bytes)
+int vjp_tc_build_basis_t(const SocsGeom& g, void* thi, void* tlo, cudaStream_t st);
+// bhi / blo: the synthesis basis of synth_tc_build_basis (Kp = 64)
+int vjp_tc_launch(const SocsGeom& g, const float2* T, const float2* ty, int nclips, int nsets, int nsplit,
+                  const void* bhi, const void* blo, const void* thi, const void* tlo, const float* targets,
+                  float alpha, float thr, float* images, double* loss, float2* gpart, int* err, cudaStream_t st);
 // centred band of FT_r2c (DC at the band centre), complex64 nby x nbx per clip
 int socs_launch_band(const SocsGeom& g, const float2* partial, int nclips, float2* band,
                      cudaStream_t st);

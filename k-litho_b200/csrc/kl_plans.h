@@ -42,6 +42,9 @@ struct kl_socs_plan_s {
   void* bhi = nullptr;
   void* blo = nullptr;
   int* status = nullptr;
+  // adjoint plans: the transposed basis of the tensor-core adjoint ([64][Lx])
+  void* thi = nullptr;
+  void* tlo = nullptr;
   // general-geometry pipeline (socs_gen.cu): any period, bands up to 4N+1 <= 256.
   // Used when the specialised kernels above do not cover the geometry (or on
   // request); `g` then only carries the sizes.

@@ -46,6 +46,8 @@ void free_plan(kl_socs_plan p) {
   cudaFree(p->bhi);
   cudaFree(p->blo);
   cudaFree(p->status);
+  cudaFree(p->thi);
+  cudaFree(p->tlo);
   delete p;
 }
 
@@ -274,6 +276,14 @@ int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int 
       return rc;
     }
     cudaMemset(p->status, 0, sizeof(int));
+    if (adjoint && kl::synth_tc_kp(g) == 64 && kl::vjp_tc_supported(g)) {
+      const size_t tb = (size_t)64 * g.Lx * 2;
+      if ((rc = alloc(&p->thi, tb, "adjoint basis")) || (rc = alloc(&p->tlo, tb, "adjoint basis")) ||
+          (rc = kl::vjp_tc_build_basis_t(g, p->thi, p->tlo, nullptr))) {
+        free_plan(p);
+        return rc;
+      }
+    }
   }
   if (adjoint) {
     const size_t nb2s = (size_t)g.nby * g.nbx;
@@ -374,9 +384,15 @@ int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nc
   if ((rc = kl::socs_launch_spectral(g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, ns1, p->T, st)))
     return rc;
   KL_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(double) * (size_t)nclips * p->nsets, st));
-  if ((rc = kl::vjp_launch_inverse(g, p->tx, p->ty, p->T, nclips, p->nsets, ns1, targets, alpha,
-                                   threshold, images, loss, p->gpart, st)))
-    return rc;
+  // image, resist, loss and the row DFT of dL/dI: on the tensor cores where
+  // the plan has them, unless it asks for the CUDA-core engine
+  const bool tca = p->thi && p->synth != KL_SYNTH_CUDA_CORES &&
+                   (((uintptr_t)targets | (uintptr_t)images) & 15) == 0;
+  rc = tca ? kl::vjp_tc_launch(g, p->T, p->ty, nclips, p->nsets, ns1, p->bhi, p->blo, p->thi, p->tlo, targets, alpha,
+                               threshold, images, loss, p->gpart, p->status, st)
+           : kl::vjp_launch_inverse(g, p->tx, p->ty, p->T, nclips, p->nsets, ns1, targets, alpha, threshold, images,
+                                    loss, p->gpart, st);
+  if (rc) return rc;
   const int ns2 = kl::socs_choose_split(g, nclips, p->nsets, p->K);
   if ((rc = kl::vjp_launch_spectral(g, p->partial, p->gpart, nclips, p->H, p->lam, p->K, p->nsets,
                                     ns2, p->gam, st)))

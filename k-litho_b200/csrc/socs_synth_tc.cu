@@ -39,6 +39,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cstdint>
 
 #include "kl_device.cuh"
 #include "kl_internal.h"
@@ -376,15 +377,26 @@ __global__ void __launch_bounds__(kSThreads, 1)
         cur_img = img;
         if (tid == 0) s_bound = 0u;
         const float2* Ti = T + (size_t)img * nsplit * tsz;
-        for (int i = tid; i < nty * tstr; i += 32 * kCW) {
-          const int ar = i / tstr, b = i - ar * tstr;
-          float2 v = make_float2(0.f, 0.f);
-          if (b < ntx) {
-            const size_t o = (size_t)ar * ntx + b;
-            v = __ldg(Ti + o);
-            for (int p = 1; p < nsplit; ++p) v = cadd(v, __ldg(Ti + p * tsz + o));
+        // eight independent loads in flight per thread (the first tile of a
+        // run waits on them)
+        for (int i0 = tid; i0 < nty * tstr; i0 += 8 * 32 * kCW) {
+          float2 v[8];
+          size_t o[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * 32 * kCW, ar = i / tstr, b = i - ar * tstr;
+            o[u] = (i < nty * tstr && b < ntx) ? (size_t)ar * ntx + b : SIZE_MAX;
+            v[u] = o[u] != SIZE_MAX ? __ldg(Ti + o[u]) : make_float2(0.f, 0.f);
           }
-          Ts[i] = v;
+          for (int p = 1; p < nsplit; ++p)
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+              if (o[u] != SIZE_MAX) v[u] = cadd(v[u], __ldg(Ti + p * tsz + o[u]));
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int i = i0 + u * 32 * kCW;
+            if (i < nty * tstr) Ts[i] = v[u];
+          }
         }
         asm volatile("bar.sync 1, %0;" ::"r"(32 * kCW) : "memory");
         // |Q[y][b]| <= w_b sum_a |T[a][b]|: the largest bound fixes the exponent
