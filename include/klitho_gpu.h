@@ -135,14 +135,16 @@ int kl_socs_plan_create_ex(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, i
 /* 0 if the plan runs on the specialised kernels, 1 on the general pipeline. */
 int kl_socs_plan_engine(kl_socs_plan plan);
 
-/* Engine of the image synthesis (the FI step) on the specialised kernels:
- * KL_SYNTH_CUDA_CORES, a per-lane DFT of each row's coefficients;
- * KL_SYNTH_TENSOR_CORES, the same sum as an FP16x3 split matrix product on
- * the tensor cores (periods with Lx, Ly multiples of 128 and 2(2Nx+1) <= 128;
- * image error of the same order as the CUDA-core engine's); KL_SYNTH_AUTO
+/* Engine of the mask transform (FT_r2c) and the image synthesis (the FI step)
+ * on the specialised kernels: KL_SYNTH_CUDA_CORES, per-lane DFTs of each row;
+ * KL_SYNTH_TENSOR_CORES, the same sums as FP16x3 split matrix products on the
+ * tensor cores (periods with Lx, Ly multiples of 128 and 2(2Nx+1) <= 128;
+ * image error of the same order as the CUDA-core engine's; mask values within
+ * +-2^15, others are reported by kl_socs_plan_status); KL_SYNTH_AUTO
  * (the default), the engine kl_socs_autotune picked, else the CUDA cores.
- * The gradient synthesis of kl_socs_vjp runs on the tensor cores wherever
- * the geometry allows, unless KL_SYNTH_CUDA_CORES is set.
+ * kl_socs_vjp runs its image, resist and gradient syntheses on the tensor
+ * cores wherever the geometry allows, unless KL_SYNTH_CUDA_CORES is set, and
+ * its mask transform there only with KL_SYNTH_TENSOR_CORES.
  * Returns KL_ERR_UNSUPPORTED for the tensor-core engine on other geometries
  * and on general-pipeline plans.  No counterpart in the reference. */
 #define KL_SYNTH_AUTO 0
@@ -185,7 +187,8 @@ int kl_socs_forward_host(kl_socs_plan plan, const float* masks_host, int nclips,
  * events on `stream` and keeps the fastest; later calls of kl_socs_forward
  * with nclips clips use it.  Writes images_dev (the images of the chosen
  * shape).  Synchronous.  The chosen shape is returned in *nsplit / *spc when
- * those are not NULL (*spc = -1: the tensor-core synthesis). */
+ * those are not NULL (*spc = -1: the tensor-core synthesis, -2: the tensor-core
+ * synthesis and mask transform). */
 int kl_socs_autotune(kl_socs_plan plan, const float* masks_dev, int nclips, float* images_dev,
                      void* stream, int* nsplit, int* spc);
 

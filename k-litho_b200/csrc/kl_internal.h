@@ -94,6 +94,13 @@ int synth_tc_build_basis(const SocsGeom& g, void* bhi, void* blo, cudaStream_t s
 // err: device status word, set to a nonzero code if a pipeline wait times out
 int synth_tc_launch(const SocsGeom& g, const float2* T, const float2* ty, int nsplit, const void* bhi,
                     const void* blo, int nimg, float* images, int* err, cudaStream_t st);
+// The mask transform (strip partial band spectra) on the tensor cores
+// (socs_fwd_tc.cu), in place of socs_launch_forward; thi / tlo: the transposed
+// basis of vjp_tc_build_basis_t.  Mask values must lie within +-2^15 (the
+// status word reports others).
+bool fwd_tc_supported(const SocsGeom& g);
+int fwd_tc_launch(const SocsGeom& g, const float* masks, int nclips, const float2* ty, const void* thi,
+                  const void* tlo, float2* partial, int* err, cudaStream_t st);
 // The adjoint's image + resist + loss + row DFT of dL/dI on the tensor cores
 // (socs_vjp_tc.cu), in place of vjp_launch_inverse: same outputs (images,
 // loss, strip partials of the spectrum of dL/dI).

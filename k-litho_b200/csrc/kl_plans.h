@@ -42,9 +42,11 @@ struct kl_socs_plan_s {
   void* bhi = nullptr;
   void* blo = nullptr;
   int* status = nullptr;
-  // adjoint plans: the transposed basis of the tensor-core adjoint ([64][Lx])
+  // the transposed basis ([64][Lx]) of the tensor-core mask transform and, on
+  // adjoint plans with vjp_tc, of the tensor-core adjoint
   void* thi = nullptr;
   void* tlo = nullptr;
+  bool vjp_tc = false;
   // general-geometry pipeline (socs_gen.cu): any period, bands up to 4N+1 <= 256.
   // Used when the specialised kernels above do not cover the geometry (or on
   // request); `g` then only carries the sizes.

@@ -126,6 +126,15 @@ bool use_tc_synthesis(kl_socs_plan p, int nclips) {
   return p->tune_clips == nclips && p->tune_nsplit > 0 && p->tune_spc < 0;
 }
 
+// mask transform on the tensor cores: with the tensor-core engine forced, or
+// when the autotuner picked it (tune_spc == -2) for this batch size
+bool use_tc_forward(kl_socs_plan p, int nclips, const float* masks) {
+  if (p->gen || !p->thi || !kl::fwd_tc_supported(p->g) || ((uintptr_t)masks & 15)) return false;
+  if (p->synth == KL_SYNTH_TENSOR_CORES) return true;
+  if (p->synth == KL_SYNTH_CUDA_CORES) return false;
+  return p->tune_clips == nclips && p->tune_nsplit > 0 && p->tune_spc == -2;
+}
+
 int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, cudaStream_t st,
                 const cudaEvent_t* ev4 = nullptr) {
   if (p->gen) return run_forward_gen(p, masks, nclips, images, st, ev4);
@@ -135,7 +144,11 @@ int run_forward(kl_socs_plan p, const float* masks, int nclips, float* images, c
   launch_shape(p, nclips, &nsplit, &spc);
   const bool tc = use_tc_synthesis(p, nclips) && kl::synth_tc_aligned(images);
   spc = spc > 0 ? spc : 0;
-  if ((rc = kl::socs_launch_forward(p->g, p->tx, p->ty, masks, nclips, p->partial, st))) return rc;
+  if (use_tc_forward(p, nclips, masks))
+    rc = kl::fwd_tc_launch(p->g, masks, nclips, p->ty, p->thi, p->tlo, p->partial, p->status, st);
+  else
+    rc = kl::socs_launch_forward(p->g, p->tx, p->ty, masks, nclips, p->partial, st);
+  if (rc) return rc;
   if ((rc = stage_mark(p, st, ev4, 1))) return rc;
   rc = kl::socs_launch_spectral(p->g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, nsplit,
                                 p->T, st);
@@ -276,9 +289,12 @@ int create_plan(kl_socs_plan* plan, int Lx, int Ly, int Nx, int Ny, int nk, int 
       return rc;
     }
     cudaMemset(p->status, 0, sizeof(int));
-    if (adjoint && kl::synth_tc_kp(g) == 64 && kl::vjp_tc_supported(g)) {
+    // the transposed basis of the row DFTs: the tensor-core mask transform and,
+    // on adjoint plans, the row DFT of dL/dI
+    p->vjp_tc = adjoint && kl::synth_tc_kp(g) == 64 && kl::vjp_tc_supported(g);
+    if (kl::fwd_tc_supported(g) || p->vjp_tc) {
       const size_t tb = (size_t)64 * g.Lx * 2;
-      if ((rc = alloc(&p->thi, tb, "adjoint basis")) || (rc = alloc(&p->tlo, tb, "adjoint basis")) ||
+      if ((rc = alloc(&p->thi, tb, "row DFT basis")) || (rc = alloc(&p->tlo, tb, "row DFT basis")) ||
           (rc = kl::vjp_tc_build_basis_t(g, p->thi, p->tlo, nullptr))) {
         free_plan(p);
         return rc;
@@ -380,13 +396,17 @@ int kl_socs_vjp(kl_socs_plan p, const float* masks, const float* targets, int nc
   const kl::SocsGeom& g = p->g;
   int rc;
   const int ns1 = kl::socs_choose_split(g, nclips, p->nsets, p->K);
-  if ((rc = kl::socs_launch_forward(g, p->tx, p->ty, masks, nclips, p->partial, st))) return rc;
+  if (p->synth == KL_SYNTH_TENSOR_CORES && use_tc_forward(p, nclips, masks))
+    rc = kl::fwd_tc_launch(g, masks, nclips, p->ty, p->thi, p->tlo, p->partial, p->status, st);
+  else
+    rc = kl::socs_launch_forward(g, p->tx, p->ty, masks, nclips, p->partial, st);
+  if (rc) return rc;
   if ((rc = kl::socs_launch_spectral(g, p->partial, nclips, p->H, p->lam, p->K, p->nsets, ns1, p->T, st)))
     return rc;
   KL_CUDA_TRY(cudaMemsetAsync(loss, 0, sizeof(double) * (size_t)nclips * p->nsets, st));
   // image, resist, loss and the row DFT of dL/dI: on the tensor cores where
   // the plan has them, unless it asks for the CUDA-core engine
-  const bool tca = p->thi && p->synth != KL_SYNTH_CUDA_CORES &&
+  const bool tca = p->vjp_tc && p->synth != KL_SYNTH_CUDA_CORES &&
                    (((uintptr_t)targets | (uintptr_t)images) & 15) == 0;
   rc = tca ? kl::vjp_tc_launch(g, p->T, p->ty, nclips, p->nsets, ns1, p->bhi, p->blo, p->thi, p->tlo, targets, alpha,
                                threshold, images, loss, p->gpart, p->status, st)

@@ -118,7 +118,10 @@ int kl_socs_autotune(kl_socs_plan p, const float* masks, int nclips, float* imag
     }
   }
   // ... then strips per CTA of the inverse stage, and the tensor-core synthesis
-  if (!p->gen && p->bhi && p->synth == KL_SYNTH_AUTO) spcs.push_back(-1);
+  if (!p->gen && p->bhi && p->synth == KL_SYNTH_AUTO) {
+    spcs.push_back(-1);                                  // tensor-core synthesis
+    if (p->thi && kl::fwd_tc_supported(p->g)) spcs.push_back(-2);  // ... and mask transform
+  }
   for (size_t i = 0; i < spcs.size() && !rc; ++i) {
     if ((rc = time_shape(best_ns, spcs[i], &t))) break;
     if (t < best) {

@@ -126,3 +126,23 @@ def test_tc_synthesis_autotune_and_errors(cuda):
     with pytest.raises(Exception):
         gen.set_synthesis("tensor")
     gen.close()
+
+
+def test_tc_mask_range_reported(cuda):
+    # mask values beyond the FP16 range of the tensor-core mask transform are
+    # reported through the plan status, not silently imaged
+    import torch
+    L, Nx = 256, 3
+    krn, sc = synth.random_kernels(4, Nx, Nx, seed=2)
+    plan = K.SocsPlan(L, L, Nx, Nx, 4, max_clips=1)
+    plan.set_kernels(0, krn, sc)
+    plan.set_synthesis("tensor")
+    mask = synth.rect_mask(L, 4, seed=1)
+    mask[5, 7] = 1.0e6
+    md = torch.from_numpy(mask[None].copy()).cuda()
+    out = torch.empty((1, 1, L, L), dtype=torch.float32, device="cuda")
+    plan.forward(md, out)
+    with pytest.raises(Exception):
+        plan.status()
+    plan.status()  # cleared by the previous call
+    plan.close()
