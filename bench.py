@@ -403,13 +403,11 @@ def run_ours(args):
             "dtype": "f32",
             "data": "synthetic (seeded random-rectangle masks; kernels from the GPU TCC + "
                     "subspace iteration of the annular NA 1.35 optics, K=24 per size and focus)",
-            "config": {"workload": "batched SOCS forward: 128x512^2 + 192x1024^2 + 64x2048^2 "
-                                   "clips x 3 focus, K=24",
-                       "clips_per_gpu": sum(n for _, n in CLASSES), "focus_nm": FOCUS_NM,
-                       "image_equiv_1024_per_step_per_gpu": img_equiv,
-                       "l2": "inputs larger than L2 (1.9 GB masks, 5.8 GB images per GPU)",
-                       "parallelism": f"clip sharding ({args.scaling if ws > 1 else 'weak'}), {ws} GPU(s), "
-                                      f"no collective on the data path"},
+            "config": dict(workload_config(),
+                           **{"image_equiv_1024_per_step_per_gpu": img_equiv,
+                              "l2": "inputs larger than L2 (1.9 GB masks, 5.8 GB images per GPU)",
+                              "parallelism": f"clip sharding ({args.scaling if ws > 1 else 'weak'}), {ws} GPU(s), "
+                                             f"no collective on the data path"}),
             "roofline": roof, "stages": other, "per_class": per_class, "graph_branches": branches,
             "image_err_vs_fp64_of_clear_field": (fp64 or {}).get("image_max_err_of_clear_field"),
             "clocks": clk, "e2e": e2e,
@@ -983,6 +981,12 @@ def run_e2e(plans, masks_h, args, ws, img_equiv):
 # CPU: the reference's own implementation of the path on the host cores
 # ---------------------------------------------------------------------------
 
+def workload_config():
+    """The benchmark workload (both arms): BASELINE config 2's clip mix and focus values."""
+    return {"workload": "batched SOCS forward: 128x512^2 + 192x1024^2 + 64x2048^2 clips x 3 focus, K=24",
+            "clips_per_gpu": sum(n for _, n in CLASSES), "focus_nm": FOCUS_NM}
+
+
 def _cpu_task(args):
     """One reference SOCS image (FT_r2c + calcSOCS + FI) of an L^2 clip."""
     L, seed, use_ref = args
@@ -1030,24 +1034,35 @@ def run_reference(args):
     use_ref = O.ref_available()
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
-    per_step = max(nproc, 1)
-    times = []
+    # the workload's mix of clip sizes, by image count (128 : 192 : 64 clips,
+    # every clip imaged at each focus, which costs the CPU path the same): a
+    # step images the pattern 2 x 512^2, 3 x 1024^2, 1 x 2048^2 about nproc / 2
+    # times, the pool handing out one image at a time so that the processes
+    # stay busy; the rate counts 1024^2-equivalent images
+    pattern = [2048, 1024, 1024, 1024, 512, 512]
+    reps = max(1, nproc // 2)
+    per_step = len(pattern) * reps
+    times, equiv, nimg = [], 0.0, 0
     with ctx.Pool(nproc) as pool:
         for s in range(args.warmup + args.steps):
+            sizes = pattern * reps
             t0 = time.perf_counter()
-            pool.map(_cpu_task, [(1024, 7 + s * per_step + i, use_ref) for i in range(per_step)])
+            pool.map(_cpu_task, [(L, 7 + s * per_step + i, use_ref) for i, L in enumerate(sizes)], chunksize=1)
             if s >= args.warmup:
                 times.append(time.perf_counter() - t0)
+                equiv += sum((L / 1024.0) ** 2 for L in sizes)
+                nimg += len(sizes)
     dt = float(np.mean(times))
-    value = per_step / dt
+    value = equiv / float(np.sum(times))
     kind = "reference" if use_ref else "port"
     out = {"impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": round(dt * 1e3, 2), "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "batched SOCS forward (sampled: 1024^2 clips at one focus, K=24)"},
+           "config": workload_config(),
            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": nproc, "kind": kind,
-                            "sample": f"{per_step} x 1024^2 clips per step, one process per core"},
+                            "sample": f"{nimg} images of the workload's size mix (2 x 512^2 : 3 x 1024^2 : "
+                                      f"1 x 2048^2, K=24), {per_step} per step over {nproc} processes"},
            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
