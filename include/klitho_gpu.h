@@ -344,6 +344,15 @@ int kl_tcc_plan_info(kl_tcc_plan plan, int* Nx, int* Ny, int* N, int* S, float* 
 /* Copy the FP32 factor A (N x S c64, row-major) to A_dev (fast path only). */
 int kl_tcc_factor(kl_tcc_plan plan, float* A_dev, void* stream);
 
+/* Top-K eigenpairs of a Hermitian B x B complex128 matrix on the device
+ * (row-major, 64 <= B <= 256, 1 <= K <= B): the eigensolve behind kl_topk_eig's
+ * Gram step, the part of zheevr (klitho_tcc.cpp:300-377) that remains once the
+ * TCC is reduced to its source span.  Householder tridiagonalisation on a
+ * cluster of 8 CTAs, bisection, inverse iteration; eigenvalues descending into
+ * evals_dev (K doubles), eigenvector j into column j of vecs_dev (B x K
+ * complex128, row-major).  H_dev is not modified.  Asynchronous on stream. */
+int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* vecs_dev, void* stream);
+
 /* calcTCC (klitho_tcc.cpp:186-267): the N x N Hermitian TCC, row-major, into
  * tcc_dev -- c64 on the fast path (tcgen05 tensor cores, BF16x3 split, FP32
  * accumulate), c128 on the FP64 path.  Synchronous on the fast path (reports

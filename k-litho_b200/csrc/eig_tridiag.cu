@@ -1,0 +1,498 @@
+// eig_tridiag.cu -- top-K eigenpairs of a Hermitian B x B matrix (64 <= B <= 256)
+// by Householder reduction to tridiagonal form, bisection and inverse
+// iteration: the zhetrd + dstebz + dstein route of LAPACK, which the
+// reference's zheevr (K-Litho-TCC/klitho_tcc.cpp:300-377) starts from too
+// (zheevr finishes with MRRR instead of bisection + inverse iteration).
+//
+// Four launches per batch of matrices:
+//   k_hermitian_tridiag  one thread-block cluster of 8 CTAs per matrix, the
+//                        matrix's rows dealt round-robin over the CTAs'
+//                        shared memory; B - 2 reflector steps, each a
+//                        reflector broadcast, a distributed matvec and a
+//                        rank-2 update, separated by two cluster barriers
+//   k_tridiag_bisect     one warp per wanted eigenvalue: 32-point multisection
+//                        on Sturm counts of the real tridiagonal D^H T D
+//   k_tridiag_invit      one thread per eigenvector: inverse iteration with
+//                        the unpivoted L D L^T factorisation of T - lambda I,
+//                        Gram-Schmidt against the earlier members of a cluster
+//                        of close eigenvalues (clusters run in rounds)
+//   k_tridiag_back       one warp per eigenvector: phases, then the B - 2
+//                        reflectors in reverse order
+// Everything is complex / real FP64.  No step waits on another CTA except
+// through the cluster barrier, so nothing here can spin.
+#include <cooperative_groups.h>
+
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "kl_internal.h"
+#include "kl_tcc.h"
+
+namespace kl {
+
+namespace {
+
+constexpr int kTdCl = 8;            // CTAs per matrix (a portable cluster)
+constexpr int kTdThreads = 512;     // threads per CTA of the reduction
+constexpr int kTdMaxJobs = 16;      // matrices per launch
+constexpr int kTdBisWarps = 8;      // eigenvalues per CTA of the bisection
+constexpr int kTdBackWarps = 8;     // eigenvectors per CTA of the back-transform
+constexpr int kTdInvIters = 3;      // inverse-iteration solves per eigenvector
+constexpr int kTdChunk = 8;         // elements staged in registers per memory pass
+// eigenvalues closer than this multiple of ||T|| are one cluster: their vectors
+// are orthogonalised against each other (the others are orthogonal to within
+// eps ||T|| / gap by inverse iteration itself)
+constexpr double kTdClusterTol = 1e-7;
+constexpr double kEps = 2.220446049250313e-16;  // 2^-52
+constexpr double kSafeMin = 2.2250738585072014e-308;  // smallest normal double
+
+struct TridiagJobs {
+  TridiagJob j[kTdMaxJobs];
+};
+
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__host__ __device__ inline int td_rows(int B) { return (B + kTdCl - 1) / kTdCl; }
+// shared memory of k_hermitian_tridiag: the CTA's rows, two reflector buffers, p
+__host__ __device__ inline size_t td_smem(int B) {
+  return sizeof(double2) * ((size_t)td_rows(B) * B + 3 * (size_t)B);
+}
+
+// ---------------------------------------------------------------------------
+// Householder reduction H = Q T Q^H.  Row i of H lives in CTA i % 8 (local row
+// i / 8), so the trailing rows stay spread evenly as the reduction proceeds.
+// Step k: the owner of row k forms v (unit, supported on k+1..B-1) with
+// (I - 2 v v^H) x = alpha e_{k+1} for x = column k below the diagonal
+// (= conj(row k) right of it) and writes it into every CTA; each CTA forms
+// p_i = sum_j H[i][j] v_j for its rows i > k and writes them into every CTA;
+// then every CTA updates its rows: H -= 2 (v w^H + w v^H), w = p - (v^H p) v.
+// Outputs d[k] = T[k][k], e[k] = T[k+1][k] = alpha_k, and v_k in refl row k.
+// ---------------------------------------------------------------------------
+__global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
+    k_hermitian_tridiag(TridiagJobs jobs) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char tsm[];
+  const int me = (int)cl.block_rank();
+  const TridiagJob job = jobs.j[blockIdx.x / kTdCl];
+  const int B = job.B, R = td_rows(B);
+  double2* rows = reinterpret_cast<double2*>(tsm);  // R x B
+  double2* vbuf = rows + (size_t)R * B;             // 2 x B (by step parity)
+  double2* pbuf = vbuf + 2 * (size_t)B;             // B
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kTdThreads / 32;
+  const double2 zero = make_double2(0.0, 0.0);
+  for (int x = tid; x < R * B; x += kTdThreads) {
+    const int l = x / B, j = x - l * B, i = kTdCl * l + me;
+    rows[x] = i < B ? job.H[(size_t)i * B + j] : zero;
+  }
+  __syncthreads();
+  for (int k = 0; k + 2 < B; ++k) {
+    double2* v = vbuf + (size_t)(k & 1) * B;  // the owner of step k + 1 may write the other one early
+    const int j0 = k + 1;
+    if (me == k % kTdCl && warp == 0) {
+      const double2* hk = rows + (size_t)(k / kTdCl) * B;
+      double s2 = 0.0;
+      for (int j = j0 + lane; j < B; j += 32) {
+        const double2 h = hk[j];
+        s2 = fma(h.x, h.x, fma(h.y, h.y, s2));
+      }
+      s2 = warp_sum(s2);
+      const double2 x0 = make_double2(hk[j0].x, -hk[j0].y);
+      const double ax0 = sqrt(x0.x * x0.x + x0.y * x0.y), nx = sqrt(s2);
+      double2 alpha = zero;
+      double sc = 0.0;
+      if (nx > 0.0) {
+        const double2 ph = ax0 > 0.0 ? make_double2(x0.x / ax0, x0.y / ax0) : make_double2(1.0, 0.0);
+        alpha = make_double2(-ph.x * nx, -ph.y * nx);
+        sc = 1.0 / sqrt(2.0 * nx * (nx + ax0));  // 1 / ||x - alpha e||
+      }
+      for (int j = j0 + lane; j < B; j += 32) {
+        double2 x = make_double2(hk[j].x, -hk[j].y);
+        if (j == j0) x = make_double2(x.x - alpha.x, x.y - alpha.y);
+        const double2 vj = make_double2(x.x * sc, x.y * sc);
+        job.refl[(size_t)k * B + j] = vj;
+#pragma unroll
+        for (int c = 0; c < kTdCl; ++c) cl.map_shared_rank(v, c)[j] = vj;
+      }
+      if (lane == 0) {
+        job.d[k] = hk[k].x;
+        job.e[k] = alpha;
+      }
+    }
+    cl.sync();  // v of step k is in every CTA
+    const int lfirst = k < me ? 0 : (k - me) / kTdCl + 1;  // first local row below row k
+    for (int l = lfirst + warp; l < R; l += nwarp) {
+      const int i = kTdCl * l + me;
+      if (i >= B) break;
+      const double2* hr = rows + (size_t)l * B;
+      double ax = 0.0, ay = 0.0;
+      for (int j = j0 + lane; j < B; j += 32) {
+        const double2 h = hr[j], vj = v[j];
+        ax = fma(h.x, vj.x, fma(-h.y, vj.y, ax));
+        ay = fma(h.x, vj.y, fma(h.y, vj.x, ay));
+      }
+      ax = warp_sum(ax);
+      ay = warp_sum(ay);
+      if (lane < kTdCl) cl.map_shared_rank(pbuf, lane)[i] = make_double2(ax, ay);
+    }
+    cl.sync();  // p of step k is in every CTA
+    // c = Re(v^H p), the same sum in every warp
+    double c = 0.0;
+    for (int j = j0 + lane; j < B; j += 32) {
+      const double2 a = v[j], b = pbuf[j];
+      c = fma(a.x, b.x, fma(a.y, b.y, c));
+    }
+    c = warp_sum(c);
+    for (int l = lfirst + warp; l < R; l += nwarp) {
+      const int i = kTdCl * l + me;
+      if (i >= B) break;
+      double2* hr = rows + (size_t)l * B;
+      const double2 vi = v[i], pi = pbuf[i];
+      // 2 v_i and 2 w_i
+      const double2 v2 = make_double2(2.0 * vi.x, 2.0 * vi.y);
+      const double2 w2 = make_double2(2.0 * (pi.x - c * vi.x), 2.0 * (pi.y - c * vi.y));
+      for (int j = j0 + lane; j < B; j += 32) {
+        const double2 vj = v[j], pj = pbuf[j];
+        const double2 wj = make_double2(pj.x - c * vj.x, pj.y - c * vj.y);
+        double2 h = hr[j];
+        // h -= 2 v_i conj(w_j) + 2 w_i conj(v_j)
+        h.x -= fma(v2.x, wj.x, fma(v2.y, wj.y, fma(w2.x, vj.x, w2.y * vj.y)));
+        h.y -= fma(v2.y, wj.x, fma(-v2.x, wj.y, fma(w2.y, vj.x, -w2.x * vj.y)));
+        hr[j] = h;
+      }
+    }
+    __syncthreads();  // the owner of row k + 1 reads it next
+  }
+  // the trailing 2 x 2 block (or the 1 x 1 matrix)
+  if (tid == 0) {
+    for (int i = B >= 2 ? B - 2 : 0; i < B; ++i) {
+      if (i % kTdCl != me) continue;
+      const double2* hr = rows + (size_t)(i / kTdCl) * B;
+      job.d[i] = hr[i].x;
+      if (i + 1 < B) job.e[i] = make_double2(hr[i + 1].x, -hr[i + 1].y);  // T[i+1][i] = conj(H[i][i+1])
+    }
+  }
+  cl.sync();  // no CTA leaves while a peer may still address its shared memory
+}
+
+// Sturm count of the real tridiagonal (d, e2 = |e|^2): eigenvalues below x
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int B, double x, double pivmin) {
+  double q = d[0] - x;
+  if (fabs(q) <= pivmin) q = -pivmin;
+  int c = q < 0.0;
+  for (int i = 1; i < B; ++i) {
+    q = (d[i] - x) - e2[i - 1] / q;
+    if (fabs(q) <= pivmin) q = -pivmin;
+    c += q < 0.0;
+  }
+  return c;
+}
+
+// w[j] = the j-th largest eigenvalue: each lane counts at one of 32 points
+// splitting the warp's interval into 33 parts; the interval shrinks to the
+// part holding eigenvalue B - 1 - j (ascending) until it is a few ulps wide.
+__global__ void __launch_bounds__(32 * kTdBisWarps) k_tridiag_bisect(TridiagJobs jobs) {
+  const TridiagJob job = jobs.j[blockIdx.y];
+  const int B = job.B;
+  __shared__ double s_d[kTridiagMaxB], s_e2[kTridiagMaxB], s_ea[kTridiagMaxB];
+  for (int i = threadIdx.x; i < B; i += blockDim.x) {
+    s_d[i] = job.d[i];
+    const double2 e = i + 1 < B ? job.e[i] : make_double2(0.0, 0.0);
+    s_e2[i] = e.x * e.x + e.y * e.y;
+    s_ea[i] = sqrt(s_e2[i]);
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, j = blockIdx.x * kTdBisWarps + (threadIdx.x >> 5);
+  if (j >= job.K) return;
+  // Gershgorin interval
+  double lo = 1e300, hi = -1e300, e2max = 0.0;
+  for (int i = lane; i < B; i += 32) {
+    const double r = s_ea[i] + (i ? s_ea[i - 1] : 0.0);
+    lo = fmin(lo, s_d[i] - r);
+    hi = fmax(hi, s_d[i] + r);
+    e2max = fmax(e2max, s_e2[i]);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    e2max = fmax(e2max, __shfl_xor_sync(0xffffffffu, e2max, o));
+  }
+  const double tn = fmax(fabs(lo), fabs(hi));
+  const double pivmin = kSafeMin * fmax(1.0, e2max);
+  lo -= 4.0 * kEps * tn + 2.0 * pivmin;
+  hi += 4.0 * kEps * tn + 2.0 * pivmin;
+  const int m = B - 1 - j;
+  for (int it = 0; it < 64; ++it) {
+    const double width = hi - lo;
+    if (width <= fmax(2.0 * kEps * fmax(fabs(lo), fabs(hi)), 4.0 * kEps * tn) + pivmin) break;
+    const double x = lo + width * (double)(lane + 1) * (1.0 / 33.0);
+    const int cnt = sturm_count(s_d, s_e2, B, x, pivmin);
+    const int nle = __popc(__ballot_sync(0xffffffffu, cnt <= m));  // counts grow with x: a prefix of lanes
+    const double xlo = __shfl_sync(0xffffffffu, x, nle > 0 ? nle - 1 : 0);
+    const double xhi = __shfl_sync(0xffffffffu, x, nle < 32 ? nle : 31);
+    if (nle > 0) lo = xlo;
+    if (nle < 32) hi = xhi;
+  }
+  if (lane == 0) job.w[j] = 0.5 * (lo + hi);
+}
+
+// start vector of inverse iteration: splitmix64 of (vector, row) mapped to [-0.5, 0.5)
+__device__ __forceinline__ double td_start(int j, int i) {
+  unsigned long long z = 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1) +
+                         0xBF58476D1CE4E5B9ull * (unsigned long long)(j + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z ^= z >> 31;
+  return (double)(z >> 11) * (1.0 / 9007199254740992.0) - 0.5;
+}
+
+// Y[:, j] = eigenvector j of the real tridiagonal (d, |e|) for eigenvalue w[j]:
+// kTdInvIters solves (T - w_j I) y' = y with T - w_j I = L D L^T unpivoted
+// (pivots below eps ||T|| raised to it), each followed by Gram-Schmidt against
+// the finished members of j's cluster and normalisation.  Round r solves the
+// r-th member of every cluster.  Y and the multipliers L are B x K, row-major
+// ([i][j]: the threads of a warp touch consecutive words).
+__global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs) {
+  const TridiagJob job = jobs.j[blockIdx.x];
+  const int B = job.B, K = job.K, j = threadIdx.x;
+  __shared__ double s_d[kTridiagMaxB], s_e[kTridiagMaxB], s_w[kTridiagMaxB];
+  __shared__ int s_first[kTridiagMaxB], s_pos[kTridiagMaxB];
+  __shared__ double s_tn;
+  __shared__ int s_rounds;
+  for (int i = j; i < B; i += blockDim.x) {
+    s_d[i] = job.d[i];
+    const double2 e = i + 1 < B ? job.e[i] : make_double2(0.0, 0.0);
+    s_e[i] = sqrt(e.x * e.x + e.y * e.y);
+  }
+  for (int i = j; i < K; i += blockDim.x) s_w[i] = job.w[i];
+  __syncthreads();
+  if (j == 0) {
+    double tn = 0.0;
+    for (int i = 0; i < B; ++i) tn = fmax(tn, fabs(s_d[i]) + s_e[i] + (i ? s_e[i - 1] : 0.0));
+    s_tn = tn;
+    int rounds = 1;
+    s_first[0] = 0;
+    s_pos[0] = 0;
+    for (int m = 1; m < K; ++m) {
+      const bool same = s_w[m - 1] - s_w[m] <= kTdClusterTol * tn;
+      s_first[m] = same ? s_first[m - 1] : m;
+      s_pos[m] = same ? s_pos[m - 1] + 1 : 0;
+      rounds = max(rounds, s_pos[m] + 1);
+    }
+    s_rounds = rounds;
+  }
+  __syncthreads();
+  const double floor = kEps * s_tn;
+  double* __restrict__ Y = job.Y;
+  double* __restrict__ L = job.lw;
+  const int nr = s_rounds;
+  for (int r = 0; r < nr; ++r) {
+    if (j < K && s_pos[j] == r) {
+      const double lam = s_w[j];
+      for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] = td_start(j, i);
+      for (int it = 0; it < kTdInvIters; ++it) {
+        // forward: q_i = (d_i - lam) - e_{i-1} l_{i-1}, l_i = e_i / q_i, z_i = y_i - l_{i-1} z_{i-1};
+        // Y[i] <- z_i / q_i
+        double q = s_d[0] - lam;
+        if (fabs(q) < floor) q = copysign(floor, q);
+        double z = 0.0, lprev = 0.0;
+        for (int i0 = 0; i0 < B; i0 += kTdChunk) {
+          double yv[kTdChunk], zq[kTdChunk], lv[kTdChunk];
+#pragma unroll
+          for (int u = 0; u < kTdChunk; ++u) yv[u] = i0 + u < B ? Y[(size_t)(i0 + u) * K + j] : 0.0;
+#pragma unroll
+          for (int u = 0; u < kTdChunk; ++u) {
+            const int i = i0 + u;
+            if (i < B) {
+              if (i > 0) {
+                q = (s_d[i] - lam) - s_e[i - 1] * lprev;
+                if (fabs(q) < floor) q = copysign(floor, q);
+              }
+              z = yv[u] - lprev * z;
+              lprev = s_e[i] / q;
+              zq[u] = z / q;
+              lv[u] = lprev;
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kTdChunk; ++u)
+            if (i0 + u < B) {
+              Y[(size_t)(i0 + u) * K + j] = zq[u];
+              L[(size_t)(i0 + u) * K + j] = lv[u];
+            }
+        }
+        // backward: y_i = Y[i] - l_i y_{i+1}
+        double y = 0.0, nrm = 0.0;
+        for (int i1 = B; i1 > 0; i1 -= kTdChunk) {
+          double zv[kTdChunk], lv[kTdChunk];
+#pragma unroll
+          for (int u = 0; u < kTdChunk; ++u) {
+            const int i = i1 - 1 - u;
+            zv[u] = i >= 0 ? Y[(size_t)i * K + j] : 0.0;
+            lv[u] = i >= 0 ? L[(size_t)i * K + j] : 0.0;
+          }
+#pragma unroll
+          for (int u = 0; u < kTdChunk; ++u) {
+            const int i = i1 - 1 - u;
+            if (i >= 0) {
+              y = i == B - 1 ? zv[u] : zv[u] - lv[u] * y;
+              zv[u] = y;
+              nrm = fma(y, y, nrm);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < kTdChunk; ++u) {
+            const int i = i1 - 1 - u;
+            if (i >= 0) Y[(size_t)i * K + j] = zv[u];
+          }
+        }
+        // modified Gram-Schmidt against the cluster's finished members
+        if (s_first[j] < j) {
+          for (int m = s_first[j]; m < j; ++m) {
+            double dot = 0.0;
+            for (int i = 0; i < B; ++i) dot = fma(Y[(size_t)i * K + m], Y[(size_t)i * K + j], dot);
+            for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] -= dot * Y[(size_t)i * K + m];
+          }
+          nrm = 0.0;
+          for (int i = 0; i < B; ++i) nrm = fma(Y[(size_t)i * K + j], Y[(size_t)i * K + j], nrm);
+        }
+        const double s = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+        for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] *= s;
+      }
+    }
+    __syncthreads();  // this round's vectors are final before the next round reads them
+  }
+}
+
+// Q[:, j] = H_0 H_1 ... H_{B-3} D Y[:, j], D = diag(phase) making the
+// subdiagonal real (phase_{k+1} = phase_k e_k / |e_k|).  A warp holds its
+// column in registers (lane: rows lane + 32 t).
+__global__ void __launch_bounds__(32 * kTdBackWarps) k_tridiag_back(TridiagJobs jobs) {
+  constexpr int T = kTridiagMaxB / 32;
+  const TridiagJob job = jobs.j[blockIdx.y];
+  const int B = job.B, K = job.K;
+  __shared__ double2 s_ph[kTridiagMaxB];
+  if (threadIdx.x == 0) {
+    double2 ph = make_double2(1.0, 0.0);
+    s_ph[0] = ph;
+    for (int k = 0; k + 1 < B; ++k) {
+      const double2 e = job.e[k];
+      const double a = sqrt(e.x * e.x + e.y * e.y);
+      if (a > 0.0) ph = zmul(ph, make_double2(e.x / a, e.y / a));
+      s_ph[k + 1] = ph;
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, j = blockIdx.x * kTdBackWarps + (threadIdx.x >> 5);
+  if (j >= K) return;
+  double2 vc[T];
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const int i = lane + 32 * t;
+    const double y = i < B ? job.Y[(size_t)i * K + j] : 0.0;
+    vc[t] = i < B ? make_double2(s_ph[i].x * y, s_ph[i].y * y) : make_double2(0.0, 0.0);
+  }
+  double2 nx[T];  // the next reflector, loaded one step ahead
+  auto load = [&](int k, double2* dst) {
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const int i = lane + 32 * t;
+      dst[t] = (k >= 0 && i > k && i < B) ? job.refl[(size_t)k * B + i] : make_double2(0.0, 0.0);
+    }
+  };
+  load(B - 3, nx);
+  for (int k = B - 3; k >= 0; --k) {
+    double2 v[T];
+#pragma unroll
+    for (int t = 0; t < T; ++t) v[t] = nx[t];
+    load(k - 1, nx);
+    double sx = 0.0, sy = 0.0;  // s = v^H column
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      sx = fma(v[t].x, vc[t].x, fma(v[t].y, vc[t].y, sx));
+      sy = fma(v[t].x, vc[t].y, fma(-v[t].y, vc[t].x, sy));
+    }
+    sx = 2.0 * warp_sum(sx);
+    sy = 2.0 * warp_sum(sy);
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      vc[t].x -= v[t].x * sx - v[t].y * sy;
+      vc[t].y -= v[t].x * sy + v[t].y * sx;
+    }
+  }
+#pragma unroll
+  for (int t = 0; t < T; ++t) {
+    const int i = lane + 32 * t;
+    if (i < B) job.Q[(size_t)i * job.ldq + j] = vc[t];
+  }
+}
+
+std::mutex g_td_mu;
+
+}  // namespace
+
+bool tridiag_eig_supported(int B) {
+  if (B < kTridiagMinB || B > kTridiagMaxB) return false;
+  static std::vector<int> known;  // per device: -1 unknown, 0 no, 1 yes
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  std::lock_guard<std::mutex> lock(g_td_mu);
+  if ((int)known.size() <= dev) known.resize(dev + 1, -1);
+  int& ok = known[dev];
+  if (ok < 0) {
+    ok = 0;
+    const size_t sm = td_smem(kTridiagMaxB);
+    if (cudaFuncSetAttribute(k_hermitian_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm) ==
+        cudaSuccess) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(kTdCl);
+      cfg.blockDim = dim3(kTdThreads);
+      cfg.dynamicSmemBytes = sm;
+      int n = 0;
+      if (cudaOccupancyMaxActiveClusters(&n, k_hermitian_tridiag, &cfg) == cudaSuccess && n > 0) ok = 1;
+    }
+    (void)cudaGetLastError();
+  }
+  return ok == 1;
+}
+
+int tridiag_eig_batch(const std::vector<TridiagJob>& all, cudaStream_t st) {
+  for (const TridiagJob& j : all)
+    KL_CHECK_ARG(j.B >= kTridiagMinB && j.B <= kTridiagMaxB && j.K >= 1 && j.K <= j.B && j.ldq >= j.K,
+                 "tridiag_eig: matrix order or K out of range");
+  for (size_t j0 = 0; j0 < all.size(); j0 += kTdMaxJobs) {
+    const int nj = (int)std::min(all.size() - j0, (size_t)kTdMaxJobs);
+    TridiagJobs jobs{};
+    int bmax = 1, kmax = 1;
+    for (int j = 0; j < nj; ++j) {
+      jobs.j[j] = all[j0 + j];
+      bmax = std::max(bmax, jobs.j[j].B);
+      kmax = std::max(kmax, jobs.j[j].K);
+    }
+    const size_t sm = td_smem(bmax);
+    KL_CUDA_TRY(cudaFuncSetAttribute(k_hermitian_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_hermitian_tridiag<<<nj * kTdCl, kTdThreads, sm, st>>>(jobs);
+    KL_CUDA_TRY(cudaGetLastError());
+    k_tridiag_bisect<<<dim3((kmax + kTdBisWarps - 1) / kTdBisWarps, nj), 32 * kTdBisWarps, 0, st>>>(jobs);
+    KL_CUDA_TRY(cudaGetLastError());
+    k_tridiag_invit<<<nj, kTridiagMaxB, 0, st>>>(jobs);
+    KL_CUDA_TRY(cudaGetLastError());
+    k_tridiag_back<<<dim3((kmax + kTdBackWarps - 1) / kTdBackWarps, nj), 32 * kTdBackWarps, 0, st>>>(jobs);
+    KL_CUDA_TRY(cudaGetLastError());
+  }
+  return KL_OK;
+}
+
+}  // namespace kl

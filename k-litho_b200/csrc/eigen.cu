@@ -1445,27 +1445,56 @@ __global__ void k_ritz_scale(const double2* __restrict__ Q, int ldq, const doubl
 
 // TCC = A A^H with S <= kGramMaxS columns: the TCC's range is span(A), so the
 // Rayleigh-Ritz step on that span is exact.  G = A^H A (S x S, FP64 products
-// of the FP32 factor), G = V diag(w) V^H by Jacobi, U = A V diag(w)^{-1/2}.
-// The Jacobi eigensolves of all problems run in one launch, one CTA each.
+// of the FP32 factor), G = V diag(w) V^H, U = A V diag(w)^{-1/2}.  Orders the
+// cluster reduction handles (64 .. 256) take the tridiagonal solver
+// (eig_tridiag.cu), smaller ones Jacobi on one CTA; all problems of a path are
+// solved in one batch of launches.
 int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
   const size_t n = pr.size();
   std::vector<Workspace> ws(n);
-  std::vector<JacobiJob> jobs(n);
+  std::vector<JacobiJob> jobs;
+  std::vector<TridiagJob> tjobs;
+  std::vector<char> tri(n, 0);
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S, K = pr[i].K;
     Workspace& w = ws[i];
     w.st = st;
+    tri[i] = tridiag_eig_supported(S) ? 1 : 0;
     int arc;
     if ((arc = w.get(&w.G, (size_t)S * S)) || (arc = w.get(&w.Q, (size_t)S * S)) ||
-        (arc = w.get(&w.rot, jacobi_log_elems(S))) || (arc = w.get(&w.jst, (size_t)S + 1)) ||
-        (arc = w.get(&w.W, (size_t)S * K)) || (arc = w.get(&w.w, (size_t)S)))
+        (arc = w.get(&w.jst, (size_t)S + 1)) || (arc = w.get(&w.W, (size_t)S * K)) || (arc = w.get(&w.w, (size_t)S)))
       return arc;
+    if (tri[i]) {
+      TridiagJob t{};
+      double* lw = nullptr;
+      double* y = nullptr;
+      double* d = nullptr;
+      double2* e = nullptr;
+      if ((arc = w.get(&w.Z, (size_t)S * S)) || (arc = w.get(&d, (size_t)S)) || (arc = w.get(&e, (size_t)S)) ||
+          (arc = w.get(&lw, (size_t)S * K)) || (arc = w.get(&y, (size_t)S * K)))
+        return arc;
+      t.H = w.G;
+      t.refl = w.Z;
+      t.d = d;
+      t.e = e;
+      t.w = w.w;
+      t.lw = lw;
+      t.Y = y;
+      t.Q = w.Q;
+      t.B = S;
+      t.K = K;
+      t.ldq = S;
+      tjobs.push_back(t);
+    } else {
+      if ((arc = w.get(&w.rot, jacobi_log_elems(S)))) return arc;
+      jobs.push_back(JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S});
+    }
     int rc = zgemm<G_AHA>(pr[i].A, S, pr[i].A, S, w.G, S, S, S, pr[i].N, st);
     if (rc) return rc;
-    jobs[i] = JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S};
   }
   int rc = jacobi_batch(jobs, st);
   if (rc) return rc;
+  if ((rc = tridiag_eig_batch(tjobs, st))) return rc;
   std::vector<int> nsteps(n, 0);
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S, K = pr[i].K;
@@ -1473,11 +1502,18 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
     KL_CUDA_TRY(cudaGetLastError());
     if ((rc = zgemm<G_AY>(pr[i].A, S, ws[i].W, K, pr[i].U, K, pr[i].N, K, S, st))) return rc;
     KL_CUDA_TRY(cudaMemcpyAsync(pr[i].evals, ws[i].w, sizeof(double) * K, cudaMemcpyDeviceToDevice, st));
-    KL_CUDA_TRY(cudaMemcpyAsync(&nsteps[i], ws[i].jst, sizeof(int), cudaMemcpyDeviceToHost, st));
+    if (!tri[i]) KL_CUDA_TRY(cudaMemcpyAsync(&nsteps[i], ws[i].jst, sizeof(int), cudaMemcpyDeviceToHost, st));
   }
   KL_CUDA_TRY(cudaStreamSynchronize(st));
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S;
+    if (tri[i]) {
+      if (pr[i].res) {
+        pr[i].res->iterations = 1;  // one direct solve
+        pr[i].res->residual = 0.0;
+      }
+      continue;
+    }
     if (nsteps[i] < 0) {
       set_error("eig_topk_factor: the cluster Jacobi eigensolve timed out exchanging rotations");
       return KL_ERR_CUDA;

@@ -75,7 +75,8 @@ struct EigenOptions {
 };
 
 struct EigenResult {
-  int iterations;   // subspace iterations, or Jacobi sweeps of a one-step Gram solve
+  int iterations;   // subspace iterations; Jacobi sweeps of a one-step Gram solve (1 when it
+                    // ran the tridiagonal solver)
   double residual;  // max relative Ritz-value change at the last check
 };
 
@@ -103,6 +104,26 @@ int eig_topk_dense(const double2* tcc, int N, const EigenOptions& opt, double2* 
 // Operator given by a materialised FP32 TCC (N x N).
 int eig_topk_dense_c64(const float2* tcc, int N, const EigenOptions& opt, double2* U,
                        double* evals, EigenResult* res, cudaStream_t st);
+
+// Top-K eigenpairs of a Hermitian B x B matrix, kTridiagMinB <= B <= kTridiagMaxB, by
+// Householder tridiagonalisation on a thread-block cluster, bisection and inverse
+// iteration (eig_tridiag.cu).  The work buffers belong to the caller.
+constexpr int kTridiagMinB = 64;
+constexpr int kTridiagMaxB = 256;
+struct TridiagJob {
+  const double2* H;  // B x B Hermitian, row-major (read only)
+  double2* refl;     // B x B work: Householder vector k in row k, columns k+1 .. B-1
+  double* d;         // B work: diagonal of the tridiagonal T
+  double2* e;        // B work: e[k] = T[k+1][k]
+  double* w;         // K eigenvalues, descending
+  double* lw;        // B x K work: multipliers of the inverse-iteration solves
+  double* Y;         // B x K work: eigenvectors of the real tridiagonal
+  double2* Q;        // B x ldq, row-major: column j < K = eigenvector j
+  int B, K, ldq;
+};
+// true when the device can run the cluster reduction for order B
+bool tridiag_eig_supported(int B);
+int tridiag_eig_batch(const std::vector<TridiagJob>& jobs, cudaStream_t st);
 
 // Kernels in the reference layout: krn[k][j] = U[n-1-j][k] (klitho_tcc.cpp:358-362),
 // as separate float32 planes.

@@ -307,6 +307,35 @@ int topk_finish(TopkBuffers& b, int N, int K, int nk, float* krn_re_host, float*
 
 }  // namespace
 
+int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* vecs_dev, void* stream) {
+  KL_CHECK_ARG(H_dev && evals_dev && vecs_dev, "kl_hermitian_topk: NULL argument");
+  KL_CHECK_ARG(B >= kl::kTridiagMinB && B <= kl::kTridiagMaxB, "kl_hermitian_topk: B must be in [64, 256]");
+  KL_CHECK_ARG(K >= 1 && K <= B, "kl_hermitian_topk: K must be in [1, B]");
+  KL_CHECK_ARG(kl::tridiag_eig_supported(B),
+               "kl_hermitian_topk: this device cannot co-schedule the 8-CTA cluster of the reduction");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const size_t n2 = sizeof(double2) * B * B, nv = sizeof(double) * B * K;
+  const size_t bytes = n2 + sizeof(double) * B + sizeof(double2) * B + 2 * nv;
+  void* buf = nullptr;
+  if (int rc = kl::scratch_alloc(&buf, bytes, st, "kl_hermitian_topk work")) return rc;
+  char* c = static_cast<char*>(buf);
+  kl::TridiagJob j{};
+  j.H = static_cast<const double2*>(H_dev);
+  j.refl = reinterpret_cast<double2*>(c);
+  j.e = reinterpret_cast<double2*>(c + n2);
+  j.d = reinterpret_cast<double*>(c + n2 + sizeof(double2) * B);
+  j.lw = reinterpret_cast<double*>(c + n2 + sizeof(double2) * B + sizeof(double) * B);
+  j.Y = j.lw + (size_t)B * K;
+  j.w = evals_dev;
+  j.Q = static_cast<double2*>(vecs_dev);
+  j.B = B;
+  j.K = K;
+  j.ldq = K;
+  const int rc = kl::tridiag_eig_batch({j}, st);
+  kl::scratch_free(buf, st);
+  return rc;
+}
+
 int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn_im_host,
                 float* scales_host, double* evals_host, int* iterations) {
   KL_CHECK_ARG(p && krn_re_host && krn_im_host && scales_host, "kl_topk_eig: NULL argument");

@@ -93,6 +93,7 @@ def lib() -> ctypes.CDLL:
         L.kl_tcc_plan_destroy.argtypes = [_vp]
         L.kl_tcc_plan_info.argtypes = [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_float_p]
         L.kl_tcc_factor.argtypes = [_vp, _vp, _vp]
+        L.kl_hermitian_topk.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
         L.kl_tcc_build.argtypes = [_vp, _vp, _vp]
         L.kl_tcc_minmax.argtypes = [_vp, _vp, ctypes.POINTER(ctypes.c_double), _vp]
         L.kl_topk_eig.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _c_float_p, _c_float_p,
@@ -508,6 +509,15 @@ def fp64_socs_forward(masks_dev, Nx: int, Ny: int, kernels_dev, scales_dev, imag
     check(lib().kl_fp64_socs_forward(_dev_ptr(masks_dev), int(n), int(Lx), int(Ly), int(Nx), int(Ny),
                                      _dev_ptr(kernels_dev), _dev_ptr(scales_dev), int(nk),
                                      _dev_ptr(images_dev), _stream_ptr(stream)), "kl_fp64_socs_forward")
+
+
+def hermitian_topk(H_dev, K: int, evals_dev, vecs_dev, stream=None) -> None:
+    """Top-K eigenpairs of the Hermitian H (B, B) complex128 on the device,
+    64 <= B <= 256: eigenvalues descending into evals (K,) float64, eigenvector j
+    into vecs[:, j] of vecs (B, K) complex128."""
+    B = H_dev.shape[0]
+    check(lib().kl_hermitian_topk(_dev_ptr(H_dev), int(B), int(K), _dev_ptr(evals_dev), _dev_ptr(vecs_dev),
+                                  _stream_ptr(stream)), "kl_hermitian_topk")
 
 
 def fp64_mask_spectrum(mask_dev, spectrum_dev, stream=None) -> None:
