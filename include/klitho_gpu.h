@@ -344,6 +344,13 @@ int kl_tcc_plan_info(kl_tcc_plan plan, int* Nx, int* Ny, int* N, int* S, float* 
 /* Copy the FP32 factor A (N x S c64, row-major) to A_dev (fast path only). */
 int kl_tcc_factor(kl_tcc_plan plan, float* A_dev, void* stream);
 
+/* G = A^H A (S x S complex128, row-major) of a TCC factor A (N x S complex64,
+ * row-major, e.g. from kl_tcc_factor) on the device: the Gram step of
+ * kl_topk_eig.  Exact products of the FP32 factor in FP64 -- integer digits on
+ * the tensor cores for S <= 256 and N <= 500000 on B200, FP64 CUDA cores
+ * otherwise.  Synchronous (reports pipeline timeouts). */
+int kl_factor_gram(const void* A_dev, int N, int S, void* G_dev, void* stream);
+
 /* Top-K eigenpairs of a Hermitian B x B complex128 matrix on the device
  * (row-major, 64 <= B <= 256, 1 <= K <= B): the eigensolve behind kl_topk_eig's
  * Gram step, the part of zheevr (klitho_tcc.cpp:300-377) that remains once the

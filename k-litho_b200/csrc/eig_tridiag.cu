@@ -8,16 +8,20 @@
 //   k_hermitian_tridiag  one thread-block cluster of 8 CTAs per matrix, the
 //                        matrix's rows dealt round-robin over the CTAs'
 //                        shared memory; B - 2 reflector steps, each a
-//                        reflector broadcast, a distributed matvec and a
-//                        rank-2 update, separated by two cluster barriers
-//   k_tridiag_bisect     one warp per wanted eigenvalue: 32-point multisection
-//                        on Sturm counts of the real tridiagonal D^H T D
+//                        distributed matvec and a rank-2 update after two
+//                        cluster barriers, the next reflector formed by the
+//                        warp that updates its row as soon as it has
+//   k_tridiag_bisect     one CTA per wanted eigenvalue: 256-point multisection
+//                        on division-free Sturm counts of the real tridiagonal
+//                        D^H T D
 //   k_tridiag_invit      one thread per eigenvector: inverse iteration with
 //                        the unpivoted L D L^T factorisation of T - lambda I,
 //                        Gram-Schmidt against the earlier members of a cluster
-//                        of close eigenvalues (clusters run in rounds)
+//                        of close eigenvalues (clusters run in rounds); the
+//                        vectors stay in shared memory when they fit
 //   k_tridiag_back       one warp per eigenvector: phases, then the B - 2
-//                        reflectors in reverse order
+//                        reflectors in reverse order, staged through shared
+//                        memory 16 at a time
 // Everything is complex / real FP64.  No step waits on another CTA except
 // through the cluster barrier, so nothing here can spin.
 #include <cooperative_groups.h>
@@ -36,8 +40,10 @@ namespace {
 constexpr int kTdCl = 8;            // CTAs per matrix (a portable cluster)
 constexpr int kTdThreads = 512;     // threads per CTA of the reduction
 constexpr int kTdMaxJobs = 16;      // matrices per launch
-constexpr int kTdBisWarps = 8;      // eigenvalues per CTA of the bisection
-constexpr int kTdBackWarps = 8;     // eigenvectors per CTA of the back-transform
+constexpr int kTdBisPoints = 256;   // Sturm counts per pass of the bisection (threads per eigenvalue)
+constexpr int kTdBackWarps = 16;    // eigenvectors per CTA of the back-transform
+constexpr int kTdBackRefl = 16;     // reflectors staged per pass of the back-transform
+constexpr size_t kTdInvSmemCap = 200 * 1024;  // inverse iteration keeps its vectors on chip up to this
 constexpr int kTdInvIters = 3;      // inverse-iteration solves per eigenvector
 constexpr int kTdChunk = 8;         // elements staged in registers per memory pass
 // eigenvalues closer than this multiple of ||T|| are one cluster: their vectors
@@ -69,13 +75,49 @@ __host__ __device__ inline size_t td_smem(int B) {
 // ---------------------------------------------------------------------------
 // Householder reduction H = Q T Q^H.  Row i of H lives in CTA i % 8 (local row
 // i / 8), so the trailing rows stay spread evenly as the reduction proceeds.
-// Step k: the owner of row k forms v (unit, supported on k+1..B-1) with
-// (I - 2 v v^H) x = alpha e_{k+1} for x = column k below the diagonal
-// (= conj(row k) right of it) and writes it into every CTA; each CTA forms
+// Step k: warp 0 of the CTA holding row k forms v (unit, supported on
+// k+1..B-1) with (I - 2 v v^H) x = alpha e_{k+1} for x = column k below the
+// diagonal (= conj(row k) right of it) as soon as row k is updated, and writes
+// it into every CTA; after a cluster barrier each CTA forms
 // p_i = sum_j H[i][j] v_j for its rows i > k and writes them into every CTA;
-// then every CTA updates its rows: H -= 2 (v w^H + w v^H), w = p - (v^H p) v.
+// after a second barrier every CTA updates its rows: H -= 2 (v w^H + w v^H), w = p - (v^H p) v.
 // Outputs d[k] = T[k][k], e[k] = T[k+1][k] = alpha_k, and v_k in refl row k.
 // ---------------------------------------------------------------------------
+// the reflector of step k, by one warp of the CTA holding row k (hk, already
+// updated through step k - 1): v into vdst of every CTA of the cluster and row
+// k of refl; d[k] and e[k] = alpha
+__device__ __forceinline__ void td_reflector(cooperative_groups::cluster_group& cl, const TridiagJob& job,
+                                             const double2* hk, double2* vdst, int k, int lane) {
+  const int B = job.B, j0 = k + 1;
+  double s2 = 0.0;
+  for (int j = j0 + lane; j < B; j += 32) {
+    const double2 h = hk[j];
+    s2 = fma(h.x, h.x, fma(h.y, h.y, s2));
+  }
+  s2 = warp_sum(s2);
+  const double2 x0 = make_double2(hk[j0].x, -hk[j0].y);
+  const double ax0 = sqrt(x0.x * x0.x + x0.y * x0.y), nx = sqrt(s2);
+  double2 alpha = make_double2(0.0, 0.0);
+  double sc = 0.0;
+  if (nx > 0.0) {
+    const double2 ph = ax0 > 0.0 ? make_double2(x0.x / ax0, x0.y / ax0) : make_double2(1.0, 0.0);
+    alpha = make_double2(-ph.x * nx, -ph.y * nx);
+    sc = 1.0 / sqrt(2.0 * nx * (nx + ax0));  // 1 / ||x - alpha e||
+  }
+  for (int j = j0 + lane; j < B; j += 32) {
+    double2 x = make_double2(hk[j].x, -hk[j].y);
+    if (j == j0) x = make_double2(x.x - alpha.x, x.y - alpha.y);
+    const double2 vj = make_double2(x.x * sc, x.y * sc);
+    job.refl[(size_t)k * B + j] = vj;
+#pragma unroll
+    for (int c = 0; c < kTdCl; ++c) cl.map_shared_rank(vdst, c)[j] = vj;
+  }
+  if (lane == 0) {
+    job.d[k] = hk[k].x;
+    job.e[k] = alpha;
+  }
+}
+
 __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
     k_hermitian_tridiag(TridiagJobs jobs) {
   namespace cg = cooperative_groups;
@@ -94,40 +136,13 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
     rows[x] = i < B ? job.H[(size_t)i * B + j] : zero;
   }
   __syncthreads();
+  if (B > 2 && me == 0 && warp == 0) td_reflector(cl, job, rows, vbuf, 0, lane);
   for (int k = 0; k + 2 < B; ++k) {
-    double2* v = vbuf + (size_t)(k & 1) * B;  // the owner of step k + 1 may write the other one early
+    // v of step k (by the warp that finished row k last step) is in every CTA,
+    // and every row of this CTA is updated through step k - 1
+    cl.sync();
+    const double2* v = vbuf + (size_t)(k & 1) * B;
     const int j0 = k + 1;
-    if (me == k % kTdCl && warp == 0) {
-      const double2* hk = rows + (size_t)(k / kTdCl) * B;
-      double s2 = 0.0;
-      for (int j = j0 + lane; j < B; j += 32) {
-        const double2 h = hk[j];
-        s2 = fma(h.x, h.x, fma(h.y, h.y, s2));
-      }
-      s2 = warp_sum(s2);
-      const double2 x0 = make_double2(hk[j0].x, -hk[j0].y);
-      const double ax0 = sqrt(x0.x * x0.x + x0.y * x0.y), nx = sqrt(s2);
-      double2 alpha = zero;
-      double sc = 0.0;
-      if (nx > 0.0) {
-        const double2 ph = ax0 > 0.0 ? make_double2(x0.x / ax0, x0.y / ax0) : make_double2(1.0, 0.0);
-        alpha = make_double2(-ph.x * nx, -ph.y * nx);
-        sc = 1.0 / sqrt(2.0 * nx * (nx + ax0));  // 1 / ||x - alpha e||
-      }
-      for (int j = j0 + lane; j < B; j += 32) {
-        double2 x = make_double2(hk[j].x, -hk[j].y);
-        if (j == j0) x = make_double2(x.x - alpha.x, x.y - alpha.y);
-        const double2 vj = make_double2(x.x * sc, x.y * sc);
-        job.refl[(size_t)k * B + j] = vj;
-#pragma unroll
-        for (int c = 0; c < kTdCl; ++c) cl.map_shared_rank(v, c)[j] = vj;
-      }
-      if (lane == 0) {
-        job.d[k] = hk[k].x;
-        job.e[k] = alpha;
-      }
-    }
-    cl.sync();  // v of step k is in every CTA
     const int lfirst = k < me ? 0 : (k - me) / kTdCl + 1;  // first local row below row k
     for (int l = lfirst + warp; l < R; l += nwarp) {
       const int i = kTdCl * l + me;
@@ -151,6 +166,10 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
       c = fma(a.x, b.x, fma(a.y, b.y, c));
     }
     c = warp_sum(c);
+    // row k + 1 is the first row below k of its CTA, so warp 0 there updates it
+    // first and then forms the next step's reflector at once (the buffer it
+    // writes was last read in step k - 1, before the first barrier above)
+    const bool next = k + 3 < B && me == (k + 1) % kTdCl;
     for (int l = lfirst + warp; l < R; l += nwarp) {
       const int i = kTdCl * l + me;
       if (i >= B) break;
@@ -168,9 +187,13 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
         h.y -= fma(v2.y, wj.x, fma(-v2.x, wj.y, fma(w2.y, vj.x, -w2.x * vj.y)));
         hr[j] = h;
       }
+      if (next && l == lfirst) {
+        __syncwarp();
+        td_reflector(cl, job, hr, vbuf + (size_t)((k + 1) & 1) * B, k + 1, lane);
+      }
     }
-    __syncthreads();  // the owner of row k + 1 reads it next
   }
+  __syncthreads();
   // the trailing 2 x 2 block (or the 1 x 1 matrix)
   if (tid == 0) {
     for (int i = B >= 2 ? B - 2 : 0; i < B; ++i) {
@@ -183,66 +206,97 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
   cl.sync();  // no CTA leaves while a peer may still address its shared memory
 }
 
-// Sturm count of the real tridiagonal (d, e2 = |e|^2): eigenvalues below x
-__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int B, double x, double pivmin) {
-  double q = d[0] - x;
-  if (fabs(q) <= pivmin) q = -pivmin;
-  int c = q < 0.0;
+// Sturm count of the real tridiagonal: the number of eigenvalues below x, as
+// the sign changes along p_0 = 1, p_i = (d_{i-1} - x) p_{i-1} - e2_{i-2} p_{i-2}
+// (the characteristic polynomials of the leading submatrices; Sturm's theorem).
+// d and e2 = |e|^2 come scaled by powers of two so that ||T|| is near 1; the
+// pair (p_{i-1}, p_i) is rescaled by a power of two every 4 steps, which keeps
+// it in range (a step grows it by at most ~3) and changes no sign.  A zero
+// takes the sign opposite to its predecessor.  One FMA per step on the
+// dependency chain (the ratio form q_i = p_i / p_{i-1} needs a division).
+__device__ __forceinline__ int sturm_count(const double* d, const double* e2, int B, double x) {
+  double pm = 1.0, p = d[0] - x;
+  int neg = p < 0.0 || p == 0.0;  // sign of p_1 (a zero counts as negative after p_0 = 1)
+  int c = neg;
   for (int i = 1; i < B; ++i) {
-    q = (d[i] - x) - e2[i - 1] / q;
-    if (fabs(q) <= pivmin) q = -pivmin;
-    c += q < 0.0;
+    const double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
+    pm = p;
+    p = pn;
+    if ((i & 3) == 0) {
+      const double a = fabs(p);
+      if (a > 0x1p400 || (a < 0x1p-400 && a > 0.0)) {
+        const double s = scalbn(1.0, -ilogb(a));
+        p *= s;
+        pm *= s;
+      }
+    }
+    const int n = p < 0.0 || (p == 0.0 && !neg);
+    c += n != neg;
+    neg = n;
   }
   return c;
 }
 
-// w[j] = the j-th largest eigenvalue: each lane counts at one of 32 points
-// splitting the warp's interval into 33 parts; the interval shrinks to the
-// part holding eigenvalue B - 1 - j (ascending) until it is a few ulps wide.
-__global__ void __launch_bounds__(32 * kTdBisWarps) k_tridiag_bisect(TridiagJobs jobs) {
+// w[j] = the j-th largest eigenvalue, one CTA each: its threads count at
+// kTdBisPoints points splitting the interval into kTdBisPoints + 1 parts, and
+// the interval shrinks to the part holding eigenvalue B - 1 - j (ascending)
+// until it is a few ulps wide (7 passes from the Gershgorin interval).
+__global__ void __launch_bounds__(kTdBisPoints) k_tridiag_bisect(TridiagJobs jobs) {
   const TridiagJob job = jobs.j[blockIdx.y];
-  const int B = job.B;
-  __shared__ double s_d[kTridiagMaxB], s_e2[kTridiagMaxB], s_ea[kTridiagMaxB];
-  for (int i = threadIdx.x; i < B; i += blockDim.x) {
-    s_d[i] = job.d[i];
+  const int B = job.B, j = blockIdx.x, tid = threadIdx.x;
+  if (j >= job.K) return;  // the whole CTA
+  __shared__ double s_d[kTridiagMaxB], s_e2[kTridiagMaxB];
+  __shared__ double s_lo[kTdBisPoints / 32], s_hi[kTdBisPoints / 32];
+  // Gershgorin interval and the norm scale
+  double lo = 1e300, hi = -1e300;
+  for (int i = tid; i < B; i += blockDim.x) {
     const double2 e = i + 1 < B ? job.e[i] : make_double2(0.0, 0.0);
-    s_e2[i] = e.x * e.x + e.y * e.y;
-    s_ea[i] = sqrt(s_e2[i]);
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, j = blockIdx.x * kTdBisWarps + (threadIdx.x >> 5);
-  if (j >= job.K) return;
-  // Gershgorin interval
-  double lo = 1e300, hi = -1e300, e2max = 0.0;
-  for (int i = lane; i < B; i += 32) {
-    const double r = s_ea[i] + (i ? s_ea[i - 1] : 0.0);
-    lo = fmin(lo, s_d[i] - r);
-    hi = fmax(hi, s_d[i] + r);
-    e2max = fmax(e2max, s_e2[i]);
+    const double2 f = i > 0 ? job.e[i - 1] : make_double2(0.0, 0.0);
+    const double r = sqrt(e.x * e.x + e.y * e.y) + sqrt(f.x * f.x + f.y * f.y), di = job.d[i];
+    lo = fmin(lo, di - r);
+    hi = fmax(hi, di + r);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
     hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    e2max = fmax(e2max, __shfl_xor_sync(0xffffffffu, e2max, o));
+  }
+  if ((tid & 31) == 0) {
+    s_lo[tid >> 5] = lo;
+    s_hi[tid >> 5] = hi;
+  }
+  __syncthreads();
+  for (int w = 0; w < (int)blockDim.x / 32; ++w) {
+    lo = fmin(lo, s_lo[w]);
+    hi = fmax(hi, s_hi[w]);
   }
   const double tn = fmax(fabs(lo), fabs(hi));
-  const double pivmin = kSafeMin * fmax(1.0, e2max);
-  lo -= 4.0 * kEps * tn + 2.0 * pivmin;
-  hi += 4.0 * kEps * tn + 2.0 * pivmin;
+  if (!(tn > 0.0)) {  // the zero matrix
+    if (tid == 0) job.w[j] = 0.0;
+    return;
+  }
+  const double sc = scalbn(1.0, -ilogb(tn)), isc = scalbn(1.0, ilogb(tn));  // exact powers of two
+  for (int i = tid; i < B; i += blockDim.x) {
+    const double2 e = i + 1 < B ? job.e[i] : make_double2(0.0, 0.0);
+    s_d[i] = job.d[i] * sc;
+    s_e2[i] = (e.x * sc) * (e.x * sc) + (e.y * sc) * (e.y * sc);
+  }
+  __syncthreads();
+  const double tns = tn * sc;
+  lo = lo * sc - 4.0 * kEps * tns;
+  hi = hi * sc + 4.0 * kEps * tns;
   const int m = B - 1 - j;
+  constexpr double kStep = 1.0 / (kTdBisPoints + 1);
   for (int it = 0; it < 64; ++it) {
     const double width = hi - lo;
-    if (width <= fmax(2.0 * kEps * fmax(fabs(lo), fabs(hi)), 4.0 * kEps * tn) + pivmin) break;
-    const double x = lo + width * (double)(lane + 1) * (1.0 / 33.0);
-    const int cnt = sturm_count(s_d, s_e2, B, x, pivmin);
-    const int nle = __popc(__ballot_sync(0xffffffffu, cnt <= m));  // counts grow with x: a prefix of lanes
-    const double xlo = __shfl_sync(0xffffffffu, x, nle > 0 ? nle - 1 : 0);
-    const double xhi = __shfl_sync(0xffffffffu, x, nle < 32 ? nle : 31);
+    if (width <= fmax(2.0 * kEps * fmax(fabs(lo), fabs(hi)), 4.0 * kEps * tns)) break;  // uniform
+    const double x = lo + width * ((double)(tid + 1) * kStep);
+    const int nle = __syncthreads_count(sturm_count(s_d, s_e2, B, x) <= m);  // a prefix of the points
+    const double xlo = lo + width * ((double)nle * kStep), xhi = lo + width * ((double)(nle + 1) * kStep);
     if (nle > 0) lo = xlo;
-    if (nle < 32) hi = xhi;
+    if (nle < kTdBisPoints) hi = xhi;
   }
-  if (lane == 0) job.w[j] = 0.5 * (lo + hi);
+  if (tid == 0) job.w[j] = 0.5 * (lo + hi) * isc;
 }
 
 // start vector of inverse iteration: splitmix64 of (vector, row) mapped to [-0.5, 0.5)
@@ -259,9 +313,11 @@ __device__ __forceinline__ double td_start(int j, int i) {
 // kTdInvIters solves (T - w_j I) y' = y with T - w_j I = L D L^T unpivoted
 // (pivots below eps ||T|| raised to it), each followed by Gram-Schmidt against
 // the finished members of j's cluster and normalisation.  Round r solves the
-// r-th member of every cluster.  Y and the multipliers L are B x K, row-major
-// ([i][j]: the threads of a warp touch consecutive words).
-__global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs) {
+// r-th member of every cluster.  The vectors and multipliers are B x K,
+// row-major ([i][j]: the threads of a warp touch consecutive words), in shared
+// memory when they fit (smem != 0), else in the job's work buffers.
+__global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs, int smem) {
+  extern __shared__ __align__(16) double ism[];
   const TridiagJob job = jobs.j[blockIdx.x];
   const int B = job.B, K = job.K, j = threadIdx.x;
   __shared__ double s_d[kTridiagMaxB], s_e[kTridiagMaxB], s_w[kTridiagMaxB];
@@ -291,9 +347,9 @@ __global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs
     s_rounds = rounds;
   }
   __syncthreads();
-  const double floor = kEps * s_tn;
-  double* __restrict__ Y = job.Y;
-  double* __restrict__ L = job.lw;
+  const double floor = fmax(kEps * s_tn, kSafeMin);
+  double* Y = smem ? ism : job.Y;
+  double* L = smem ? ism + (size_t)B * K : job.lw;
   const int nr = s_rounds;
   for (int r = 0; r < nr; ++r) {
     if (j < K && s_pos[j] == r) {
@@ -317,9 +373,10 @@ __global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs
                 q = (s_d[i] - lam) - s_e[i - 1] * lprev;
                 if (fabs(q) < floor) q = copysign(floor, q);
               }
+              const double rq = 1.0 / q;
               z = yv[u] - lprev * z;
-              lprev = s_e[i] / q;
-              zq[u] = z / q;
+              lprev = s_e[i] * rq;
+              zq[u] = z * rq;
               lv[u] = lprev;
             }
           }
@@ -371,15 +428,20 @@ __global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs
     }
     __syncthreads();  // this round's vectors are final before the next round reads them
   }
+  if (smem)
+    for (int x = j; x < B * K; x += blockDim.x) job.Y[x] = ism[x];
 }
 
 // Q[:, j] = H_0 H_1 ... H_{B-3} D Y[:, j], D = diag(phase) making the
 // subdiagonal real (phase_{k+1} = phase_k e_k / |e_k|).  A warp holds its
-// column in registers (lane: rows lane + 32 t).
+// column in registers (lane: rows lane + 32 t); the CTA stages kTdBackRefl
+// reflectors at a time in shared memory for all its warps.
 __global__ void __launch_bounds__(32 * kTdBackWarps) k_tridiag_back(TridiagJobs jobs) {
   constexpr int T = kTridiagMaxB / 32;
+  extern __shared__ __align__(16) double2 bsm[];  // kTdBackRefl x B
   const TridiagJob job = jobs.j[blockIdx.y];
   const int B = job.B, K = job.K;
+  if ((int)blockIdx.x * kTdBackWarps >= K) return;  // the whole CTA
   __shared__ double2 s_ph[kTridiagMaxB];
   if (threadIdx.x == 0) {
     double2 ph = make_double2(1.0, 0.0);
@@ -393,42 +455,48 @@ __global__ void __launch_bounds__(32 * kTdBackWarps) k_tridiag_back(TridiagJobs 
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, j = blockIdx.x * kTdBackWarps + (threadIdx.x >> 5);
-  if (j >= K) return;
+  const bool act = j < K;
   double2 vc[T];
 #pragma unroll
   for (int t = 0; t < T; ++t) {
     const int i = lane + 32 * t;
-    const double y = i < B ? job.Y[(size_t)i * K + j] : 0.0;
+    const double y = (act && i < B) ? job.Y[(size_t)i * K + j] : 0.0;
     vc[t] = i < B ? make_double2(s_ph[i].x * y, s_ph[i].y * y) : make_double2(0.0, 0.0);
   }
-  double2 nx[T];  // the next reflector, loaded one step ahead
-  auto load = [&](int k, double2* dst) {
-#pragma unroll
-    for (int t = 0; t < T; ++t) {
-      const int i = lane + 32 * t;
-      dst[t] = (k >= 0 && i > k && i < B) ? job.refl[(size_t)k * B + i] : make_double2(0.0, 0.0);
+  // reflectors k1 .. k0 (descending) per stage
+  for (int k1 = B - 3; k1 >= 0; k1 -= kTdBackRefl) {
+    const int k0 = max(0, k1 - kTdBackRefl + 1), nref = k1 - k0 + 1;
+    __syncthreads();  // the previous stage's reflectors are used up
+    for (int x = threadIdx.x; x < nref * B; x += blockDim.x) {
+      const int r = x / B, i = x - r * B, k = k1 - r;
+      bsm[x] = i > k ? job.refl[(size_t)k * B + i] : make_double2(0.0, 0.0);
     }
-  };
-  load(B - 3, nx);
-  for (int k = B - 3; k >= 0; --k) {
-    double2 v[T];
+    __syncthreads();
+    if (!act) continue;
+    for (int r = 0; r < nref; ++r) {
+      const double2* v = bsm + (size_t)r * B;
+      double2 vr[T];
 #pragma unroll
-    for (int t = 0; t < T; ++t) v[t] = nx[t];
-    load(k - 1, nx);
-    double sx = 0.0, sy = 0.0;  // s = v^H column
+      for (int t = 0; t < T; ++t) {
+        const int i = lane + 32 * t;
+        vr[t] = i < B ? v[i] : make_double2(0.0, 0.0);
+      }
+      double sx = 0.0, sy = 0.0;  // s = v^H column
 #pragma unroll
-    for (int t = 0; t < T; ++t) {
-      sx = fma(v[t].x, vc[t].x, fma(v[t].y, vc[t].y, sx));
-      sy = fma(v[t].x, vc[t].y, fma(-v[t].y, vc[t].x, sy));
-    }
-    sx = 2.0 * warp_sum(sx);
-    sy = 2.0 * warp_sum(sy);
+      for (int t = 0; t < T; ++t) {
+        sx = fma(vr[t].x, vc[t].x, fma(vr[t].y, vc[t].y, sx));
+        sy = fma(vr[t].x, vc[t].y, fma(-vr[t].y, vc[t].x, sy));
+      }
+      sx = 2.0 * warp_sum(sx);
+      sy = 2.0 * warp_sum(sy);
 #pragma unroll
-    for (int t = 0; t < T; ++t) {
-      vc[t].x -= v[t].x * sx - v[t].y * sy;
-      vc[t].y -= v[t].x * sy + v[t].y * sx;
+      for (int t = 0; t < T; ++t) {
+        vc[t].x -= vr[t].x * sx - vr[t].y * sy;
+        vc[t].y -= vr[t].x * sy + vr[t].y * sx;
+      }
     }
   }
+  if (!act) return;
 #pragma unroll
   for (int t = 0; t < T; ++t) {
     const int i = lane + 32 * t;
@@ -485,11 +553,17 @@ int tridiag_eig_batch(const std::vector<TridiagJob>& all, cudaStream_t st) {
     KL_CUDA_TRY(cudaFuncSetAttribute(k_hermitian_tridiag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_hermitian_tridiag<<<nj * kTdCl, kTdThreads, sm, st>>>(jobs);
     KL_CUDA_TRY(cudaGetLastError());
-    k_tridiag_bisect<<<dim3((kmax + kTdBisWarps - 1) / kTdBisWarps, nj), 32 * kTdBisWarps, 0, st>>>(jobs);
+    k_tridiag_bisect<<<dim3(kmax, nj), kTdBisPoints, 0, st>>>(jobs);
     KL_CUDA_TRY(cudaGetLastError());
-    k_tridiag_invit<<<nj, kTridiagMaxB, 0, st>>>(jobs);
+    const size_t ism = sizeof(double) * 2 * (size_t)bmax * kmax;
+    const bool on_chip = ism <= kTdInvSmemCap;
+    if (on_chip)
+      KL_CUDA_TRY(cudaFuncSetAttribute(k_tridiag_invit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ism));
+    k_tridiag_invit<<<nj, kTridiagMaxB, on_chip ? ism : 0, st>>>(jobs, on_chip ? 1 : 0);
     KL_CUDA_TRY(cudaGetLastError());
-    k_tridiag_back<<<dim3((kmax + kTdBackWarps - 1) / kTdBackWarps, nj), 32 * kTdBackWarps, 0, st>>>(jobs);
+    const size_t bsm = sizeof(double2) * kTdBackRefl * (size_t)bmax;
+    KL_CUDA_TRY(cudaFuncSetAttribute(k_tridiag_back, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+    k_tridiag_back<<<dim3((kmax + kTdBackWarps - 1) / kTdBackWarps, nj), 32 * kTdBackWarps, bsm, st>>>(jobs);
     KL_CUDA_TRY(cudaGetLastError());
   }
   return KL_OK;

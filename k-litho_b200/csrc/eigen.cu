@@ -1444,8 +1444,9 @@ __global__ void k_ritz_scale(const double2* __restrict__ Q, int ldq, const doubl
 }
 
 // TCC = A A^H with S <= kGramMaxS columns: the TCC's range is span(A), so the
-// Rayleigh-Ritz step on that span is exact.  G = A^H A (S x S, FP64 products
-// of the FP32 factor), G = V diag(w) V^H, U = A V diag(w)^{-1/2}.  Orders the
+// Rayleigh-Ritz step on that span is exact.  G = A^H A (S x S, exact FP64
+// products of the FP32 factor: integer digits on the tensor cores, gram_i8.cu,
+// or FP64 CUDA cores elsewhere), G = V diag(w) V^H, U = A V diag(w)^{-1/2}.  Orders the
 // cluster reduction handles (64 .. 256) take the tridiagonal solver
 // (eig_tridiag.cu), smaller ones Jacobi on one CTA; all problems of a path are
 // solved in one batch of launches.
@@ -1489,15 +1490,17 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
       if ((arc = w.get(&w.rot, jacobi_log_elems(S)))) return arc;
       jobs.push_back(JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S});
     }
-    int rc = zgemm<G_AHA>(pr[i].A, S, pr[i].A, S, w.G, S, S, S, pr[i].N, st);
-    if (rc) return rc;
+    if ((arc = w.get(&w.status, 1))) return arc;
+    KL_CUDA_TRY(cudaMemsetAsync(w.status, 0, sizeof(int), st));
+    if (int rc = gram_factor(pr[i].A, pr[i].N, S, w.G, w.status, st)) return rc;
   }
   int rc = jacobi_batch(jobs, st);
   if (rc) return rc;
   if ((rc = tridiag_eig_batch(tjobs, st))) return rc;
-  std::vector<int> nsteps(n, 0);
+  std::vector<int> nsteps(n, 0), gerr(n, 0);
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S, K = pr[i].K;
+    if (ws[i].status) KL_CUDA_TRY(cudaMemcpyAsync(&gerr[i], ws[i].status, sizeof(int), cudaMemcpyDeviceToHost, st));
     k_ritz_scale<<<(S * K + 255) / 256, 256, 0, st>>>(ws[i].Q, S, ws[i].w, S, K, ws[i].W);
     KL_CUDA_TRY(cudaGetLastError());
     if ((rc = zgemm<G_AY>(pr[i].A, S, ws[i].W, K, pr[i].U, K, pr[i].N, K, S, st))) return rc;
@@ -1507,6 +1510,11 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
   KL_CUDA_TRY(cudaStreamSynchronize(st));
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S;
+    if (gerr[i]) {
+      set_error("eig_topk_factor: the tensor-core Gram product timed out in its pipeline (code " +
+                std::to_string(gerr[i]) + ")");
+      return KL_ERR_CUDA;
+    }
     if (tri[i]) {
       if (pr[i].res) {
         pr[i].res->iterations = 1;  // one direct solve
@@ -1533,6 +1541,11 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
 }
 
 }  // namespace
+
+int gram_factor(const float2* A, int N, int S, double2* G, int* err_dev, cudaStream_t st) {
+  if (gram_i8_supported(N, S)) return gram_i8(A, N, S, G, err_dev, st);  // tensor cores, integer digits
+  return zgemm<G_AHA>(A, S, A, S, G, S, S, S, N, st);                    // FP64 CUDA cores
+}
 
 int eig_topk_factor(const float2* A, int N, int S, const EigenOptions& opt, double2* U,
                     double* evals, EigenResult* res, cudaStream_t st) {

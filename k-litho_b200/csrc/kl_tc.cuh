@@ -1,7 +1,8 @@
 // kl_tc.cuh -- building blocks of the tcgen05 kernels (sm_100a): mbarriers
 // with bounded waits, TMA tile loads, shared-memory matrix descriptors in the
 // 128-byte-swizzled K-major layout, tcgen05.mma of kind f16 (FP16 or BF16
-// operands, FP32 accumulator in TMEM), commits and TMEM loads; and the host
+// operands, FP32 accumulator in TMEM) and kind i8 (signed 8-bit operands,
+// 32-bit integer accumulator), commits and TMEM loads; and the host
 // side tensor-map encoder (cuTensorMapEncodeTiled through the runtime's
 // driver entry point).
 #pragma once
@@ -19,6 +20,11 @@ namespace tc {
 
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s bound on any pipeline wait
 
+// Instruction descriptor of tcgen05.mma kind::i8: dense, signed 32-bit
+// accumulator (D format 2), A and B signed 8-bit (format 1), both K-major.
+__host__ __device__ constexpr uint32_t idesc_s8(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
 // Instruction descriptor of tcgen05.mma kind::f16: dense, FP32 accumulator,
 // A and B both K-major, M x N tile; bf16 selects BF16 operands (else FP16).
 __host__ __device__ constexpr uint32_t idesc_f16(int M, int N, bool bf16) {
@@ -139,6 +145,14 @@ __device__ __forceinline__ void mma_f16(uint32_t tmem_d, uint64_t da, uint64_t d
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
       "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(0), "r"(0), "r"(0), "r"(0));
 }
+// signed 8-bit A and B from shared memory, signed 32-bit accumulator
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accum), "r"(0), "r"(0), "r"(0), "r"(0));
+}
 // A operand in TMEM (row m in lane m, two 16-bit K elements per 32-bit column)
 __device__ __forceinline__ void mma_f16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t db, uint32_t idesc,
                                            uint32_t accum) {
@@ -209,6 +223,28 @@ inline int make_map_2b(CUtensorMap* m, const void* base, int rows, int Kp, int b
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(m, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
+    return KL_ERR_CUDA;
+  }
+  return KL_OK;
+}
+
+// map of a row-major [rows][Kp] matrix of 1-byte elements, boxes of box_k x box_rows,
+// 128-byte swizzle (box_k must be 128)
+inline int make_map_1b(CUtensorMap* m, const void* base, int rows, int Kp, int box_k, int box_rows) {
+  EncodeTiledFn enc = encode_fn();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is unavailable");
+    return KL_ERR_CUDA;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)Kp, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)Kp};
+  const cuuint32_t box[2] = {(cuuint32_t)box_k, (cuuint32_t)box_rows};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
     return KL_ERR_CUDA;

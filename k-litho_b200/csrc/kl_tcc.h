@@ -105,6 +105,16 @@ int eig_topk_dense(const double2* tcc, int N, const EigenOptions& opt, double2* 
 int eig_topk_dense_c64(const float2* tcc, int N, const EigenOptions& opt, double2* U,
                        double* evals, EigenResult* res, cudaStream_t st);
 
+// G = A^H A (S x S complex128, row-major) of an FP32 factor A (N x S complex64),
+// exact to the factor's precision, by an integer-digit split on the tcgen05
+// tensor cores (gram_i8.cu).  err_dev (zeroed by the caller) receives a
+// nonzero code if a pipeline wait gave up.
+constexpr int kGramI8MaxS = 256;
+bool gram_i8_supported(int N, int S);
+int gram_i8(const float2* A, int N, int S, double2* G, int* err_dev, cudaStream_t st);
+// G = A^H A by gram_i8 where it applies, else by the FP64 CUDA-core GEMM
+int gram_factor(const float2* A, int N, int S, double2* G, int* err_dev, cudaStream_t st);
+
 // Top-K eigenpairs of a Hermitian B x B matrix, kTridiagMinB <= B <= kTridiagMaxB, by
 // Householder tridiagonalisation on a thread-block cluster, bisection and inverse
 // iteration (eig_tridiag.cu).  The work buffers belong to the caller.

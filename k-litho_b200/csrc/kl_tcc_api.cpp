@@ -307,6 +307,30 @@ int topk_finish(TopkBuffers& b, int N, int K, int nk, float* krn_re_host, float*
 
 }  // namespace
 
+int kl_factor_gram(const void* A_dev, int N, int S, void* G_dev, void* stream) {
+  KL_CHECK_ARG(A_dev && G_dev && N >= 1 && S >= 1, "kl_factor_gram: NULL argument or empty factor");
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int* err = nullptr;
+  if (int rc = kl::scratch_alloc((void**)&err, sizeof(int), st, "kl_factor_gram status")) return rc;
+  int rc = KL_OK, herr = 0;
+  if (cudaMemsetAsync(err, 0, sizeof(int), st) != cudaSuccess) {
+    kl::set_error("kl_factor_gram: cudaMemsetAsync failed");
+    rc = KL_ERR_CUDA;
+  }
+  if (!rc) rc = kl::gram_factor(static_cast<const float2*>(A_dev), N, S, static_cast<double2*>(G_dev), err, st);
+  if (!rc && (cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+              cudaStreamSynchronize(st) != cudaSuccess)) {
+    kl::set_error(std::string("kl_factor_gram: ") + cudaGetErrorString(cudaGetLastError()));
+    rc = KL_ERR_CUDA;
+  }
+  kl::scratch_free(err, st);
+  if (!rc && herr) {
+    kl::set_error("kl_factor_gram: a tensor-core pipeline wait gave up (code " + std::to_string(herr) + ")");
+    rc = KL_ERR_CUDA;
+  }
+  return rc;
+}
+
 int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* vecs_dev, void* stream) {
   KL_CHECK_ARG(H_dev && evals_dev && vecs_dev, "kl_hermitian_topk: NULL argument");
   KL_CHECK_ARG(B >= kl::kTridiagMinB && B <= kl::kTridiagMaxB, "kl_hermitian_topk: B must be in [64, 256]");

@@ -94,6 +94,7 @@ def lib() -> ctypes.CDLL:
         L.kl_tcc_plan_info.argtypes = [_vp, _c_int_p, _c_int_p, _c_int_p, _c_int_p, _c_float_p]
         L.kl_tcc_factor.argtypes = [_vp, _vp, _vp]
         L.kl_hermitian_topk.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
+        L.kl_factor_gram.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp]
         L.kl_tcc_build.argtypes = [_vp, _vp, _vp]
         L.kl_tcc_minmax.argtypes = [_vp, _vp, ctypes.POINTER(ctypes.c_double), _vp]
         L.kl_topk_eig.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _c_float_p, _c_float_p,
@@ -509,6 +510,13 @@ def fp64_socs_forward(masks_dev, Nx: int, Ny: int, kernels_dev, scales_dev, imag
     check(lib().kl_fp64_socs_forward(_dev_ptr(masks_dev), int(n), int(Lx), int(Ly), int(Nx), int(Ny),
                                      _dev_ptr(kernels_dev), _dev_ptr(scales_dev), int(nk),
                                      _dev_ptr(images_dev), _stream_ptr(stream)), "kl_fp64_socs_forward")
+
+
+def factor_gram(A_dev, G_dev, stream=None) -> None:
+    """G = A^H A (S, S) complex128 of a factor A (N, S) complex64 on the device."""
+    N, S = A_dev.shape
+    check(lib().kl_factor_gram(_dev_ptr(A_dev), int(N), int(S), _dev_ptr(G_dev), _stream_ptr(stream)),
+          "kl_factor_gram")
 
 
 def hermitian_topk(H_dev, K: int, evals_dev, vecs_dev, stream=None) -> None:
