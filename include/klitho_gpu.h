@@ -391,11 +391,18 @@ int kl_topk_eig(kl_tcc_plan plan, int nk, int block, float* krn_re_host, float* 
  * outputs of kl_topk_eig back to back: plan i's kernels at
  * krn_re_host + i*nk*N, its scales at scales_host + i*nk, evals_host (optional)
  * likewise, iterations (optional) at iterations[i].  On the fast path with
- * S <= 128 source points the Rayleigh-Ritz step on span(A) is exact and the
- * plans' eigensolves run concurrently in one launch; otherwise (or for FP64
- * plans) the plans are solved one after another. */
+ * S <= 256 source points the Rayleigh-Ritz step on span(A) is exact and the
+ * plans' eigensolves run concurrently in one batch of launches; otherwise (or
+ * for FP64 plans) the plans are solved one after another. */
 int kl_topk_eig_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, float* krn_re_host,
                       float* krn_im_host, float* scales_host, double* evals_host, int* iterations);
+/* kl_topk_eig / kl_topk_eig_batch with the kernels as interleaved complex64
+ * (re, im pairs: nk x N x 2 floats per plan) in one host buffer, for callers
+ * that hold kernels as complex arrays: one copy instead of two planes. */
+int kl_topk_eig_c64(kl_tcc_plan plan, int nk, int block, float* krn_host, float* scales_host,
+                    double* evals_host, int* iterations);
+int kl_topk_eig_batch_c64(const kl_tcc_plan* plans, int nplans, int nk, int block, float* krn_host,
+                          float* scales_host, double* evals_host, int* iterations);
 
 /* Hopkins image (calcImage + FT_c2r, klitho_tcc.cpp:269-290, :150-183) of
  * nclips masks: sum_s J_s |IFFT(P(.,s) conj . M)|^2, the source-point form

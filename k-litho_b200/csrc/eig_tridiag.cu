@@ -89,12 +89,16 @@ __host__ __device__ inline size_t td_smem(int B) {
 __device__ __forceinline__ void td_reflector(cooperative_groups::cluster_group& cl, const TridiagJob& job,
                                              const double2* hk, double2* vdst, int k, int lane) {
   const int B = job.B, j0 = k + 1;
-  double s2 = 0.0;
-  for (int j = j0 + lane; j < B; j += 32) {
+  double s2a = 0.0, s2b = 0.0;  // two partial sums: half the FP64 dependency chain
+  for (int j = j0 + lane; j < B; j += 64) {
     const double2 h = hk[j];
-    s2 = fma(h.x, h.x, fma(h.y, h.y, s2));
+    s2a += fma(h.x, h.x, h.y * h.y);
+    if (j + 32 < B) {
+      const double2 g = hk[j + 32];
+      s2b += fma(g.x, g.x, g.y * g.y);
+    }
   }
-  s2 = warp_sum(s2);
+  const double s2 = warp_sum(s2a + s2b);
   const double2 x0 = make_double2(hk[j0].x, -hk[j0].y);
   const double ax0 = sqrt(x0.x * x0.x + x0.y * x0.y), nx = sqrt(s2);
   double2 alpha = make_double2(0.0, 0.0);
@@ -148,24 +152,33 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
       const int i = kTdCl * l + me;
       if (i >= B) break;
       const double2* hr = rows + (size_t)l * B;
-      double ax = 0.0, ay = 0.0;
-      for (int j = j0 + lane; j < B; j += 32) {
+      double ax = 0.0, ay = 0.0, bx = 0.0, by = 0.0;  // two partial sums per part
+      for (int j = j0 + lane; j < B; j += 64) {
         const double2 h = hr[j], vj = v[j];
-        ax = fma(h.x, vj.x, fma(-h.y, vj.y, ax));
-        ay = fma(h.x, vj.y, fma(h.y, vj.x, ay));
+        ax += fma(h.x, vj.x, -h.y * vj.y);
+        ay += fma(h.x, vj.y, h.y * vj.x);
+        if (j + 32 < B) {
+          const double2 g = hr[j + 32], wj = v[j + 32];
+          bx += fma(g.x, wj.x, -g.y * wj.y);
+          by += fma(g.x, wj.y, g.y * wj.x);
+        }
       }
-      ax = warp_sum(ax);
-      ay = warp_sum(ay);
+      ax = warp_sum(ax + bx);
+      ay = warp_sum(ay + by);
       if (lane < kTdCl) cl.map_shared_rank(pbuf, lane)[i] = make_double2(ax, ay);
     }
     cl.sync();  // p of step k is in every CTA
     // c = Re(v^H p), the same sum in every warp
-    double c = 0.0;
-    for (int j = j0 + lane; j < B; j += 32) {
+    double ca = 0.0, cb = 0.0;
+    for (int j = j0 + lane; j < B; j += 64) {
       const double2 a = v[j], b = pbuf[j];
-      c = fma(a.x, b.x, fma(a.y, b.y, c));
+      ca += fma(a.x, b.x, a.y * b.y);
+      if (j + 32 < B) {
+        const double2 a2 = v[j + 32], b2 = pbuf[j + 32];
+        cb += fma(a2.x, b2.x, a2.y * b2.y);
+      }
     }
-    c = warp_sum(c);
+    const double c = warp_sum(ca + cb);
     // row k + 1 is the first row below k of its CTA, so warp 0 there updates it
     // first and then forms the next step's reflector at once (the buffer it
     // writes was last read in step k - 1, before the first barrier above)
@@ -481,14 +494,27 @@ __global__ void __launch_bounds__(32 * kTdBackWarps) k_tridiag_back(TridiagJobs 
         const int i = lane + 32 * t;
         vr[t] = i < B ? v[i] : make_double2(0.0, 0.0);
       }
-      double sx = 0.0, sy = 0.0;  // s = v^H column
+      double px[T], py[T];  // s = v^H column: independent products, then a tree
 #pragma unroll
       for (int t = 0; t < T; ++t) {
-        sx = fma(vr[t].x, vc[t].x, fma(vr[t].y, vc[t].y, sx));
-        sy = fma(vr[t].x, vc[t].y, fma(-vr[t].y, vc[t].x, sy));
+        px[t] = fma(vr[t].x, vc[t].x, vr[t].y * vc[t].y);
+        py[t] = fma(vr[t].x, vc[t].y, -vr[t].y * vc[t].x);
       }
-      sx = 2.0 * warp_sum(sx);
-      sy = 2.0 * warp_sum(sy);
+#pragma unroll
+      for (int h = T / 2; h > 0; h >>= 1)
+#pragma unroll
+        for (int t = 0; t < h; ++t) {
+          px[t] += px[t + h];
+          py[t] += py[t + h];
+        }
+      double sx = px[0], sy = py[0];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        sx += __shfl_xor_sync(0xffffffffu, sx, o);
+        sy += __shfl_xor_sync(0xffffffffu, sy, o);
+      }
+      sx *= 2.0;
+      sy *= 2.0;
 #pragma unroll
       for (int t = 0; t < T; ++t) {
         vc[t].x -= vr[t].x * sx - vr[t].y * sy;

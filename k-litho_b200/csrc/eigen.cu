@@ -1094,15 +1094,20 @@ __global__ void __launch_bounds__(32 * kVecWarps) k_jacobi_vectors(JacobiJobs jo
     for (int p = lane; p < B; p += 32) Q[(size_t)k * B + jst[1 + p]] = row[p];
 }
 
-// krn[k][j] = U[N-1-j][k] as float planes (klitho_tcc.cpp:358-362)
+// krn[k][j] = U[N-1-j][k] as float planes (klitho_tcc.cpp:358-362), or as
+// interleaved complex64 in re when im is null
 __global__ void k_to_kernels(const double2* __restrict__ U, int N, int ldu, int K,
                              float* __restrict__ re, float* __restrict__ im) {
   const size_t n = (size_t)N * K;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     const int k = (int)(i / N), j = (int)(i % N);
     const double2 v = U[(size_t)(N - 1 - j) * ldu + k];
-    re[i] = (float)v.x;
-    im[i] = (float)v.y;
+    if (im) {
+      re[i] = (float)v.x;
+      im[i] = (float)v.y;
+    } else {
+      reinterpret_cast<float2*>(re)[i] = make_float2((float)v.x, (float)v.y);
+    }
   }
 }
 

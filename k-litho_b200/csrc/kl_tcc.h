@@ -90,8 +90,8 @@ struct FactorProblem {
 };
 
 // Top-K eigenpairs of several TCC = A A^H at once (e.g. one per focus value):
-// factors with S <= 128 columns share one batched Gram eigensolve launch; the
-// rest are solved one after another by subspace iteration.
+// factors with S <= 256 columns share one batched Gram eigensolve; the rest
+// are solved one after another by subspace iteration.
 int eig_topk_factor_batch(const std::vector<FactorProblem>& problems, const EigenOptions& opt,
                           cudaStream_t st);
 
@@ -136,7 +136,7 @@ bool tridiag_eig_supported(int B);
 int tridiag_eig_batch(const std::vector<TridiagJob>& jobs, cudaStream_t st);
 
 // Kernels in the reference layout: krn[k][j] = U[n-1-j][k] (klitho_tcc.cpp:358-362),
-// as separate float32 planes.
+// as separate float32 planes, or interleaved complex64 in re (2 N K floats) when im is null.
 int eig_to_kernels(const double2* U, int N, int K, float* re, float* im, cudaStream_t st);
 
 }  // namespace kl

@@ -246,17 +246,19 @@ int kl_tcc_build_minmax(kl_tcc_plan p, double* out4) {
 namespace {
 
 // device buffers of one top-K solve
+// device buffers of one top-K solve; c64: the kernels interleaved (re holds
+// 2 N K floats, im is unused) instead of as two planes
 struct TopkBuffers {
   double2* U = nullptr;
   double* ev = nullptr;
   float *re = nullptr, *im = nullptr;
   kl::EigenResult res{};
-  int alloc(int N, int K) {
+  int alloc(int N, int K, bool c64) {
     int rc;
     if ((rc = kl::scratch_alloc((void**)&U, sizeof(double2) * (size_t)N * K, nullptr, "eigenvectors")) ||
         (rc = kl::scratch_alloc((void**)&ev, sizeof(double) * K, nullptr, "eigenvalues")) ||
-        (rc = kl::scratch_alloc((void**)&re, sizeof(float) * (size_t)N * K, nullptr, "kernels")) ||
-        (rc = kl::scratch_alloc((void**)&im, sizeof(float) * (size_t)N * K, nullptr, "kernels")))
+        (rc = kl::scratch_alloc((void**)&re, sizeof(float) * (size_t)N * K * (c64 ? 2 : 1), nullptr, "kernels")) ||
+        (!c64 && (rc = kl::scratch_alloc((void**)&im, sizeof(float) * (size_t)N * K, nullptr, "kernels"))))
       return rc;
     return KL_OK;
   }
@@ -280,13 +282,16 @@ kl::EigenOptions topk_options(int K, int block) {
 
 // kernels (reference layout) and eigenvalues to the host; the nk - K kernels
 // beyond the TCC's rank are zero
+// kernels, scales and eigenvalues to the host; krn_im_host null: the kernels
+// go interleaved (complex64) into krn_re_host
 int topk_finish(TopkBuffers& b, int N, int K, int nk, float* krn_re_host, float* krn_im_host,
                 float* scales_host, double* evals_host, int* iterations, cudaStream_t st) {
-  int rc = kl::eig_to_kernels(b.U, N, K, b.re, b.im, st);
+  const bool c64 = krn_im_host == nullptr;
+  int rc = kl::eig_to_kernels(b.U, N, K, b.re, c64 ? nullptr : b.im, st);
   if (rc) return rc;
   std::vector<double> evh(K);
-  cudaMemcpy(krn_re_host, b.re, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
-  cudaMemcpy(krn_im_host, b.im, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
+  cudaMemcpy(krn_re_host, b.re, sizeof(float) * (size_t)N * K * (c64 ? 2 : 1), cudaMemcpyDeviceToHost);
+  if (!c64) cudaMemcpy(krn_im_host, b.im, sizeof(float) * (size_t)N * K, cudaMemcpyDeviceToHost);
   cudaMemcpy(evh.data(), b.ev, sizeof(double) * K, cudaMemcpyDeviceToHost);
   if (cudaDeviceSynchronize() != cudaSuccess) {
     kl::set_error(std::string("kl_topk_eig: ") + cudaGetErrorString(cudaGetLastError()));
@@ -298,6 +303,10 @@ int topk_finish(TopkBuffers& b, int N, int K, int nk, float* krn_re_host, float*
     if (evals_host) evals_host[k] = v;
   }
   for (int k = K; k < nk; ++k) {
+    if (c64) {
+      std::memset(krn_re_host + 2 * (size_t)k * N, 0, 2 * sizeof(float) * N);
+      continue;
+    }
     std::memset(krn_re_host + (size_t)k * N, 0, sizeof(float) * N);
     std::memset(krn_im_host + (size_t)k * N, 0, sizeof(float) * N);
   }
@@ -360,9 +369,11 @@ int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* 
   return rc;
 }
 
-int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn_im_host,
-                float* scales_host, double* evals_host, int* iterations) {
-  KL_CHECK_ARG(p && krn_re_host && krn_im_host && scales_host, "kl_topk_eig: NULL argument");
+namespace {
+
+// kl_topk_eig; krn_im_host null: interleaved kernels (kl_topk_eig_c64)
+int topk_one(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn_im_host, float* scales_host,
+             double* evals_host, int* iterations) {
   const int N = p->pp.N, S = p->pp.S;
   KL_CHECK_ARG(nk > 0 && nk <= N, "kl_topk_eig: nk must be in [1, N]");
   cudaStream_t st = nullptr;
@@ -371,7 +382,7 @@ int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn
   const int K = std::min(nk, std::min(N, S));
   const kl::EigenOptions opt = topk_options(K, block);
   TopkBuffers b;
-  int rc = b.alloc(N, K);
+  int rc = b.alloc(N, K, krn_im_host == nullptr);
   if (rc) return rc;
   if (p->precision == KL_PREC_FAST) {
     rc = kl::eig_topk_factor(p->A, N, S, opt, b.U, b.ev, &b.res, st);
@@ -383,10 +394,10 @@ int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn
   return topk_finish(b, N, K, nk, krn_re_host, krn_im_host, scales_host, evals_host, iterations, st);
 }
 
-int kl_topk_eig_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, float* krn_re_host,
-                      float* krn_im_host, float* scales_host, double* evals_host, int* iterations) {
-  KL_CHECK_ARG(plans && nplans > 0 && krn_re_host && krn_im_host && scales_host,
-               "kl_topk_eig_batch: NULL argument or empty batch");
+// kl_topk_eig_batch; krn_im_host null: interleaved kernels (kl_topk_eig_batch_c64)
+int topk_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, float* krn_re_host, float* krn_im_host,
+               float* scales_host, double* evals_host, int* iterations) {
+  const bool c64 = krn_im_host == nullptr;
   const int N = plans[0] ? plans[0]->pp.N : 0;
   bool fast = true;
   for (int i = 0; i < nplans; ++i) {
@@ -396,11 +407,12 @@ int kl_topk_eig_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, f
   }
   KL_CHECK_ARG(nk > 0 && nk <= N, "kl_topk_eig_batch: nk must be in [1, N]");
   const size_t kstride = (size_t)nk * N;
+  const size_t rstride = kstride * (c64 ? 2 : 1);  // floats of one plan's kernels in krn_re_host
   if (!fast) {  // the FP64 path solves one plan after another
     for (int i = 0; i < nplans; ++i) {
-      const int rc = kl_topk_eig(plans[i], nk, block, krn_re_host + i * kstride, krn_im_host + i * kstride,
-                                 scales_host + (size_t)i * nk, evals_host ? evals_host + (size_t)i * nk : nullptr,
-                                 iterations ? iterations + i : nullptr);
+      const int rc = topk_one(plans[i], nk, block, krn_re_host + i * rstride,
+                              c64 ? nullptr : krn_im_host + i * kstride, scales_host + (size_t)i * nk,
+                              evals_host ? evals_host + (size_t)i * nk : nullptr, iterations ? iterations + i : nullptr);
       if (rc) return rc;
     }
     return KL_OK;
@@ -412,19 +424,46 @@ int kl_topk_eig_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, f
   for (int i = 0; i < nplans; ++i) {
     const int K = std::min(nk, std::min(N, plans[i]->pp.S));
     kmax = std::max(kmax, K);
-    int rc = bufs[i].alloc(N, K);
+    int rc = bufs[i].alloc(N, K, c64);
     if (rc) return rc;
     pr[i] = kl::FactorProblem{plans[i]->A, N, plans[i]->pp.S, K, bufs[i].U, bufs[i].ev, &bufs[i].res};
   }
   int rc = kl::eig_topk_factor_batch(pr, topk_options(kmax, block), st);
   if (rc) return rc;
   for (int i = 0; i < nplans; ++i) {
-    rc = topk_finish(bufs[i], N, pr[i].K, nk, krn_re_host + i * kstride, krn_im_host + i * kstride,
+    rc = topk_finish(bufs[i], N, pr[i].K, nk, krn_re_host + i * rstride, c64 ? nullptr : krn_im_host + i * kstride,
                      scales_host + (size_t)i * nk, evals_host ? evals_host + (size_t)i * nk : nullptr,
                      iterations ? iterations + i : nullptr, st);
     if (rc) return rc;
   }
   return KL_OK;
+}
+
+}  // namespace
+
+int kl_topk_eig(kl_tcc_plan p, int nk, int block, float* krn_re_host, float* krn_im_host, float* scales_host,
+                double* evals_host, int* iterations) {
+  KL_CHECK_ARG(p && krn_re_host && krn_im_host && scales_host, "kl_topk_eig: NULL argument");
+  return topk_one(p, nk, block, krn_re_host, krn_im_host, scales_host, evals_host, iterations);
+}
+
+int kl_topk_eig_c64(kl_tcc_plan p, int nk, int block, float* krn_host, float* scales_host, double* evals_host,
+                    int* iterations) {
+  KL_CHECK_ARG(p && krn_host && scales_host, "kl_topk_eig_c64: NULL argument");
+  return topk_one(p, nk, block, krn_host, nullptr, scales_host, evals_host, iterations);
+}
+
+int kl_topk_eig_batch(const kl_tcc_plan* plans, int nplans, int nk, int block, float* krn_re_host,
+                      float* krn_im_host, float* scales_host, double* evals_host, int* iterations) {
+  KL_CHECK_ARG(plans && nplans > 0 && krn_re_host && krn_im_host && scales_host,
+               "kl_topk_eig_batch: NULL argument or empty batch");
+  return topk_batch(plans, nplans, nk, block, krn_re_host, krn_im_host, scales_host, evals_host, iterations);
+}
+
+int kl_topk_eig_batch_c64(const kl_tcc_plan* plans, int nplans, int nk, int block, float* krn_host,
+                          float* scales_host, double* evals_host, int* iterations) {
+  KL_CHECK_ARG(plans && nplans > 0 && krn_host && scales_host, "kl_topk_eig_batch_c64: NULL argument or empty batch");
+  return topk_batch(plans, nplans, nk, block, krn_host, nullptr, scales_host, evals_host, iterations);
 }
 
 int kl_fp64_hopkins_image(kl_tcc_plan p, const float* masks_dev, int nclips, double* images_dev, void* stream) {

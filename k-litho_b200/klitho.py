@@ -102,6 +102,10 @@ def lib() -> ctypes.CDLL:
         L.kl_topk_eig_batch.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         _c_float_p, _c_float_p, _c_float_p,
                                         ctypes.POINTER(ctypes.c_double), _c_int_p]
+        L.kl_topk_eig_c64.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _c_float_p, _c_float_p,
+                                      ctypes.POINTER(ctypes.c_double), _c_int_p]
+        L.kl_topk_eig_batch_c64.argtypes = [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            _c_float_p, _c_float_p, ctypes.POINTER(ctypes.c_double), _c_int_p]
         L.kl_hopkins_image.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
         L.kl_fp64_hopkins_image.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp]
         L.kl_fp64_socs_forward.argtypes = [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
@@ -140,14 +144,6 @@ def check(rc: int, where: str) -> None:
 
 def _fp(a: np.ndarray):
     return a.ctypes.data_as(_c_float_p)
-
-
-def _planes_to_complex(re: np.ndarray, im: np.ndarray, shape) -> np.ndarray:
-    """complex64 array of `shape` from separate real and imaginary float32 planes."""
-    out = np.empty(shape, dtype=np.complex64)
-    out.real = re.reshape(shape)
-    out.imag = im.reshape(shape)
-    return out
 
 
 def _stream_ptr(stream) -> int | None:
@@ -448,31 +444,28 @@ class TccPlan:
     def topk(self, nk: int, block: int = 0):
         """(kernels nk x N complex64 in the reference layout, scales float32,
         eigenvalues float64, iterations)."""
-        re = np.empty(nk * self.N, dtype=np.float32)  # every entry is written
-        im = np.empty(nk * self.N, dtype=np.float32)
+        krn = np.empty((nk, self.N), dtype=np.complex64)  # every entry is written
         sc = np.zeros(nk, dtype=np.float32)
         ev = np.zeros(nk, dtype=np.float64)
         it = ctypes.c_int()
-        check(lib().kl_topk_eig(self._h, int(nk), int(block), _fp(re), _fp(im), _fp(sc),
-                                ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                ctypes.byref(it)), "kl_topk_eig")
-        return _planes_to_complex(re, im, (nk, self.N)), sc, ev, it.value
+        check(lib().kl_topk_eig_c64(self._h, int(nk), int(block), krn.ctypes.data_as(_c_float_p), _fp(sc),
+                                    ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                    ctypes.byref(it)), "kl_topk_eig_c64")
+        return krn, sc, ev, it.value
 
     @staticmethod
     def topk_batch(plans, nk: int, block: int = 0):
         """kl_topk_eig over several plans sharing N (e.g. a focus sweep) in one
         call: lists of (kernels, scales, eigenvalues, iterations) per plan."""
         n, N = len(plans), plans[0].N
-        re = np.empty(n * nk * N, dtype=np.float32)  # every entry is written
-        im = np.empty(n * nk * N, dtype=np.float32)
+        k = np.empty((n, nk, N), dtype=np.complex64)  # every entry is written
         sc = np.zeros(n * nk, dtype=np.float32)
         ev = np.zeros(n * nk, dtype=np.float64)
         it = np.zeros(n, dtype=np.int32)
         hs = (_vp * n)(*[p._h for p in plans])
-        check(lib().kl_topk_eig_batch(hs, n, int(nk), int(block), _fp(re), _fp(im), _fp(sc),
-                                      ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
-                                      it.ctypes.data_as(_c_int_p)), "kl_topk_eig_batch")
-        k = _planes_to_complex(re, im, (n, nk, N))
+        check(lib().kl_topk_eig_batch_c64(hs, n, int(nk), int(block), k.ctypes.data_as(_c_float_p), _fp(sc),
+                                          ev.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                          it.ctypes.data_as(_c_int_p)), "kl_topk_eig_batch_c64")
         return ([k[i] for i in range(n)], list(sc.reshape(n, nk)), list(ev.reshape(n, nk)),
                 [int(x) for x in it])
 

@@ -321,3 +321,27 @@ def test_config4_fast_vs_fp64_gpu_path(cuda):
     del Tf, T64
     tf.close()
     t64.close()
+
+
+def test_topk_planes_and_interleaved_agree(cuda):
+    # kl_topk_eig (two float planes, the CLI's layout) and kl_topk_eig_c64
+    # (interleaved, behind TccPlan.topk) return the same kernels bit for bit,
+    # including the zero kernels beyond the rank (nk > S)
+    import ctypes
+    src = K.createSource(71, "CrossQuadrupole", radius=0.12, offset=0.75)
+    plan = K.TccPlan(src, 1.35, synth.defocus_arg(-20.0), 1024, 1024, n_medium=1.44)
+    nk, N = plan.S + 4, plan.N
+    assert nk <= N  # rank S < nk: the last four kernels are zero
+    krn, sc, ev, it = plan.topk(nk)
+    re = np.empty(nk * N, np.float32)
+    im = np.empty(nk * N, np.float32)
+    sc2 = np.zeros(nk, np.float32)
+    ev2 = np.zeros(nk, np.float64)
+    it2 = ctypes.c_int()
+    K.check(K.lib().kl_topk_eig(plan._h, nk, 0, re.ctypes.data_as(K._c_float_p), im.ctypes.data_as(K._c_float_p),
+                                sc2.ctypes.data_as(K._c_float_p), ev2.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                ctypes.byref(it2)), "kl_topk_eig")
+    plan.close()
+    assert np.array_equal(krn.real.ravel(), re) and np.array_equal(krn.imag.ravel(), im)
+    assert np.array_equal(sc, sc2) and np.array_equal(ev, ev2) and it == it2.value
+    assert np.all(krn[-4:] == 0) and np.all(ev[-4:] == 0)
