@@ -8,9 +8,11 @@
 //   k_hermitian_tridiag  one thread-block cluster of 8 CTAs per matrix, the
 //                        matrix's rows dealt round-robin over the CTAs'
 //                        shared memory; B - 2 reflector steps, each a
-//                        distributed matvec and a rank-2 update after two
-//                        cluster barriers, the next reflector formed by the
-//                        warp that updates its row as soon as it has
+//                        distributed matvec and a rank-2 update, with the
+//                        reflector and the matvec exchanged as st.async
+//                        stores completing on the receivers' mbarriers; the
+//                        next reflector is formed by the warp that updates
+//                        its row as soon as it has
 //   k_tridiag_bisect     one CTA per wanted eigenvalue: 256-point multisection
 //                        on division-free Sturm counts of the real tridiagonal
 //                        D^H T D
@@ -22,8 +24,8 @@
 //   k_tridiag_back       one warp per eigenvector: phases, then the B - 2
 //                        reflectors in reverse order, staged through shared
 //                        memory 16 at a time
-// Everything is complex / real FP64.  No step waits on another CTA except
-// through the cluster barrier, so nothing here can spin.
+// Everything is complex / real FP64.  The reduction's exchange waits are
+// bounded (2 s): a timeout sets the job's error word instead of spinning.
 #include <cooperative_groups.h>
 
 #include <algorithm>
@@ -41,10 +43,10 @@ constexpr int kTdCl = 8;            // CTAs per matrix (a portable cluster)
 constexpr int kTdThreads = 512;     // threads per CTA of the reduction
 constexpr int kTdMaxJobs = 16;      // matrices per launch
 constexpr int kTdBisPoints = 256;   // Sturm counts per pass of the bisection (threads per eigenvalue)
-constexpr int kTdBackWarps = 16;    // eigenvectors per CTA of the back-transform
+constexpr int kTdBackWarps = 4;     // eigenvectors per CTA of the back-transform (more SMs per matrix)
 constexpr int kTdBackRefl = 16;     // reflectors staged per pass of the back-transform
 constexpr size_t kTdInvSmemCap = 200 * 1024;  // inverse iteration keeps its vectors on chip up to this
-constexpr int kTdInvIters = 3;      // inverse-iteration solves per eigenvector
+constexpr int kTdInvIters = 2;      // inverse-iteration solves per eigenvector (from a shift exact to a few ulps)
 constexpr int kTdChunk = 8;         // elements staged in registers per memory pass
 // eigenvalues closer than this multiple of ||T|| are one cluster: their vectors
 // are orthogonalised against each other (the others are orthogonal to within
@@ -52,6 +54,7 @@ constexpr int kTdChunk = 8;         // elements staged in registers per memory p
 constexpr double kTdClusterTol = 1e-7;
 constexpr double kEps = 2.220446049250313e-16;  // 2^-52
 constexpr double kSafeMin = 2.2250738585072014e-308;  // smallest normal double
+constexpr unsigned long long kTdWaitNs = 2000000000ull;  // bound on one exchange wait of the reduction
 
 struct TridiagJobs {
   TridiagJob j[kTdMaxJobs];
@@ -67,9 +70,52 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 __host__ __device__ inline int td_rows(int B) { return (B + kTdCl - 1) / kTdCl; }
-// shared memory of k_hermitian_tridiag: the CTA's rows, two reflector buffers, p
+// shared memory of k_hermitian_tridiag: the CTA's rows, two reflector and two
+// matvec buffers (by step parity)
 __host__ __device__ inline size_t td_smem(int B) {
-  return sizeof(double2) * ((size_t)td_rows(B) * B + 3 * (size_t)B);
+  return sizeof(double2) * ((size_t)td_rows(B) * B + 4 * (size_t)B);
+}
+
+// bytes one step k of order B delivers into each CTA's reflector (and matvec) buffer
+__host__ __device__ inline uint32_t td_step_bytes(int B, int k) { return (uint32_t)(B - k - 1) * 16u; }
+
+__device__ __forceinline__ uint32_t td_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+// address of `p`'s counterpart in the shared memory of CTA `cta` of the cluster
+__device__ __forceinline__ uint32_t td_cluster_addr(const void* p, uint32_t cta) {
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(td_smem_u32(p)), "r"(cta));
+  return r;
+}
+// dst[0] of CTA `cta` <- v; the 16 bytes complete on that CTA's barrier `bar`
+__device__ __forceinline__ void td_push(double2* dst, double2 v, uint64_t* bar, uint32_t cta) {
+  asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.f64 [%0], {%1, %2}, [%3];" ::"r"(
+                   td_cluster_addr(dst, cta)),
+               "d"(v.x), "d"(v.y), "r"(td_cluster_addr(bar, cta))
+               : "memory");
+}
+// this CTA expects `bytes` on `bar` in the barrier's current phase
+__device__ __forceinline__ void td_arm(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(td_smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// bounded wait for the phase of `bar` with `parity`; false after kTdWaitNs
+__device__ __forceinline__ bool td_wait(uint64_t* bar, uint32_t parity) {
+  unsigned long long t0 = 0;
+  for (int n = 0;; ++n) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(td_smem_u32(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (n == 0) t0 = t;
+    else if (t - t0 > kTdWaitNs) return false;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -77,17 +123,27 @@ __host__ __device__ inline size_t td_smem(int B) {
 // i / 8), so the trailing rows stay spread evenly as the reduction proceeds.
 // Step k: warp 0 of the CTA holding row k forms v (unit, supported on
 // k+1..B-1) with (I - 2 v v^H) x = alpha e_{k+1} for x = column k below the
-// diagonal (= conj(row k) right of it) as soon as row k is updated, and writes
-// it into every CTA; after a cluster barrier each CTA forms
-// p_i = sum_j H[i][j] v_j for its rows i > k and writes them into every CTA;
-// after a second barrier every CTA updates its rows: H -= 2 (v w^H + w v^H), w = p - (v^H p) v.
+// diagonal (= conj(row k) right of it) as soon as row k is updated, and sends
+// it into every CTA; each CTA, once its copy of v has landed, forms
+// p_i = sum_j H[i][j] v_j for its rows i > k and sends them into every CTA;
+// once all of p has landed, every CTA updates its rows:
+// H -= 2 (v w^H + w v^H), w = p - (v^H p) v.
+// The sends are st.async stores that complete their bytes on the receiving
+// CTA's mbarrier for that buffer (no cluster barrier per step).  Buffers
+// alternate by step parity; a CTA re-arms a buffer's barrier for step k + 2
+// as soon as its step-k data has landed, and the data of step k + 2 can only
+// be sent after every CTA has finished step k (it depends on all of step
+// k + 1's matvec), so no byte reaches an unarmed phase and no buffer is
+// overwritten while it is read.  Waits are bounded; a CTA that gives up
+// raises the job's error word and leaves the loop, and its peers then give
+// up on their next wait.
 // Outputs d[k] = T[k][k], e[k] = T[k+1][k] = alpha_k, and v_k in refl row k.
 // ---------------------------------------------------------------------------
 // the reflector of step k, by one warp of the CTA holding row k (hk, already
-// updated through step k - 1): v into vdst of every CTA of the cluster and row
-// k of refl; d[k] and e[k] = alpha
-__device__ __forceinline__ void td_reflector(cooperative_groups::cluster_group& cl, const TridiagJob& job,
-                                             const double2* hk, double2* vdst, int k, int lane) {
+// updated through step k - 1): v into vdst of every CTA of the cluster (bytes
+// on vbar) and row k of refl; d[k] and e[k] = alpha
+__device__ __forceinline__ void td_reflector(const TridiagJob& job, const double2* hk, double2* vdst,
+                                             uint64_t* vbar, int k, int lane, bool send) {
   const int B = job.B, j0 = k + 1;
   double s2a = 0.0, s2b = 0.0;  // two partial sums: half the FP64 dependency chain
   for (int j = j0 + lane; j < B; j += 64) {
@@ -113,8 +169,9 @@ __device__ __forceinline__ void td_reflector(cooperative_groups::cluster_group& 
     if (j == j0) x = make_double2(x.x - alpha.x, x.y - alpha.y);
     const double2 vj = make_double2(x.x * sc, x.y * sc);
     job.refl[(size_t)k * B + j] = vj;
+    if (send)
 #pragma unroll
-    for (int c = 0; c < kTdCl; ++c) cl.map_shared_rank(vdst, c)[j] = vj;
+      for (int c = 0; c < kTdCl; ++c) td_push(vdst + j, vj, vbar, (uint32_t)c);
   }
   if (lane == 0) {
     job.d[k] = hk[k].x;
@@ -127,25 +184,44 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
   namespace cg = cooperative_groups;
   cg::cluster_group cl = cg::this_cluster();
   extern __shared__ __align__(16) unsigned char tsm[];
+  __shared__ __align__(8) uint64_t s_vbar[2], s_pbar[2];
+  __shared__ int s_fail;
   const int me = (int)cl.block_rank();
   const TridiagJob job = jobs.j[blockIdx.x / kTdCl];
-  const int B = job.B, R = td_rows(B);
+  const int B = job.B, R = td_rows(B), nsteps = B - 2;
   double2* rows = reinterpret_cast<double2*>(tsm);  // R x B
   double2* vbuf = rows + (size_t)R * B;             // 2 x B (by step parity)
-  double2* pbuf = vbuf + 2 * (size_t)B;             // B
+  double2* pbuf = vbuf + 2 * (size_t)B;             // 2 x B
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = kTdThreads / 32;
   const double2 zero = make_double2(0.0, 0.0);
   for (int x = tid; x < R * B; x += kTdThreads) {
     const int l = x / B, j = x - l * B, i = kTdCl * l + me;
     rows[x] = i < B ? job.H[(size_t)i * B + j] : zero;
   }
-  __syncthreads();
-  if (B > 2 && me == 0 && warp == 0) td_reflector(cl, job, rows, vbuf, 0, lane);
-  for (int k = 0; k + 2 < B; ++k) {
-    // v of step k (by the warp that finished row k last step) is in every CTA,
-    // and every row of this CTA is updated through step k - 1
-    cl.sync();
-    const double2* v = vbuf + (size_t)(k & 1) * B;
+  if (tid == 0) {
+    for (int b = 0; b < 2; ++b) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(td_smem_u32(&s_vbar[b])), "r"(1) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(td_smem_u32(&s_pbar[b])), "r"(1) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    for (int k = 0; k < 2 && k < nsteps; ++k) {
+      td_arm(&s_vbar[k], td_step_bytes(B, k));
+      td_arm(&s_pbar[k], td_step_bytes(B, k));
+    }
+    s_fail = 0;
+  }
+  cl.sync();  // every CTA's barriers are armed before the first bytes are sent
+  bool fail = false;
+  if (nsteps > 0 && me == 0 && warp == 0) td_reflector(job, rows, vbuf, &s_vbar[0], 0, lane, true);
+  for (int k = 0; k < nsteps; ++k) {
+    const int par = k & 1;
+    const uint32_t ph = (uint32_t)((k >> 1) & 1);
+    const double2* v = vbuf + (size_t)par * B;
+    double2* pb = pbuf + (size_t)par * B;
+    // v of step k has landed, and every row of this CTA is updated through step k - 1
+    fail = !td_wait(&s_vbar[par], ph);
+    if (__syncthreads_or(fail)) break;
+    if (tid == 0 && k + 2 < nsteps) td_arm(&s_vbar[par], td_step_bytes(B, k + 2));
     const int j0 = k + 1;
     const int lfirst = k < me ? 0 : (k - me) / kTdCl + 1;  // first local row below row k
     for (int l = lfirst + warp; l < R; l += nwarp) {
@@ -165,34 +241,36 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
       }
       ax = warp_sum(ax + bx);
       ay = warp_sum(ay + by);
-      if (lane < kTdCl) cl.map_shared_rank(pbuf, lane)[i] = make_double2(ax, ay);
+      if (lane < kTdCl && !s_fail) td_push(pb + i, make_double2(ax, ay), &s_pbar[par], (uint32_t)lane);
     }
-    cl.sync();  // p of step k is in every CTA
+    // all of p has landed
+    fail = !td_wait(&s_pbar[par], ph);
+    if (__syncthreads_or(fail)) break;
+    if (tid == 0 && k + 2 < nsteps) td_arm(&s_pbar[par], td_step_bytes(B, k + 2));
     // c = Re(v^H p), the same sum in every warp
     double ca = 0.0, cb = 0.0;
     for (int j = j0 + lane; j < B; j += 64) {
-      const double2 a = v[j], b = pbuf[j];
+      const double2 a = v[j], b = pb[j];
       ca += fma(a.x, b.x, a.y * b.y);
       if (j + 32 < B) {
-        const double2 a2 = v[j + 32], b2 = pbuf[j + 32];
+        const double2 a2 = v[j + 32], b2 = pb[j + 32];
         cb += fma(a2.x, b2.x, a2.y * b2.y);
       }
     }
     const double c = warp_sum(ca + cb);
     // row k + 1 is the first row below k of its CTA, so warp 0 there updates it
-    // first and then forms the next step's reflector at once (the buffer it
-    // writes was last read in step k - 1, before the first barrier above)
-    const bool next = k + 3 < B && me == (k + 1) % kTdCl;
+    // first and then forms and sends the next step's reflector at once
+    const bool next = k + 1 < nsteps && me == (k + 1) % kTdCl;
     for (int l = lfirst + warp; l < R; l += nwarp) {
       const int i = kTdCl * l + me;
       if (i >= B) break;
       double2* hr = rows + (size_t)l * B;
-      const double2 vi = v[i], pi = pbuf[i];
+      const double2 vi = v[i], pi = pb[i];
       // 2 v_i and 2 w_i
       const double2 v2 = make_double2(2.0 * vi.x, 2.0 * vi.y);
       const double2 w2 = make_double2(2.0 * (pi.x - c * vi.x), 2.0 * (pi.y - c * vi.y));
       for (int j = j0 + lane; j < B; j += 32) {
-        const double2 vj = v[j], pj = pbuf[j];
+        const double2 vj = v[j], pj = pb[j];
         const double2 wj = make_double2(pj.x - c * vj.x, pj.y - c * vj.y);
         double2 h = hr[j];
         // h -= 2 v_i conj(w_j) + 2 w_i conj(v_j)
@@ -202,9 +280,14 @@ __global__ void __cluster_dims__(kTdCl, 1, 1) __launch_bounds__(kTdThreads, 1)
       }
       if (next && l == lfirst) {
         __syncwarp();
-        td_reflector(cl, job, hr, vbuf + (size_t)((k + 1) & 1) * B, k + 1, lane);
+        td_reflector(job, hr, vbuf + (size_t)(par ^ 1) * B, &s_vbar[par ^ 1], k + 1, lane, !s_fail);
       }
     }
+    __syncthreads();  // the rows are updated before the next step's matvec reads them
+  }
+  if (fail && tid == 0) {
+    if (job.err) atomicExch(job.err, 41);
+    for (int c = 0; c < kTdCl; ++c) *cl.map_shared_rank(&s_fail, c) = 1;  // peers stop sending
   }
   __syncthreads();
   // the trailing 2 x 2 block (or the 1 x 1 matrix)
@@ -231,18 +314,35 @@ __device__ __forceinline__ int sturm_count(const double* d, const double* e2, in
   double pm = 1.0, p = d[0] - x;
   int neg = p < 0.0 || p == 0.0;  // sign of p_1 (a zero counts as negative after p_0 = 1)
   int c = neg;
-  for (int i = 1; i < B; ++i) {
+  int i = 1;
+  // four steps per pass, their table entries loaded ahead of the chain
+  for (; i + 3 < B; i += 4) {
+    double dx[4], ee[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      dx[u] = d[i + u] - x;
+      ee[u] = e2[i + u - 1];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double pn = fma(dx[u], p, -ee[u] * pm);
+      pm = p;
+      p = pn;
+      const int n = p < 0.0 || (p == 0.0 && !neg);
+      c += n != neg;
+      neg = n;
+    }
+    const double a = fabs(p);
+    if (a > 0x1p400 || (a < 0x1p-400 && a > 0.0)) {
+      const double s = scalbn(1.0, -ilogb(a));
+      p *= s;
+      pm *= s;
+    }
+  }
+  for (; i < B; ++i) {
     const double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
     pm = p;
     p = pn;
-    if ((i & 3) == 0) {
-      const double a = fabs(p);
-      if (a > 0x1p400 || (a < 0x1p-400 && a > 0.0)) {
-        const double s = scalbn(1.0, -ilogb(a));
-        p *= s;
-        pm *= s;
-      }
-    }
     const int n = p < 0.0 || (p == 0.0 && !neg);
     c += n != neg;
     neg = n;

@@ -1468,8 +1468,11 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
     tri[i] = tridiag_eig_supported(S) ? 1 : 0;
     int arc;
     if ((arc = w.get(&w.G, (size_t)S * S)) || (arc = w.get(&w.Q, (size_t)S * S)) ||
-        (arc = w.get(&w.jst, (size_t)S + 1)) || (arc = w.get(&w.W, (size_t)S * K)) || (arc = w.get(&w.w, (size_t)S)))
+        (arc = w.get(&w.jst, (size_t)S + 1)) || (arc = w.get(&w.W, (size_t)S * K)) || (arc = w.get(&w.w, (size_t)S)) ||
+        (arc = w.get(&w.status, 1)))
       return arc;
+    // one status word for the Gram product's and the reduction's bounded waits
+    KL_CUDA_TRY(cudaMemsetAsync(w.status, 0, sizeof(int), st));
     if (tri[i]) {
       TridiagJob t{};
       double* lw = nullptr;
@@ -1490,13 +1493,12 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
       t.B = S;
       t.K = K;
       t.ldq = S;
+      t.err = w.status;
       tjobs.push_back(t);
     } else {
       if ((arc = w.get(&w.rot, jacobi_log_elems(S)))) return arc;
       jobs.push_back(JacobiJob{w.G, w.rot, w.Q, w.w, w.jst, S});
     }
-    if ((arc = w.get(&w.status, 1))) return arc;
-    KL_CUDA_TRY(cudaMemsetAsync(w.status, 0, sizeof(int), st));
     if (int rc = gram_factor(pr[i].A, pr[i].N, S, w.G, w.status, st)) return rc;
   }
   int rc = jacobi_batch(jobs, st);
@@ -1516,8 +1518,8 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
   for (size_t i = 0; i < n; ++i) {
     const int S = pr[i].S;
     if (gerr[i]) {
-      set_error("eig_topk_factor: the tensor-core Gram product timed out in its pipeline (code " +
-                std::to_string(gerr[i]) + ")");
+      set_error("eig_topk_factor: a bounded wait gave up (code " + std::to_string(gerr[i]) +
+                ": 31-35 the tensor-core Gram product, 41 the tridiagonal reduction's exchange)");
       return KL_ERR_CUDA;
     }
     if (tri[i]) {

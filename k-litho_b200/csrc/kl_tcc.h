@@ -129,6 +129,7 @@ struct TridiagJob {
   double* lw;        // B x K work: multipliers of the inverse-iteration solves
   double* Y;         // B x K work: eigenvectors of the real tridiagonal
   double2* Q;        // B x ldq, row-major: column j < K = eigenvector j
+  int* err;          // optional: set nonzero if an exchange wait of the reduction gave up
   int B, K, ldq;
 };
 // true when the device can run the cluster reduction for order B

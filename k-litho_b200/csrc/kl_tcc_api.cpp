@@ -348,7 +348,7 @@ int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* 
                "kl_hermitian_topk: this device cannot co-schedule the 8-CTA cluster of the reduction");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t n2 = sizeof(double2) * B * B, nv = sizeof(double) * B * K;
-  const size_t bytes = n2 + sizeof(double) * B + sizeof(double2) * B + 2 * nv;
+  const size_t bytes = n2 + sizeof(double) * B + sizeof(double2) * B + 2 * nv + 16;
   void* buf = nullptr;
   if (int rc = kl::scratch_alloc(&buf, bytes, st, "kl_hermitian_topk work")) return rc;
   char* c = static_cast<char*>(buf);
@@ -364,8 +364,23 @@ int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* 
   j.B = B;
   j.K = K;
   j.ldq = K;
-  const int rc = kl::tridiag_eig_batch({j}, st);
+  j.err = reinterpret_cast<int*>(j.Y + (size_t)B * K);
+  int rc = KL_OK, herr = 0;
+  if (cudaMemsetAsync(j.err, 0, sizeof(int), st) != cudaSuccess) {
+    kl::set_error("kl_hermitian_topk: cudaMemsetAsync failed");
+    rc = KL_ERR_CUDA;
+  }
+  if (!rc) rc = kl::tridiag_eig_batch({j}, st);
+  if (!rc && (cudaMemcpyAsync(&herr, j.err, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+              cudaStreamSynchronize(st) != cudaSuccess)) {
+    kl::set_error(std::string("kl_hermitian_topk: ") + cudaGetErrorString(cudaGetLastError()));
+    rc = KL_ERR_CUDA;
+  }
   kl::scratch_free(buf, st);
+  if (!rc && herr) {
+    kl::set_error("kl_hermitian_topk: the reduction's exchange wait gave up (code " + std::to_string(herr) + ")");
+    rc = KL_ERR_CUDA;
+  }
   return rc;
 }
 
