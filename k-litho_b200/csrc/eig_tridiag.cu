@@ -4,7 +4,7 @@
 // reference's zheevr (K-Litho-TCC/klitho_tcc.cpp:300-377) starts from too
 // (zheevr finishes with MRRR instead of bisection + inverse iteration).
 //
-// Four launches per batch of matrices:
+// Five launches per batch of matrices:
 //   k_hermitian_tridiag  one thread-block cluster of 8 CTAs per matrix, the
 //                        matrix's rows dealt round-robin over the CTAs'
 //                        shared memory; B - 2 reflector steps, each a
@@ -21,9 +21,9 @@
 //                        Gram-Schmidt against the earlier members of a cluster
 //                        of close eigenvalues (clusters run in rounds); the
 //                        vectors stay in shared memory when they fit
-//   k_tridiag_back       one warp per eigenvector: phases, then the B - 2
-//                        reflectors in reverse order, staged through shared
-//                        memory 16 at a time
+//   k_tridiag_wy         the compact WY factor T of each block of 8 reflectors
+//   k_tridiag_back       one warp per eigenvector: phases, then the reflector
+//                        blocks in reverse order, 8 reflectors per round
 // Everything is complex / real FP64.  The reduction's exchange waits are
 // bounded (2 s): a timeout sets the job's error word instead of spinning.
 #include <cooperative_groups.h>
@@ -43,8 +43,8 @@ constexpr int kTdCl = 8;            // CTAs per matrix (a portable cluster)
 constexpr int kTdThreads = 512;     // threads per CTA of the reduction
 constexpr int kTdMaxJobs = 16;      // matrices per launch
 constexpr int kTdBisPoints = 256;   // Sturm counts per pass of the bisection (threads per eigenvalue)
-constexpr int kTdBackWarps = 4;     // eigenvectors per CTA of the back-transform (more SMs per matrix)
-constexpr int kTdBackRefl = 16;     // reflectors staged per pass of the back-transform
+constexpr int kTdBackWarps = 8;     // eigenvectors per CTA of the back-transform (threads = kTridiagMaxB)
+constexpr int kTdNB = 8;            // reflectors per block of the back-transform
 constexpr size_t kTdInvSmemCap = 200 * 1024;  // inverse iteration keeps its vectors on chip up to this
 constexpr int kTdInvIters = 2;      // inverse-iteration solves per eigenvector (from a shift exact to a few ulps)
 constexpr int kTdChunk = 8;         // elements staged in registers per memory pass
@@ -92,8 +92,7 @@ __device__ __forceinline__ void td_push(double2* dst, double2 v, uint64_t* bar, 
                    td_cluster_addr(dst, cta)),
                "d"(v.x), "d"(v.y), "r"(td_cluster_addr(bar, cta))
                : "memory");
-}
-// this CTA expects `bytes` on `bar` in the barrier's current phase
+}// this CTA expects `bytes` on `bar` in the barrier's current phase
 __device__ __forceinline__ void td_arm(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(td_smem_u32(bar)), "r"(bytes)
                : "memory");
@@ -545,29 +544,90 @@ __global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs
     for (int x = j; x < B * K; x += blockDim.x) job.Y[x] = ism[x];
 }
 
-// Q[:, j] = H_0 H_1 ... H_{B-3} D Y[:, j], D = diag(phase) making the
-// subdiagonal real (phase_{k+1} = phase_k e_k / |e_k|).  A warp holds its
-// column in registers (lane: rows lane + 32 t); the CTA stages kTdBackRefl
-// reflectors at a time in shared memory for all its warps.
-__global__ void __launch_bounds__(32 * kTdBackWarps) k_tridiag_back(TridiagJobs jobs) {
-  constexpr int T = kTridiagMaxB / 32;
-  extern __shared__ __align__(16) double2 bsm[];  // kTdBackRefl x B
+// Compact WY factors of the reflector blocks: block b holds reflectors
+// k0 = kTdNB b .. k0 + nb - 1, and H_k0 ... H_{k0+nb-1} = I - V T V^H with
+// V = [v_k0 .. v_{k0+nb-1}] and T = (I/2 + striu(V^H V))^{-1} for unit v
+// (Joffrain, Low, Quintana-Orti, van de Geijn and Van Zee, "Accumulating
+// Householder transformations, revisited", ACM TOMS 2006).  One CTA per block:
+// its warps form the strictly upper part of V^H V, one thread inverts the
+// nb x nb triangle; T (zero-padded to kTdNB x kTdNB) goes to wy[b].
+__global__ void __launch_bounds__(256) k_tridiag_wy(TridiagJobs jobs) {
   const TridiagJob job = jobs.j[blockIdx.y];
-  const int B = job.B, K = job.K;
-  if ((int)blockIdx.x * kTdBackWarps >= K) return;  // the whole CTA
-  __shared__ double2 s_ph[kTridiagMaxB];
-  if (threadIdx.x == 0) {
-    double2 ph = make_double2(1.0, 0.0);
-    s_ph[0] = ph;
-    for (int k = 0; k + 1 < B; ++k) {
-      const double2 e = job.e[k];
-      const double a = sqrt(e.x * e.x + e.y * e.y);
-      if (a > 0.0) ph = zmul(ph, make_double2(e.x / a, e.y / a));
-      s_ph[k + 1] = ph;
+  const int B = job.B, b = blockIdx.x, k0 = kTdNB * b, nb = min(kTdNB, B - 2 - k0);
+  if (nb <= 0) return;  // the whole CTA
+  __shared__ double2 s_u[kTdNB][kTdNB];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int pq = warp; pq < kTdNB * kTdNB; pq += nwarp) {
+    const int r = pq / kTdNB, q = pq % kTdNB;
+    double ax = 0.0, ay = 0.0;
+    if (r < q && q < nb) {
+      const double2* vr = job.refl + (size_t)(k0 + r) * B;
+      const double2* vq = job.refl + (size_t)(k0 + q) * B;
+      for (int i = k0 + q + 1 + lane; i < B; i += 32) {  // v_q is supported on k0+q+1 ..
+        const double2 a = vr[i], c = vq[i];
+        ax += fma(a.x, c.x, a.y * c.y);
+        ay += fma(a.x, c.y, -a.y * c.x);
+      }
+      ax = warp_sum(ax);
+      ay = warp_sum(ay);
     }
+    if (lane == 0) s_u[r][q] = make_double2(ax, ay);  // conj(v_r) . v_q above the diagonal, else 0
   }
   __syncthreads();
-  const int lane = threadIdx.x & 31, j = blockIdx.x * kTdBackWarps + (threadIdx.x >> 5);
+  if (threadIdx.x == 0) {
+    double2 t[kTdNB][kTdNB];
+    for (int c = 0; c < kTdNB; ++c)
+      for (int r = kTdNB - 1; r >= 0; --r) {
+        if (r > c || c >= nb) {
+          t[r][c] = make_double2(0.0, 0.0);
+          continue;
+        }
+        // (I/2 + U) T = I: T[r][c] = 2 (delta_rc - sum_{q > r} U[r][q] T[q][c])
+        double sx = r == c ? 1.0 : 0.0, sy = 0.0;
+        for (int q = r + 1; q <= c; ++q) {
+          const double2 u = s_u[r][q], v = t[q][c];
+          sx -= u.x * v.x - u.y * v.y;
+          sy -= u.x * v.y + u.y * v.x;
+        }
+        t[r][c] = make_double2(2.0 * sx, 2.0 * sy);
+      }
+    double2* out = job.wy + (size_t)b * kTdNB * kTdNB;
+    for (int r = 0; r < kTdNB; ++r)
+      for (int c = 0; c < kTdNB; ++c) out[r * kTdNB + c] = t[r][c];
+  }
+}
+
+// Q[:, j] = H_0 H_1 ... H_{B-3} D Y[:, j], D = diag(phase) making the
+// subdiagonal real (phase_0 = 1, phase_{k+1} = phase_k e_k / |e_k|, a parallel
+// prefix product).  A warp holds its column x in registers (lane: rows
+// lane + 32 t) and applies the reflector blocks last to first, each as
+// x -= V (T (V^H x)): kTdNB dot products reduced together, then the update.
+// The CTA stages each block's V and T in shared memory for its warps.
+__global__ void __launch_bounds__(32 * kTdBackWarps) k_tridiag_back(TridiagJobs jobs) {
+  constexpr int T = kTridiagMaxB / 32;
+  extern __shared__ __align__(16) double2 bsm[];  // kTdNB x B block of V, then kTdNB x kTdNB T
+  const TridiagJob job = jobs.j[blockIdx.y];
+  const int B = job.B, K = job.K, tid = threadIdx.x;
+  if ((int)blockIdx.x * kTdBackWarps >= K) return;  // the whole CTA
+  __shared__ double2 s_ph[kTridiagMaxB];
+  {
+    const double2 one = make_double2(1.0, 0.0);
+    double2 u = one;  // factor tid of the product: e_{tid-1} / |e_{tid-1}|
+    if (tid >= 1 && tid < B) {
+      const double2 e = job.e[tid - 1];
+      const double a = sqrt(e.x * e.x + e.y * e.y);
+      if (a > 0.0) u = make_double2(e.x / a, e.y / a);
+    }
+    s_ph[tid] = u;
+    __syncthreads();
+    for (int off = 1; off < kTridiagMaxB; off <<= 1) {  // inclusive scan (Hillis-Steele)
+      const double2 o = tid >= off ? s_ph[tid - off] : one;
+      __syncthreads();
+      s_ph[tid] = zmul(o, s_ph[tid]);
+      __syncthreads();
+    }
+  }
+  const int lane = tid & 31, j = blockIdx.x * kTdBackWarps + (tid >> 5);
   const bool act = j < K;
   double2 vc[T];
 #pragma unroll
@@ -576,49 +636,86 @@ __global__ void __launch_bounds__(32 * kTdBackWarps) k_tridiag_back(TridiagJobs 
     const double y = (act && i < B) ? job.Y[(size_t)i * K + j] : 0.0;
     vc[t] = i < B ? make_double2(s_ph[i].x * y, s_ph[i].y * y) : make_double2(0.0, 0.0);
   }
-  // reflectors k1 .. k0 (descending) per stage
-  for (int k1 = B - 3; k1 >= 0; k1 -= kTdBackRefl) {
-    const int k0 = max(0, k1 - kTdBackRefl + 1), nref = k1 - k0 + 1;
-    __syncthreads();  // the previous stage's reflectors are used up
-    for (int x = threadIdx.x; x < nref * B; x += blockDim.x) {
-      const int r = x / B, i = x - r * B, k = k1 - r;
-      bsm[x] = i > k ? job.refl[(size_t)k * B + i] : make_double2(0.0, 0.0);
+  double2* sv = bsm;
+  double2* st = bsm + (size_t)kTdNB * B;
+  const int nblk = (B - 2 + kTdNB - 1) / kTdNB;
+  // this thread's share (entries tid + 256 u) of a block's V and T, loaded one
+  // block ahead so that the L2 latency overlaps the current block's work
+  constexpr int kPre = kTdNB * kTridiagMaxB / (32 * kTdBackWarps);
+  double2 pre[kPre], pret = make_double2(0.0, 0.0);
+  auto fetch = [&](int b) {
+    const int k0 = kTdNB * b;
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      const int x = tid + 32 * kTdBackWarps * u, r = x / B, i = x - r * B, k = k0 + r;
+      pre[u] = (x < kTdNB * B && k < B - 2 && i > k) ? job.refl[(size_t)k * B + i] : make_double2(0.0, 0.0);
     }
+    if (tid < kTdNB * kTdNB) pret = job.wy[(size_t)b * kTdNB * kTdNB + tid];
+  };
+  fetch(nblk - 1);
+  for (int b = nblk - 1; b >= 0; --b) {
+    __syncthreads();  // the previous block is used up
+#pragma unroll
+    for (int u = 0; u < kPre; ++u) {
+      const int x = tid + 32 * kTdBackWarps * u;
+      if (x < kTdNB * B) sv[x] = pre[u];
+    }
+    if (tid < kTdNB * kTdNB) st[tid] = pret;
     __syncthreads();
+    if (b > 0) fetch(b - 1);
     if (!act) continue;
-    for (int r = 0; r < nref; ++r) {
-      const double2* v = bsm + (size_t)r * B;
-      double2 vr[T];
+    // w = V^H x
+    double wx[kTdNB], wy[kTdNB];
+#pragma unroll
+    for (int r = 0; r < kTdNB; ++r) {
+      double ax = 0.0, ay = 0.0;
 #pragma unroll
       for (int t = 0; t < T; ++t) {
         const int i = lane + 32 * t;
-        vr[t] = i < B ? v[i] : make_double2(0.0, 0.0);
-      }
-      double px[T], py[T];  // s = v^H column: independent products, then a tree
-#pragma unroll
-      for (int t = 0; t < T; ++t) {
-        px[t] = fma(vr[t].x, vc[t].x, vr[t].y * vc[t].y);
-        py[t] = fma(vr[t].x, vc[t].y, -vr[t].y * vc[t].x);
-      }
-#pragma unroll
-      for (int h = T / 2; h > 0; h >>= 1)
-#pragma unroll
-        for (int t = 0; t < h; ++t) {
-          px[t] += px[t + h];
-          py[t] += py[t + h];
+        if (i < B) {
+          const double2 v = sv[r * B + i], x = vc[t];
+          ax = fma(v.x, x.x, fma(v.y, x.y, ax));
+          ay = fma(v.x, x.y, fma(-v.y, x.x, ay));
         }
-      double sx = px[0], sy = py[0];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        sx += __shfl_xor_sync(0xffffffffu, sx, o);
-        sy += __shfl_xor_sync(0xffffffffu, sy, o);
       }
-      sx *= 2.0;
-      sy *= 2.0;
+      wx[r] = ax;
+      wy[r] = ay;
+    }
 #pragma unroll
-      for (int t = 0; t < T; ++t) {
-        vc[t].x -= vr[t].x * sx - vr[t].y * sy;
-        vc[t].y -= vr[t].x * sy + vr[t].y * sx;
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int r = 0; r < kTdNB; ++r) {
+        wx[r] += __shfl_xor_sync(0xffffffffu, wx[r], o);
+        wy[r] += __shfl_xor_sync(0xffffffffu, wy[r], o);
+      }
+    // w' = T w (every lane)
+    double zx[kTdNB], zy[kTdNB];
+#pragma unroll
+    for (int r = 0; r < kTdNB; ++r) {
+      double ax = 0.0, ay = 0.0;
+#pragma unroll
+      for (int c = r; c < kTdNB; ++c) {
+        const double2 t = st[r * kTdNB + c];
+        ax += t.x * wx[c] - t.y * wy[c];
+        ay += t.x * wy[c] + t.y * wx[c];
+      }
+      zx[r] = ax;
+      zy[r] = ay;
+    }
+    // x -= V w'
+#pragma unroll
+    for (int t = 0; t < T; ++t) {
+      const int i = lane + 32 * t;
+      if (i < B) {
+        double dx = 0.0, dy = 0.0;
+#pragma unroll
+        for (int r = 0; r < kTdNB; ++r) {
+          const double2 v = sv[r * B + i];
+          dx += v.x * zx[r] - v.y * zy[r];
+          dy += v.x * zy[r] + v.y * zx[r];
+        }
+        vc[t].x -= dx;
+        vc[t].y -= dy;
       }
     }
   }
@@ -687,8 +784,9 @@ int tridiag_eig_batch(const std::vector<TridiagJob>& all, cudaStream_t st) {
       KL_CUDA_TRY(cudaFuncSetAttribute(k_tridiag_invit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ism));
     k_tridiag_invit<<<nj, kTridiagMaxB, on_chip ? ism : 0, st>>>(jobs, on_chip ? 1 : 0);
     KL_CUDA_TRY(cudaGetLastError());
-    const size_t bsm = sizeof(double2) * kTdBackRefl * (size_t)bmax;
-    KL_CUDA_TRY(cudaFuncSetAttribute(k_tridiag_back, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsm));
+    k_tridiag_wy<<<dim3(tridiag_wy_blocks(bmax), nj), 256, 0, st>>>(jobs);
+    KL_CUDA_TRY(cudaGetLastError());
+    const size_t bsm = sizeof(double2) * kTdNB * ((size_t)bmax + kTdNB);
     k_tridiag_back<<<dim3((kmax + kTdBackWarps - 1) / kTdBackWarps, nj), 32 * kTdBackWarps, bsm, st>>>(jobs);
     KL_CUDA_TRY(cudaGetLastError());
   }

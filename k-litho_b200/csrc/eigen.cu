@@ -1479,9 +1479,12 @@ int eig_topk_gram(const std::vector<FactorProblem>& pr, cudaStream_t st) {
       double* y = nullptr;
       double* d = nullptr;
       double2* e = nullptr;
+      double2* wyb = nullptr;
       if ((arc = w.get(&w.Z, (size_t)S * S)) || (arc = w.get(&d, (size_t)S)) || (arc = w.get(&e, (size_t)S)) ||
-          (arc = w.get(&lw, (size_t)S * K)) || (arc = w.get(&y, (size_t)S * K)))
+          (arc = w.get(&lw, (size_t)S * K)) || (arc = w.get(&y, (size_t)S * K)) ||
+          (arc = w.get(&wyb, (size_t)tridiag_wy_blocks(S) * 64)))
         return arc;
+      t.wy = wyb;
       t.H = w.G;
       t.refl = w.Z;
       t.d = d;

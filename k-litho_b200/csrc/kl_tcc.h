@@ -129,9 +129,12 @@ struct TridiagJob {
   double* lw;        // B x K work: multipliers of the inverse-iteration solves
   double* Y;         // B x K work: eigenvectors of the real tridiagonal
   double2* Q;        // B x ldq, row-major: column j < K = eigenvector j
+  double2* wy;       // tridiag_wy_blocks(B) x 8 x 8 work: compact WY factors of the reflector blocks
   int* err;          // optional: set nonzero if an exchange wait of the reduction gave up
   int B, K, ldq;
 };
+// reflector blocks of the back-transform of an order-B reduction
+inline int tridiag_wy_blocks(int B) { return (B - 2 + 7) / 8; }
 // true when the device can run the cluster reduction for order B
 bool tridiag_eig_supported(int B);
 int tridiag_eig_batch(const std::vector<TridiagJob>& jobs, cudaStream_t st);

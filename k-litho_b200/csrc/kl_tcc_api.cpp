@@ -348,13 +348,16 @@ int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* 
                "kl_hermitian_topk: this device cannot co-schedule the 8-CTA cluster of the reduction");
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   const size_t n2 = sizeof(double2) * B * B, nv = sizeof(double) * B * K;
-  const size_t bytes = n2 + sizeof(double) * B + sizeof(double2) * B + 2 * nv + 16;
+  const size_t nwy = sizeof(double2) * 64 * (size_t)kl::tridiag_wy_blocks(B);
+  const size_t bytes = n2 + nwy + sizeof(double) * B + sizeof(double2) * B + 2 * nv + 16;
   void* buf = nullptr;
   if (int rc = kl::scratch_alloc(&buf, bytes, st, "kl_hermitian_topk work")) return rc;
   char* c = static_cast<char*>(buf);
   kl::TridiagJob j{};
   j.H = static_cast<const double2*>(H_dev);
   j.refl = reinterpret_cast<double2*>(c);
+  j.wy = reinterpret_cast<double2*>(c + n2);
+  c += nwy;
   j.e = reinterpret_cast<double2*>(c + n2);
   j.d = reinterpret_cast<double*>(c + n2 + sizeof(double2) * B);
   j.lw = reinterpret_cast<double*>(c + n2 + sizeof(double2) * B + sizeof(double) * B);
