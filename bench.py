@@ -755,7 +755,8 @@ def bench_tcc_eigen(args):
     61^2 grid (98 source points), NA 1.35 water, K = 32, focus -50..50 nm in
     five steps.  Seconds per focus for
       fast (one focus per call): FP32 pupil factor, tcgen05 BF16x3 TCC, and the
-        top-K by one exact Rayleigh-Ritz step on span(A) (FP64 Gram + Jacobi);
+        top-K by one exact Rayleigh-Ritz step on span(A) (exact Gram on the
+        tensor cores + tridiagonal eigensolve on a thread-block cluster);
       fast (focus sweep): the five focus values through kl_topk_eig_batch,
         whose eigensolves share one launch (total / 5);
       plain FP64 GPU path: FP64 pupil table, FP64 TCC by direct accumulation,
@@ -829,7 +830,7 @@ def bench_tcc_eigen(args):
             "fast_plan_s_each": [round(x, 5) for x in fast_plan_t],
             "fp64_plan_s_each": [round(x, 5) for x in fp64_plan_t],
             "N": N, "S": int(K.sourcePointCount(src, K.getOuterSigma(src))), "focus_nm": focus,
-            "jacobi_sweeps": its, "tcc_rel_frobenius_err_vs_fp64": max(tcc_err),
+            "gram_solve_iterations": its, "tcc_rel_frobenius_err_vs_fp64": max(tcc_err),
             "eigenvalue_rel_err_vs_fp64": max(ev_err), "sweep_vs_single_eigenvalue_dev": batch_dev,
             "max_principal_angle_rad_vs_fp64": max(x["max_principal_angle_rad"] for x in subs),
             "weighted_projector_rel_err_vs_fp64": max(x["weighted_projector_rel_err"] for x in subs),
@@ -843,8 +844,9 @@ def bench_tcc_eigen_large(args):
     """TCC + top-K eigen at the stress field: 4096^2, cross-quadrupole
     (0.75, 0.12) on an 81^2 grid (196 source points), NA 1.35 water, K = 64,
     block 96.  Fast path: FP32 factor + the one-step Rayleigh-Ritz solve on
-    span(A) (FP64 Gram A^H A, 196 x 196, eigensolved by the thread-block-cluster
-    Jacobi); five focus values.  Plain FP64 GPU path: FP64 TCC by direct accumulation
+    span(A) (exact Gram A^H A on the tensor cores, 196 x 196, eigensolved by
+    Householder tridiagonalisation on a thread-block cluster, bisection and
+    inverse iteration); five focus values.  Plain FP64 GPU path: FP64 TCC by direct accumulation
     (N = 11449, 2.1 GB) and FP64 subspace iteration on the dense TCC, at one
     focus value (seconds per focus)."""
     import torch

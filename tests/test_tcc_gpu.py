@@ -159,7 +159,7 @@ def test_topk_batch_focus_sweep(cuda):
         assert np.abs(eb[i] - er).max() <= 1e-6 * np.abs(er).max()
         Pr = weighted_projector(kr, er)
         assert np.linalg.norm(weighted_projector(kb[i], eb[i]) - Pr) / np.linalg.norm(Pr) <= 1e-5
-        assert 0 < itb[i] < 40  # Jacobi sweeps of the one Gram solve
+        assert 0 < itb[i] < 40  # iterations of the one Gram solve (1 for the tridiagonal solver)
 
 
 def eig_residual(krn, ev, tcc):
@@ -174,9 +174,9 @@ def gap_cut(w, hi, rel=1e-3):
     return max(n for n in range(1, hi + 1) if w[n - 1] - w[n] > rel * w[0])
 
 
-def test_topk_batch_cluster_jacobi(cuda):
+def test_topk_batch_cluster_gram(cuda):
     # 196 source points: each focus value's 196 x 196 Gram eigensolve runs on
-    # one thread-block cluster, three clusters in one launch
+    # one thread-block cluster (the tridiagonal reduction), three in one launch
     L, nk = 512, 48
     src = K.createSource(71, "CrossQuadrupole", radius=0.12, offset=0.75)
     assert int((np.asarray(src) > 0).sum()) == 196
