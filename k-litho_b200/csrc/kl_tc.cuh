@@ -133,6 +133,11 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
+// the same for rows of 64 bytes with the 64-byte swizzle (8-row groups 512 B apart)
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
 // byte offset of element (row, k) of 2-byte operands inside one 64-wide K atom
 // of the layout smem_desc describes
 __host__ __device__ __forceinline__ uint32_t sw128_offset(int row, int k) {
@@ -211,7 +216,7 @@ inline EncodeTiledFn encode_fn() {
 // map of a row-major [rows][Kp] matrix of 2-byte elements, boxes of box_k x box_rows,
 // 128-byte swizzle (box_k * 2 must be 128)
 inline int make_map_2b(CUtensorMap* m, const void* base, int rows, int Kp, int box_k, int box_rows,
-                       CUtensorMapDataType dt) {
+                       CUtensorMapDataType dt, CUtensorMapSwizzle swz = CU_TENSOR_MAP_SWIZZLE_128B) {
   EncodeTiledFn enc = encode_fn();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled is unavailable");
@@ -222,7 +227,7 @@ inline int make_map_2b(CUtensorMap* m, const void* base, int rows, int Kp, int b
   const cuuint32_t box[2] = {(cuuint32_t)box_k, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(m, dt, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                   swz, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     set_error("cuTensorMapEncodeTiled failed with code " + std::to_string((int)r));
     return KL_ERR_CUDA;

@@ -41,7 +41,7 @@ int tcc_build_A(const SrcPoint* pts_dev, const PupilParams& pp, float2* A, cudaS
 
 // Device: bf16 split operands for TCC = A A^H on the tensor cores: four
 // planes X1h, X2h, X1l, X2l of N x K2p bf16 in one buffer (4 N K2p elements),
-// K2p = round_up(2 S, 64) = tcc_kp(S).
+// K2p = round_up(2 S, 32) = tcc_kp(S).
 int tcc_split_operands(const float2* A, int N, int S, int K2p, void* ops, cudaStream_t st);
 int tcc_kp(int S);
 

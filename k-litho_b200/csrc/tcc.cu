@@ -134,7 +134,7 @@ int tcc_build_A(const SrcPoint* pts_dev, const PupilParams& pp, float2* A, cudaS
 // ---------------------------------------------------------------------------
 // bf16 split operands
 // ---------------------------------------------------------------------------
-// Four planes of N x K2p bf16, K2p = round_up(2 S, 64), one after another in
+// Four planes of N x K2p bf16, K2p = round_up(2 S, 32), one after another in
 // one buffer: X1h, X2h, X1l, X2l.  With a = A[f][s] split as
 // a = ah + al (ah = bf16(a), al = bf16(a - ah)), the K index k < S holds the
 // real part of source point s = k, S <= k < 2S the imaginary part of s = k - S:
@@ -143,7 +143,7 @@ int tcc_build_A(const SrcPoint* pts_dev, const PupilParams& pp, float2* A, cudaS
 // (the three split terms; the lo x lo term is dropped), Y's tiles being X1's
 // rows of the other tile index.  Each hi tile is loaded once per k block and
 // used by two MMAs.
-int tcc_kp(int S) { return ((2 * S + 63) / 64) * 64; }
+int tcc_kp(int S) { return ((2 * S + 31) / 32) * 32; }
 
 __global__ void k_tcc_split(const float2* __restrict__ A, int N, int S, int K2p, __nv_bfloat16* __restrict__ ops) {
   const size_t n = (size_t)N * K2p, plane = n;
@@ -181,8 +181,11 @@ int tcc_split_operands(const float2* A, int N, int S, int K2p, void* ops, cudaSt
 // tcgen05 Hermitian GEMM
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int TM = 128, TN = 128, TK = 64;
-constexpr int TILE_BYTES = TM * TK * 2;         // 16 KB, one 128 x 64 bf16 tile
+// K blocks of 32 bf16: rows of 64 bytes in the 64-byte swizzle, so that four
+// stages fit in shared memory and three K blocks are in flight while one is
+// multiplied
+constexpr int TM = 128, TN = 128, TK = 32;
+constexpr int TILE_BYTES = TM * TK * 2;         // 8 KB, one 128 x 32 bf16 tile
 constexpr int STAGE_BYTES = 6 * TILE_BYTES;     // X1h X2h | X1l X2l | Yh | Yl
 // One MMA computes re and im of a tile: A = the Y tile (128 rows j), B = the X1
 // and X2 tiles stacked (256 rows: X1 then X2, adjacent in shared memory), so
@@ -197,7 +200,7 @@ using tc::mbar_init;
 using tc::mbar_wait;
 using tc::mbar_wait_ab;
 using tc::mma_commit;
-using tc::smem_desc;
+using tc::smem_desc_sw64;
 using tc::smem_u32;
 using tc::tma_load_2d;
 using tc::tmem_ld32;
@@ -215,7 +218,7 @@ __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t 
 // loads, MMAs and stores of consecutive tiles overlap.  Every wait is bounded:
 // a timeout records `err`, raises the CTA's abort flag and every role stops.
 namespace {
-constexpr int kStages = 2;
+constexpr int kStages = 4;
 constexpr int kEpiWarps = 4;
 constexpr int kGemmThreads = 32 * (2 + kEpiWarps);
 constexpr int EPI_BYTES = kEpiWarps * 32 * 33 * 8;  // per epilogue warp a 32 x 33 float2 tile
@@ -323,9 +326,9 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         for (int k = 0; k < TK / 16; ++k) {
           const uint32_t accum = (kb > 0 || k > 0) ? 1u : 0u;
           const uint32_t off = (uint32_t)(k * 32);  // 16 bf16 along K inside the swizzle atom
-          mma_bf16(acc, smem_desc(yh + off), smem_desc(xh + off), accum);
-          mma_bf16(acc, smem_desc(yl + off), smem_desc(xh + off), 1u);
-          mma_bf16(acc, smem_desc(yh + off), smem_desc(xl + off), 1u);
+          mma_bf16(acc, smem_desc_sw64(yh + off), smem_desc_sw64(xh + off), accum);
+          mma_bf16(acc, smem_desc_sw64(yl + off), smem_desc_sw64(xh + off), 1u);
+          mma_bf16(acc, smem_desc_sw64(yh + off), smem_desc_sw64(xl + off), 1u);
         }
         mma_commit(smem_u32(&empty[s]));
       }
@@ -402,7 +405,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
 
 namespace {
 int make_map(CUtensorMap* m, const void* base, int rows, int Kp) {
-  return tc::make_map_2b(m, base, rows, Kp, TK, TM, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16);
+  return tc::make_map_2b(m, base, rows, Kp, TK, TM, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, CU_TENSOR_MAP_SWIZZLE_64B);
 }
 }  // namespace
 
