@@ -526,8 +526,11 @@ int kl_socs_forward_host(kl_socs_plan p, const float* masks_host, int nclips, fl
   cudaStream_t sin = p->hs[0], scomp = p->hs[1], sout = p->hs[2];
   KL_CUDA_TRY(cudaEventRecord(p->hev[0], st));  // after earlier work on the caller's stream
   for (int i = 0; i < 3; ++i) KL_CUDA_TRY(cudaStreamWaitEvent(p->hs[i], p->hev[0], 0));
-  const int nchunks = nclips >= 16 ? 4 : (nclips >= 4 ? 2 : 1);
+  // chunks of about 64 MB of images (up to 16): the copy-out stream idles only
+  // while the first chunk is copied in and imaged, and the last copied out
   const size_t outpx = px * p->nsets;
+  const size_t outbytes = sizeof(float) * outpx * (size_t)nclips;
+  const int nchunks = (int)std::min<size_t>({(size_t)16, std::max<size_t>(1, outbytes >> 26), (size_t)nclips});
   for (int c = 0; c < nchunks; ++c) {
     const int a = (int)((long long)nclips * c / nchunks), b = (int)((long long)nclips * (c + 1) / nchunks);
     if (b == a) continue;
