@@ -345,3 +345,35 @@ def test_topk_planes_and_interleaved_agree(cuda):
     assert np.array_equal(krn.real.ravel(), re) and np.array_equal(krn.imag.ravel(), im)
     assert np.array_equal(sc, sc2) and np.array_equal(ev, ev2) and it == it2.value
     assert np.all(krn[-4:] == 0) and np.all(ev[-4:] == 0)
+
+
+def test_topk_batch_mixed_gram_orders(cuda):
+    # two sources with the same outer sigma (same band N) but 120 and 200 points:
+    # one batched launch holds Gram solves of different orders; each must equal
+    # the plan's own solve
+    sh = 20
+    far = (sh, 0)  # the same farthest point in both sources fixes sigma_o
+
+    def src_with(S, seed):
+        rng = np.random.default_rng(seed)
+        cand = [(p, q) for q in range(-sh, sh + 1) for p in range(-sh, sh + 1)
+                if p * p + q * q <= (0.8 * sh) ** 2]
+        pick = rng.choice(len(cand), size=S - 1, replace=False)
+        src = np.zeros((2 * sh + 1, 2 * sh + 1), dtype=np.float32)
+        for i in pick:
+            p, q = cand[i]
+            src[q + sh, p + sh] = 1.0
+        src[far[1] + sh, far[0] + sh] = 1.0
+        return src
+
+    L, nk = 1024, 24
+    srcs = [src_with(120, 1), src_with(200, 2)]
+    plans = [K.TccPlan(s, 1.35, synth.defocus_arg(10.0), L, L, n_medium=1.44) for s in srcs]
+    assert [p.S for p in plans] == [120, 200] and plans[0].N == plans[1].N
+    kb, sb, eb, itb = K.TccPlan.topk_batch(plans, nk)
+    for i, p in enumerate(plans):
+        k1, s1, e1, it1 = p.topk(nk)
+        assert np.abs(eb[i] - e1).max() <= 1e-12 * np.abs(e1).max()
+        assert np.linalg.norm(weighted_projector(kb[i], eb[i]) - weighted_projector(k1, e1)) <= \
+            1e-10 * np.linalg.norm(weighted_projector(k1, e1))
+        p.close()
