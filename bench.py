@@ -59,7 +59,7 @@ def peaks_tensor():
 
 
 def class_band(L):
-    # config-0 optics: annular 0.6/0.9 on 41^2, NA 1.35 (sigma_o = 0.9)
+    # the annular optics: annular 0.6/0.9 on 41^2, NA 1.35 (sigma_o = 0.9)
     import klitho as K
     src = K.createSource(41, "Annular", 0.6, 0.9)
     return K.bandSize(1.35, L, L, K.getOuterSigma(src))
@@ -214,7 +214,7 @@ def run_ours(args):
         mine = shard.partition(sizes, ws)[rank]
         counts = [sum(1 for i in mine if cls_of[i] == ci) for ci in range(len(CLASSES))]
         CLASSES[:] = [(L, c) for (L, _), c in zip(CLASSES, counts) if c > 0]
-    # kernel sets: config-0 optics (annular 0.6/0.9 on 41^2, NA 1.35, water) at
+    # kernel sets: the annular optics (annular 0.6/0.9 on 41^2, NA 1.35, water) at
     # each clip size and focus, K=24, from the GPU TCC + subspace iteration
     src = K.createSource(41, "Annular", 0.6, 0.9)
     plans, masks_d, imgs_d, masks_h, kset0, ksets = [], [], [], [], [], []
@@ -342,7 +342,7 @@ def run_ours(args):
                 "traffic": (int(TRAFFIC_PER_ALGORITHMIC_BYTE[names[dom]] * bytes_per_step[dom] / launches_per_step)
                             if names[dom] in TRAFFIC_PER_ALGORITHMIC_BYTE else None),
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the k_socs_synth_tc "
-                                  "captures at 2048^2 and 1024^2 (profiles/socs_synth_tc_full.md), scaled by pixels",
+                                  "captures at 2048^2 and 1024^2 (the ncu summaries of k_socs_synth_tc), scaled by pixels",
                 "kernels": sorted({("k_socs_synth_tc" if c["synthesis"] == "tensor" else "k_socs_inverse")
                                    for c in per_class}),
                 "algorithmic_bytes_per_launch": int(bytes_per_step[dom] / launches_per_step)}
@@ -921,8 +921,8 @@ def bench_tcc_eigen_large(args):
 def bench_tcc_gemm(args):
     """The TCC as a materialised matrix (kl_tcc_build: BF16x3 split + tcgen05
     GEMM, FP32 accumulate in TMEM, Hermitian mirror in the epilogue), CUDA
-    events around the call on its stream, at config 1 (2048^2 dipole, N = 2809,
-    S = 98) and config 4 (4096^2 cross-quadrupole, N = 11449, S = 196).
+    events around the call on its stream, at the 2048^2 dipole field (N = 2809,
+    S = 98) and the 4096^2 cross-quadrupole field (N = 11449, S = 196).
     Rooflines: tensor (8 N^2 S flop, the dense complex product counted once)
     against the measured bf16 peak, and store (N^2 x 8 B of complex64)
     against the measured HBM copy bandwidth."""
@@ -998,7 +998,7 @@ def run_e2e(plans, masks_h, args, ws, img_equiv):
 # ---------------------------------------------------------------------------
 
 def workload_config():
-    """The benchmark workload (both arms): BASELINE config 2's clip mix and focus values."""
+    """The benchmark workload (both arms): the batched forward's clip mix and focus values."""
     return {"workload": "batched SOCS forward: 128x512^2 + 192x1024^2 + 64x2048^2 clips x 3 focus, K=24",
             "clips_per_gpu": sum(n for _, n in CLASSES), "focus_nm": FOCUS_NM}
 
