@@ -422,10 +422,12 @@ __device__ __forceinline__ double td_start(int j, int i) {
 }
 
 // Y[:, j] = eigenvector j of the real tridiagonal (d, |e|) for eigenvalue w[j]:
-// kTdInvIters solves (T - w_j I) y' = y with T - w_j I = L D L^T unpivoted
-// (pivots below eps ||T|| raised to it), each followed by Gram-Schmidt against
-// the finished members of j's cluster and normalisation.  Round r solves the
-// r-th member of every cluster.  The vectors and multipliers are B x K,
+// solves (T - w_j I) y' = y with T - w_j I = L D L^T unpivoted (pivots below
+// eps ||T|| raised to it).  Round 0 gives every vector kTdInvIters solves from
+// its own start vector; round r takes the r-th member of every cluster of close
+// eigenvalues through Gram-Schmidt against the cluster's finished members, one
+// more solve and Gram-Schmidt again (three solve times for a cluster of two
+// instead of four).  The vectors and multipliers are B x K,
 // row-major ([i][j]: the threads of a warp touch consecutive words), in shared
 // memory when they fit (smem != 0), else in the job's work buffers.
 __global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs, int smem) {
@@ -462,81 +464,94 @@ __global__ void __launch_bounds__(kTridiagMaxB) k_tridiag_invit(TridiagJobs jobs
   const double floor = fmax(kEps * s_tn, kSafeMin);
   double* Y = smem ? ism : job.Y;
   double* L = smem ? ism + (size_t)B * K : job.lw;
+  const double lam = j < K ? s_w[j] : 0.0;
+  // one solve (T - lam I) y' = y in place; returns ||y'||^2
+  auto solve = [&]() -> double {
+    // forward: q_i = (d_i - lam) - e_{i-1} l_{i-1}, l_i = e_i / q_i, z_i = y_i - l_{i-1} z_{i-1};
+    // Y[i] <- z_i / q_i
+    double q = s_d[0] - lam;
+    if (fabs(q) < floor) q = copysign(floor, q);
+    double z = 0.0, lprev = 0.0;
+    for (int i0 = 0; i0 < B; i0 += kTdChunk) {
+      double yv[kTdChunk], zq[kTdChunk], lv[kTdChunk];
+#pragma unroll
+      for (int u = 0; u < kTdChunk; ++u) yv[u] = i0 + u < B ? Y[(size_t)(i0 + u) * K + j] : 0.0;
+#pragma unroll
+      for (int u = 0; u < kTdChunk; ++u) {
+        const int i = i0 + u;
+        if (i < B) {
+          if (i > 0) {
+            q = (s_d[i] - lam) - s_e[i - 1] * lprev;
+            if (fabs(q) < floor) q = copysign(floor, q);
+          }
+          const double rq = 1.0 / q;
+          z = yv[u] - lprev * z;
+          lprev = s_e[i] * rq;
+          zq[u] = z * rq;
+          lv[u] = lprev;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kTdChunk; ++u)
+        if (i0 + u < B) {
+          Y[(size_t)(i0 + u) * K + j] = zq[u];
+          L[(size_t)(i0 + u) * K + j] = lv[u];
+        }
+    }
+    // backward: y_i = Y[i] - l_i y_{i+1}
+    double y = 0.0, nrm = 0.0;
+    for (int i1 = B; i1 > 0; i1 -= kTdChunk) {
+      double zv[kTdChunk], lv[kTdChunk];
+#pragma unroll
+      for (int u = 0; u < kTdChunk; ++u) {
+        const int i = i1 - 1 - u;
+        zv[u] = i >= 0 ? Y[(size_t)i * K + j] : 0.0;
+        lv[u] = i >= 0 ? L[(size_t)i * K + j] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < kTdChunk; ++u) {
+        const int i = i1 - 1 - u;
+        if (i >= 0) {
+          y = i == B - 1 ? zv[u] : zv[u] - lv[u] * y;
+          zv[u] = y;
+          nrm = fma(y, y, nrm);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kTdChunk; ++u) {
+        const int i = i1 - 1 - u;
+        if (i >= 0) Y[(size_t)i * K + j] = zv[u];
+      }
+    }
+    return nrm;
+  };
+  // modified Gram-Schmidt against the cluster's finished members; returns ||y||^2
+  auto orthogonalise = [&]() -> double {
+    for (int m = s_first[j]; m < j; ++m) {
+      double dot = 0.0;
+      for (int i = 0; i < B; ++i) dot = fma(Y[(size_t)i * K + m], Y[(size_t)i * K + j], dot);
+      for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] -= dot * Y[(size_t)i * K + m];
+    }
+    double nrm = 0.0;
+    for (int i = 0; i < B; ++i) nrm = fma(Y[(size_t)i * K + j], Y[(size_t)i * K + j], nrm);
+    return nrm;
+  };
+  auto normalise = [&](double nrm) {
+    const double sc = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
+    for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] *= sc;
+  };
+  // round 0: every vector takes kTdInvIters solves from its start vector; round
+  // r: the r-th member of each cluster is orthogonalised against the earlier
+  // ones (final by now), solved once more and orthogonalised again
   const int nr = s_rounds;
   for (int r = 0; r < nr; ++r) {
-    if (j < K && s_pos[j] == r) {
-      const double lam = s_w[j];
+    if (j < K && r == 0) {
       for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] = td_start(j, i);
-      for (int it = 0; it < kTdInvIters; ++it) {
-        // forward: q_i = (d_i - lam) - e_{i-1} l_{i-1}, l_i = e_i / q_i, z_i = y_i - l_{i-1} z_{i-1};
-        // Y[i] <- z_i / q_i
-        double q = s_d[0] - lam;
-        if (fabs(q) < floor) q = copysign(floor, q);
-        double z = 0.0, lprev = 0.0;
-        for (int i0 = 0; i0 < B; i0 += kTdChunk) {
-          double yv[kTdChunk], zq[kTdChunk], lv[kTdChunk];
-#pragma unroll
-          for (int u = 0; u < kTdChunk; ++u) yv[u] = i0 + u < B ? Y[(size_t)(i0 + u) * K + j] : 0.0;
-#pragma unroll
-          for (int u = 0; u < kTdChunk; ++u) {
-            const int i = i0 + u;
-            if (i < B) {
-              if (i > 0) {
-                q = (s_d[i] - lam) - s_e[i - 1] * lprev;
-                if (fabs(q) < floor) q = copysign(floor, q);
-              }
-              const double rq = 1.0 / q;
-              z = yv[u] - lprev * z;
-              lprev = s_e[i] * rq;
-              zq[u] = z * rq;
-              lv[u] = lprev;
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < kTdChunk; ++u)
-            if (i0 + u < B) {
-              Y[(size_t)(i0 + u) * K + j] = zq[u];
-              L[(size_t)(i0 + u) * K + j] = lv[u];
-            }
-        }
-        // backward: y_i = Y[i] - l_i y_{i+1}
-        double y = 0.0, nrm = 0.0;
-        for (int i1 = B; i1 > 0; i1 -= kTdChunk) {
-          double zv[kTdChunk], lv[kTdChunk];
-#pragma unroll
-          for (int u = 0; u < kTdChunk; ++u) {
-            const int i = i1 - 1 - u;
-            zv[u] = i >= 0 ? Y[(size_t)i * K + j] : 0.0;
-            lv[u] = i >= 0 ? L[(size_t)i * K + j] : 0.0;
-          }
-#pragma unroll
-          for (int u = 0; u < kTdChunk; ++u) {
-            const int i = i1 - 1 - u;
-            if (i >= 0) {
-              y = i == B - 1 ? zv[u] : zv[u] - lv[u] * y;
-              zv[u] = y;
-              nrm = fma(y, y, nrm);
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < kTdChunk; ++u) {
-            const int i = i1 - 1 - u;
-            if (i >= 0) Y[(size_t)i * K + j] = zv[u];
-          }
-        }
-        // modified Gram-Schmidt against the cluster's finished members
-        if (s_first[j] < j) {
-          for (int m = s_first[j]; m < j; ++m) {
-            double dot = 0.0;
-            for (int i = 0; i < B; ++i) dot = fma(Y[(size_t)i * K + m], Y[(size_t)i * K + j], dot);
-            for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] -= dot * Y[(size_t)i * K + m];
-          }
-          nrm = 0.0;
-          for (int i = 0; i < B; ++i) nrm = fma(Y[(size_t)i * K + j], Y[(size_t)i * K + j], nrm);
-        }
-        const double s = nrm > 0.0 ? 1.0 / sqrt(nrm) : 0.0;
-        for (int i = 0; i < B; ++i) Y[(size_t)i * K + j] *= s;
-      }
+      for (int it = 0; it < kTdInvIters; ++it) normalise(solve());
+    } else if (j < K && s_pos[j] == r) {
+      normalise(orthogonalise());
+      normalise(solve());
+      normalise(orthogonalise());
     }
     __syncthreads();  // this round's vectors are final before the next round reads them
   }
