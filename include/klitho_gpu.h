@@ -378,12 +378,16 @@ int kl_tcc_build_minmax(kl_tcc_plan plan, double* out4);
  * tcc_i.png.  Synchronous. */
 int kl_tcc_build_host(kl_tcc_plan plan, float* re_host, float* im_host);
 
-/* calcKernels (klitho_tcc.cpp:300-377): top-nk eigenpairs of the TCC by
- * blocked subspace iteration (block `block`, 0 = automatic) with FP64
- * CholeskyQR2 and Rayleigh-Ritz, in descending order; kernels in the
- * reference layout krn[k][j] = v_k[N-1-j] as float planes (nk x N each),
- * scales = eigenvalues as float, evals_host (optional) in double.
- * Returns KL_ERR_NOT_CONVERGED if the iteration cap is reached. */
+/* calcKernels (klitho_tcc.cpp:300-377): top-nk eigenpairs of the TCC, in
+ * descending order.  Fast plans with S <= 256 source points take one exact
+ * Rayleigh-Ritz step on the source span: G = A^H A (kl_factor_gram), its
+ * top-nk by the tridiagonal solver (kl_hermitian_topk; Jacobi below order 64),
+ * U = A V diag(w)^-1/2; `iterations` is 1.  Otherwise blocked subspace
+ * iteration (block `block`, 0 = automatic) with FP64 CholeskyQR2 and
+ * Rayleigh-Ritz, returning KL_ERR_NOT_CONVERGED if the iteration cap is
+ * reached.  Kernels in the reference layout krn[k][j] = v_k[N-1-j] as float
+ * planes (nk x N each), scales = eigenvalues as float, evals_host (optional)
+ * in double. */
 int kl_topk_eig(kl_tcc_plan plan, int nk, int block, float* krn_re_host, float* krn_im_host,
                 float* scales_host, double* evals_host, int* iterations);
 /* kl_topk_eig for nplans plans that share the pupil band N (e.g. one per
