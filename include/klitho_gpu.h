@@ -357,8 +357,10 @@ int kl_factor_gram(const void* A_dev, int N, int S, void* G_dev, void* stream);
  * TCC is reduced to its source span.  Householder tridiagonalisation on a
  * cluster of 8 CTAs, bisection, inverse iteration; eigenvalues descending into
  * evals_dev (K doubles), eigenvector j into column j of vecs_dev (B x K
- * complex128, row-major).  H_dev is not modified.  Synchronous (reports a
- * timed-out exchange of the reduction). */
+ * complex128, row-major).  H_dev is not modified.  The reduction forms sums of
+ * squares of the entries without rescaling: entries should lie within about
+ * 1e-150 .. 1e150 in magnitude (a Gram matrix of a TCC factor is far inside).
+ * Synchronous (reports a timed-out exchange of the reduction). */
 int kl_hermitian_topk(const void* H_dev, int B, int K, double* evals_dev, void* vecs_dev, void* stream);
 
 /* calcTCC (klitho_tcc.cpp:186-267): the N x N Hermitian TCC, row-major, into
