@@ -15,6 +15,7 @@ import pytest
 
 import klitho as K
 import synth
+from oracle import oracle as O
 from pngread import read_png
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -149,6 +150,22 @@ def test_tcc_cli_matches_reference_program(tmp_path, ref_built):
     mfile = tmp_path / "mask.bin"
     mask.astype(np.float32).tofile(mfile)
     run_both_tcc(tmp_path, tcc_args(L, ms, str(mfile)), L, L)
+
+
+@pytest.mark.gpu
+def test_tcc_cli_gram_path_matches_reference_program(tmp_path, ref_built):
+    # a cross-quadrupole source of 196 points (radius 0.2, offset 0.5 on 41^2):
+    # the drop-in's kernels come from the exact Gram step (Gram product on the
+    # tensor cores, tridiagonal eigensolve on a thread-block cluster)
+    L, ms = 512, 256
+    mask = synth.rect_mask(ms, 12, seed=22)
+    mfile = tmp_path / "mask.bin"
+    mask.astype(np.float32).tofile(mfile)
+    args = tcc_args(L, ms, str(mfile), srcType="CrossQuadrupole")
+    args[13] = 0.2  # radius
+    src = K.createSource(41, "CrossQuadrupole", radius=0.2, offset=0.5)
+    assert O.source_point_count(src, O.outer_sigma(src)) == 196
+    run_both_tcc(tmp_path, args, L, L)
 
 
 # periods the reference accepts (klitho_tcc.cpp:391-429) beyond powers of two:
